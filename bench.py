@@ -1,0 +1,328 @@
+"""Benchmark of the plain production swarm (L=64, 32768 replicas per GPU,
+beta=0.54, h=0.07, all-down start, magnetisation check every 100 sweeps,
+grid dump every 1000 sweeps) in the reference-exact mode (gpu_method 2
+semantics, cuRAND XORWOW stream).
+
+One step = one check interval: 100 sweeps of every replica (32768 * 4096 *
+100 attempted flips) plus the fused magnetisation of the resulting state.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Prints one JSON line on rank 0.  Multi-GPU: replicas are independent, so each
+rank runs its own 32768 replicas (weak scaling, no data-path collective); the
+timing is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+L, R, BETA, H = 64, 32768, 0.54, 0.07
+SWEEPS_PER_STEP, MAG_INT, GRID_INT = 100, 100, 1000
+SEED = 20240501
+OPS_PER_ATTEMPT = 65  # canonical lane-op count of one exact-mode attempt
+METRIC = "spin-flip attempts/s"
+UNIT = "attempts/s"
+CONFIG = {
+    "workload": "plain production swarm, gpu_method 2 exact: L=64, 32768 replicas/GPU, "
+                "beta=0.54, h=0.07, all-down start; step = 100 sweeps + magnetisation",
+    "L": L, "replicas_per_gpu": R, "sweeps_per_step": SWEEPS_PER_STEP,
+    "mag_output_int": MAG_INT, "grid_output_int": GRID_INT,
+    "rng": "cuRAND XORWOW per replica (reference stream)",
+    "l2": "flushed between timed steps (256 MiB device write)",
+}
+CPU_SAMPLE = {"replicas_per_process": 32, "sweeps": 400}
+
+
+def load_peaks():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d.get("sm_max_mhz", 1965.0)), "measured"
+    return 1965.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.out = ""
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=10)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                self.out, _ = self.proc.communicate()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in (self.out or "").splitlines():
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_reference_sample(nproc=None, replicas=None, sweeps=None):
+    """The reference's own CPU driver (oracle/_ref/ref_cpu_bench: mc_cpu.c +
+    mt19937ar.c compiled unmodified) on every host core, one process per core
+    (its MT19937 state is a process global).  Returns attempts/s, cores, sample."""
+    exe = os.path.join(REPO, "oracle", "_ref", "ref_cpu_bench")
+    if not os.path.exists(exe):
+        return None
+    nproc = nproc or len(os.sched_getaffinity(0))
+    replicas = replicas or CPU_SAMPLE["replicas_per_process"]
+    sweeps = sweeps or CPU_SAMPLE["sweeps"]
+    t0 = time.perf_counter()
+    procs = [subprocess.Popen([exe, str(L), str(replicas), str(sweeps), str(MAG_INT), str(BETA),
+                               str(H), str(SEED + i)], stdout=subprocess.DEVNULL,
+                              stderr=subprocess.PIPE, text=True) for i in range(nproc)]
+    attempts = 0.0
+    for p in procs:
+        _, err = p.communicate()
+        a, _w = err.split()[-2:]
+        attempts += float(a)
+    wall = time.perf_counter() - t0
+    sample = (f"{nproc} processes x {replicas} replicas x {sweeps} sweeps of L={L} "
+              f"(beta={BETA}, h={H}, all-down), mc_driver_cpu unmodified")
+    return attempts / wall, nproc, sample, wall
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    res = [cpu_reference_sample() for _ in range(args.warmup)]
+    t_total, a_total = 0.0, 0.0
+    last = None
+    for _ in range(args.steps):
+        last = cpu_reference_sample()
+        if last is None:
+            break
+        rate, nproc, sample, wall = last
+        t_total += wall
+        a_total += rate * wall
+    if last is None:
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "oracle/_ref/ref_cpu_bench not built (make -C oracle ref)"}))
+        return
+    del res
+    value = a_total / t_total
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "i32",
+        "data": "synthetic", "config": CONFIG, "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": last[1], "kind": "reference",
+                         "sample": last[2]},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def read_profile_traffic():
+    """DRAM bytes per sweep launch from the committed ncu summary, if any."""
+    p = os.path.join(REPO, "profiles", "sweep_exact_L64_R32768.txt")
+    if not os.path.exists(p):
+        return None
+    for ln in open(p):
+        if ln.startswith("dram_bytes_per_launch_full_size:"):
+            try:
+                return float(ln.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+def run_e2e(args, rank, world, dist, torch, engine):
+    engine.set_stream(0)
+    host = -np.ones((R, L, L), np.int32)
+    dumped = [0]
+
+    def packed(L_, ng_, payload, isweep, m):
+        dumped[0] += payload.size
+        return 0
+
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    t0 = time.perf_counter()
+    dg2 = engine.DeviceGrids(L, R, host)
+    rng2 = engine.RngStates(R, SEED + 7919 * rank + 1)
+    _, _, _, attempts = engine.run_driver(dg2, rng2, BETA, H, SWEEPS_PER_STEP * args.steps,
+                                          MAG_INT, GRID_INT, itask=0, dn_thr=-0.9, up_thr=0.9,
+                                          packed_out=packed)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    if dist is not None:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    h2d = R * L * L * 4 + 20 * 4 + 20 * 8
+    d2h = R * 4 * (SWEEPS_PER_STEP * args.steps // MAG_INT) + dumped[0]
+    dg2.close()
+    rng2.close()
+    return {"value": attempts * world / e2e_s, "unit": UNIT,
+            "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
+            "wall_s": e2e_s,
+            "scope": "gasp_init_grid (int32 host grids) + gasp_init_rand + "
+                     "gasp_mc_driver_gpu over all steps (per-check magnetisation D2H, "
+                     "packed dumps every 1000 sweeps)"}
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    from gpu_2dising_b200 import engine
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+    engine.init_device(local_rank)
+    stream = torch.cuda.Stream()
+    engine.set_stream(stream.cuda_stream)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+
+    dg = engine.DeviceGrids(L, R, -np.ones((R, L, L), np.int32))
+    rng = engine.RngStates(R, SEED + 7919 * rank)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            dg.sweep(rng, BETA, H, SWEEPS_PER_STEP, gpu_method=2)
+        barrier()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(args.steps)]
+        with ClockSampler(local_rank) as clk:
+            for e0, e1 in evs:
+                flush.zero_()
+                e0.record(stream)
+                dg.sweep(rng, BETA, H, SWEEPS_PER_STEP, gpu_method=2)
+                e1.record(stream)
+            barrier()
+        t_ms = sum(e0.elapsed_time(e1) for e0, e1 in evs)
+    t_max = t_ms
+    if dist is not None:
+        t = torch.tensor([t_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_max = float(t.item())
+    attempts_step = float(R) * L * L * SWEEPS_PER_STEP
+    value = attempts_step * args.steps * world / (t_max / 1e3)
+    mag = dg.magnetisation()
+    assert np.all(np.abs(mag) <= 1.0)
+
+    # End to end through the public driver (gasp_mc_driver_gpu): host int32
+    # grids in, RNG seeding, K check intervals with the per-check
+    # magnetisation read back and packed grid dumps, results out.
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(args, rank, world, dist, torch, engine)
+    if rank == 0:
+        sm_max_mhz, peak_kind = load_peaks()
+        peak = 148 * 128 * sm_max_mhz * 1e6 / 1e12       # T lane-ops/s
+        launch_s = t_max / 1e3 / args.steps
+        achieved = OPS_PER_ATTEMPT * attempts_step / launch_s / 1e12
+        traffic = read_profile_traffic()
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            c = cpu_reference_sample()
+            if c is not None:
+                cpu = {"value": c[0], "unit": UNIT, "cores": c[1], "kind": "reference",
+                       "sample": c[2]}
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic (all-down L=64 lattices, seeded cuRAND streams)",
+            "config": CONFIG,
+            "roofline": {"bound": "int-issue", "achieved": achieved, "peak": peak,
+                         "unit": "Tlane-op/s", "frac": achieved / peak, "traffic": traffic,
+                         "ops_per_attempt": OPS_PER_ATTEMPT,
+                         "peak_basis": f"148 SMs x 128 lanes x {sm_max_mhz:.0f} MHz "
+                                       f"({peak_kind} sm_max_mhz)"},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": args.steps,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--sweeps-per-step", type=int, default=SWEEPS_PER_STEP,
+                    help="smaller values give a short launch for ncu captures")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    global SWEEPS_PER_STEP
+    SWEEPS_PER_STEP = args.sweeps_per_step
+    CONFIG["sweeps_per_step"] = SWEEPS_PER_STEP
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+    else:
+        run_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

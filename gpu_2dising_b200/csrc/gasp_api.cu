@@ -1,0 +1,768 @@
+// gasp_api.cu -- host implementation of the gasp-b200 C ABI (include/gasp.h):
+// device set-up, replica sets, RNG states, single sweep batches and the
+// reference-compatible driver loop (replaces mc_driver_gpu,
+// src/mc_gpu.cu:530-831).
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <chrono>
+#include <string>
+#include <vector>
+
+#include "gasp_internal.h"
+
+namespace gasp {
+
+static thread_local std::string g_err;
+static thread_local cudaStream_t g_stream = nullptr;
+
+void set_error(const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_err = buf;
+}
+
+int cuda_fail(cudaError_t e, const char *what, const char *file, int line) {
+  set_error("%s: %s (%s:%d)", what, cudaGetErrorString(e), file, line);
+  if (e == cudaErrorMemoryAllocation) return GASP_ERR_ALLOC;
+  if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return GASP_ERR_NO_DEVICE;
+  return GASP_ERR_CUDA;
+}
+
+cudaStream_t current_stream() { return g_stream; }
+
+}  // namespace gasp
+
+using namespace gasp;
+
+namespace {
+
+// Device-side table block of a replica set: thresholds, float and double
+// acceptance tables, flags.
+struct TableBlock {
+  uint32_t thr[16];
+  float pacc[20];
+  float pad_[12];
+  double pacc_cpu[20];
+  int flags[4];
+};
+
+struct GridsExtra {
+  TableBlock *d_tab = nullptr;
+  double beta = NAN, h = NAN;
+  int float_cmp = 0;
+  double *d_stream = nullptr;
+  size_t stream_cap = 0;
+  float *d_mag2 = nullptr;  // second magnetisation buffer for the driver
+  int *d_active = nullptr;
+};
+
+// Extra state kept beside the public struct (allocated with it).
+struct GridsImpl {
+  gasp_grids pub;
+  GridsExtra x;
+};
+
+GridsImpl *impl(gasp_grids_t *g) { return reinterpret_cast<GridsImpl *>(g); }
+
+void host_probs_gpu(double beta, double h, float P[20]) {
+  // src/mc_gpu.cu:21-37, with the host expf.
+  for (int i = 0; i < 20; ++i) P[i] = 0.f;
+  for (int s = -1; s < 2; s += 2)
+    for (int nsum = -4; nsum < 5; nsum += 2) {
+      const int index = 5 * (s + 1) + nsum + 4;
+      const float de = 2.0f * (float)s * ((float)nsum + (float)h);
+      P[index] = expf(-(float)beta * de);
+    }
+}
+
+void host_probs_cpu(double beta, double h, double P[20]) {
+  // src/mc_cpu.c:14-38.
+  for (int i = 0; i < 20; ++i) P[i] = 0.0;
+  for (int s = -1; s < 2; s += 2)
+    for (int nsum = -4; nsum < 5; nsum += 2) {
+      const int index = 5 * (s + 1) + nsum + 4;
+      P[index] = exp(-beta * (2.0 * (double)s * ((double)nsum + h)));
+    }
+}
+
+// Makes the replica set's tables match (beta, h).  Synchronous on change.
+int ensure_tables(gasp_grids_t *g, double beta, double h) {
+  GridsExtra &x = impl(g)->x;
+  if (x.d_tab && x.beta == beta && x.h == h) return GASP_OK;
+  if (!x.d_tab) GASP_CUDA(cudaMalloc(&x.d_tab, sizeof(TableBlock)));
+  TableBlock hb;
+  memset(&hb, 0, sizeof hb);
+  host_probs_gpu(beta, h, hb.pacc);
+  host_probs_cpu(beta, h, hb.pacc_cpu);
+  cudaStream_t s = current_stream();
+  GASP_CUDA(cudaMemcpyAsync(x.d_tab, &hb, sizeof hb, cudaMemcpyHostToDevice, s));
+  int rc = launch_build_thresholds(x.d_tab->pacc, x.d_tab->thr, x.d_tab->flags, s);
+  if (rc) return rc;
+  int flags[4];
+  GASP_CUDA(cudaMemcpyAsync(flags, x.d_tab->flags, sizeof flags, cudaMemcpyDeviceToHost, s));
+  GASP_CUDA(cudaStreamSynchronize(s));
+  x.float_cmp = flags[0] != 0;
+  x.beta = beta;
+  x.h = h;
+  return GASP_OK;
+}
+
+int check_device_of(int dev) {
+  int cur = -1;
+  GASP_CUDA(cudaGetDevice(&cur));
+  if (cur != dev) GASP_CUDA(cudaSetDevice(dev));
+  return GASP_OK;
+}
+
+int validate_L(int L, int device) {
+  if (L < 2) {
+    set_error("L must be >= 2 (got %d)", L);
+    return GASP_ERR_INVALID;
+  }
+  const int maxL = max_shared_L(device);
+  if (L > maxL) {
+    set_error("L=%d exceeds the shared-memory sweep limit %d on device %d", L, maxL, device);
+    return GASP_ERR_UNSUPPORTED;
+  }
+  return GASP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *gasp_status_string(int status) {
+  switch (status) {
+    case GASP_OK: return "ok";
+    case GASP_ERR_INVALID: return "invalid argument";
+    case GASP_ERR_CUDA: return "CUDA error";
+    case GASP_ERR_NO_DEVICE: return "no CUDA device";
+    case GASP_ERR_ALLOC: return "allocation failed";
+    case GASP_ERR_IO: return "I/O error";
+    case GASP_ERR_FORMAT: return "file format mismatch";
+    case GASP_ERR_CALLBACK: return "output callback failed";
+    case GASP_ERR_UNSUPPORTED: return "unsupported configuration";
+    case GASP_ERR_TIMEOUT: return "device wait timed out";
+    default: return "unknown status";
+  }
+}
+
+const char *gasp_last_error(void) { return g_err.c_str(); }
+const char *gasp_version(void) { return "gasp-b200 0.1 (sm_100a)"; }
+
+int gasp_set_stream(void *stream) {
+  g_stream = reinterpret_cast<cudaStream_t>(stream);
+  return GASP_OK;
+}
+
+int gasp_init_device(int device_index, int verbose, int *device_out, int *nsms_out) {
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0) {
+    if (verbose) fprintf(stdout, "No CUDA supported devices are available in this system.\n");
+    set_error("no CUDA device (%s)", cudaGetErrorString(e));
+    return GASP_ERR_NO_DEVICE;
+  }
+  if (verbose) {
+    // The reference's device summary (src/gpu_tools.cu:31-76).
+    fprintf(stdout, "Found %d CUDA devices in this system\n", count);
+    for (int d = 0; d < count; ++d) {
+      cudaDeviceProp prop;
+      GASP_CUDA(cudaGetDeviceProperties(&prop, d));
+      int optin = 0;
+      GASP_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, d));
+      fprintf(stdout, "Device %d : %s\n", d, prop.name);
+      fprintf(stdout, "================================\n");
+      fprintf(stdout, "Number of SMs       : %d\n", prop.multiProcessorCount);
+      fprintf(stdout, "Max SHMEM per block : %ld KB\n", (long)(prop.sharedMemPerBlock / 1024));
+      fprintf(stdout, "Max Opt in shared   : %d KB\n", optin / 1024);
+      fprintf(stdout, "Recommended ngrids  : %d\n", 4 * prop.warpSize * prop.multiProcessorCount);
+      fprintf(stdout, "\n");
+      fprintf(stdout, "Estimated largest L for shared memory code path : %d\n", max_shared_L(d));
+      fprintf(stdout, "(Assumes threadsPerBlock = 32)\n");
+      fprintf(stdout, "\n");
+    }
+  }
+  if (device_index != -1) {
+    if (device_index < 0 || device_index >= count) {
+      set_error("device index %d out of range (%d devices)", device_index, count);
+      return GASP_ERR_INVALID;
+    }
+    GASP_CUDA(cudaSetDevice(device_index));
+  }
+  int dev = 0;
+  GASP_CUDA(cudaGetDevice(&dev));
+  if (verbose) {
+    fprintf(stdout, "Using CUDA device : %d\n", dev);
+    fflush(stdout);
+  }
+  cudaDeviceProp prop;
+  GASP_CUDA(cudaGetDeviceProperties(&prop, dev));
+  if (device_out) *device_out = dev;
+  if (nsms_out) *nsms_out = prop.multiProcessorCount;
+  return GASP_OK;
+}
+
+int gasp_select_gpu_method(int L, int ngrids, int threads_per_block, int gpu_device,
+                           int *method_out) {
+  (void)ngrids;
+  if (!method_out || threads_per_block <= 0) {
+    set_error("invalid arguments to gasp_select_gpu_method");
+    return GASP_ERR_INVALID;
+  }
+  int dev = gpu_device;
+  if (dev < 0) GASP_CUDA(cudaGetDevice(&dev));
+  cudaDeviceProp prop;
+  GASP_CUDA(cudaGetDeviceProperties(&prop, dev));
+  // src/gpu_tools.cu:211-224, the same arithmetic.
+  const int max_shmem = (int)prop.sharedMemPerBlock;
+  const double value = (8.0 * max_shmem) / threads_per_block;
+  int maxL = (int)sqrt(value);
+  maxL = (int)sqrt(32 * (maxL * maxL / 32));
+  *method_out = (L <= maxL) ? 2 : 0;
+  return GASP_OK;
+}
+
+int gasp_acceptance_table(double beta, double h, float table_out[20]) {
+  if (!table_out) return GASP_ERR_INVALID;
+  host_probs_gpu(beta, h, table_out);
+  return GASP_OK;
+}
+
+int gasp_max_shared_L(int device, int *maxL_out) {
+  if (!maxL_out) return GASP_ERR_INVALID;
+  int dev = device;
+  if (dev < 0) GASP_CUDA(cudaGetDevice(&dev));
+  *maxL_out = max_shared_L(dev);
+  return GASP_OK;
+}
+
+size_t gasp_frame_bytes(int L, int ngrids) {
+  return (size_t)(((long long)L * L * ngrids + 7) / 8);
+}
+
+int gasp_init_grid(int L, int ngrids, int threads_per_block, const int *host_grids,
+                   gasp_grids_t **grids_out) {
+  (void)threads_per_block;
+  if (!grids_out || ngrids <= 0) {
+    set_error("gasp_init_grid: ngrids must be positive and grids_out non-NULL");
+    return GASP_ERR_INVALID;
+  }
+  *grids_out = nullptr;
+  int dev = 0;
+  GASP_CUDA(cudaGetDevice(&dev));
+  int rc = validate_L(L, dev);
+  if (rc) return rc;
+  GridsImpl *im = new (std::nothrow) GridsImpl();
+  if (!im) return GASP_ERR_ALLOC;
+  gasp_grids &g = im->pub;
+  g.device = dev;
+  g.L = L;
+  g.N = L * L;
+  g.W = words_per_replica(L);
+  g.ngrids = ngrids;
+  g.ntiles = tiles_for(ngrids);
+  g.frame_bytes = gasp_frame_bytes(L, ngrids);
+  const size_t words = (size_t)g.ntiles * g.W * kTile;
+  cudaError_t e = cudaMalloc(&g.d_lat, words * sizeof(uint32_t));
+  if (e == cudaSuccess) e = cudaMalloc(&g.d_mag, (size_t)g.ntiles * kTile * sizeof(float));
+  if (e == cudaSuccess) e = cudaMemsetAsync(g.d_lat, 0, words * sizeof(uint32_t), current_stream());
+  if (e != cudaSuccess) {
+    cudaFree(g.d_lat);
+    cudaFree(g.d_mag);
+    delete im;
+    return cuda_fail(e, "gasp_init_grid allocation", __FILE__, __LINE__);
+  }
+  *grids_out = &g;
+  if (host_grids) return gasp_grids_upload(&g, host_grids);
+  return GASP_OK;
+}
+
+int gasp_free_grid(gasp_grids_t *g) {
+  if (!g) return GASP_OK;
+  GridsImpl *im = impl(g);
+  cudaFree(g->d_lat);
+  cudaFree(g->d_mag);
+  cudaFree(g->d_frame);
+  cudaFree(g->d_scratch32);
+  cudaFree(im->x.d_tab);
+  cudaFree(im->x.d_stream);
+  cudaFree(im->x.d_mag2);
+  cudaFree(im->x.d_active);
+  delete im;
+  return GASP_OK;
+}
+
+static int ensure_scratch32(gasp_grids_t *g) {
+  if (!g->d_scratch32)
+    GASP_CUDA(cudaMalloc(&g->d_scratch32, (size_t)g->ngrids * g->N * sizeof(int)));
+  return GASP_OK;
+}
+
+int gasp_grids_upload(gasp_grids_t *g, const int *host_grids) {
+  if (!g || !host_grids) return GASP_ERR_INVALID;
+  int rc = check_device_of(g->device);
+  if (rc) return rc;
+  if ((rc = ensure_scratch32(g))) return rc;
+  cudaStream_t s = current_stream();
+  GASP_CUDA(cudaMemcpyAsync(g->d_scratch32, host_grids, (size_t)g->ngrids * g->N * sizeof(int),
+                            cudaMemcpyHostToDevice, s));
+  rc = launch_pack_grids(g->d_scratch32, g->d_lat, g->L, g->ngrids, s);
+  if (rc) return rc;
+  GASP_CUDA(cudaStreamSynchronize(s));
+  return GASP_OK;
+}
+
+int gasp_grids_download(gasp_grids_t *g, int *host_grids) {
+  if (!g || !host_grids) return GASP_ERR_INVALID;
+  int rc = check_device_of(g->device);
+  if (rc) return rc;
+  if ((rc = ensure_scratch32(g))) return rc;
+  cudaStream_t s = current_stream();
+  rc = launch_unpack_grids(g->d_lat, g->d_scratch32, g->L, g->ngrids, s);
+  if (rc) return rc;
+  GASP_CUDA(cudaMemcpyAsync(host_grids, g->d_scratch32, (size_t)g->ngrids * g->N * sizeof(int),
+                            cudaMemcpyDeviceToHost, s));
+  GASP_CUDA(cudaStreamSynchronize(s));
+  return GASP_OK;
+}
+
+int gasp_grids_shape(const gasp_grids_t *g, int *L_out, int *ngrids_out) {
+  if (!g) return GASP_ERR_INVALID;
+  if (L_out) *L_out = g->L;
+  if (ngrids_out) *ngrids_out = g->ngrids;
+  return GASP_OK;
+}
+
+int gasp_init_rand(int ngrids, int threads_per_block, unsigned long long seed,
+                   gasp_rng_t **rng_out) {
+  (void)threads_per_block;
+  if (!rng_out || ngrids <= 0) {
+    set_error("gasp_init_rand: ngrids must be positive and rng_out non-NULL");
+    return GASP_ERR_INVALID;
+  }
+  *rng_out = nullptr;
+  gasp_rng *r = new (std::nothrow) gasp_rng();
+  if (!r) return GASP_ERR_ALLOC;
+  cudaError_t e = cudaGetDevice(&r->device);
+  r->ngrids = ngrids;
+  r->stride = tiles_for(ngrids) * kTile;
+  if (e == cudaSuccess)
+    e = cudaMalloc(&r->d_state, (size_t)kRngWords * r->stride * sizeof(uint32_t));
+  if (e != cudaSuccess) {
+    delete r;
+    return cuda_fail(e, "gasp_init_rand allocation", __FILE__, __LINE__);
+  }
+  cudaStream_t s = current_stream();
+  int rc = launch_rng_init(r->d_state, ngrids, r->stride, seed, s);
+  if (rc == GASP_OK) {
+    e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) rc = cuda_fail(e, "gasp_init_rand", __FILE__, __LINE__);
+  }
+  if (rc) {
+    cudaFree(r->d_state);
+    delete r;
+    return rc;
+  }
+  *rng_out = r;
+  return GASP_OK;
+}
+
+int gasp_free_rand(gasp_rng_t *r) {
+  if (!r) return GASP_OK;
+  cudaFree(r->d_state);
+  delete r;
+  return GASP_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+SweepLaunch base_launch(gasp_grids_t *g) {
+  SweepLaunch p;
+  memset(&p, 0, sizeof p);
+  GridsExtra &x = impl(g)->x;
+  p.lat = g->d_lat;
+  p.L = g->L;
+  p.ngrids = g->ngrids;
+  p.n_active = g->ngrids;
+  p.thr = x.d_tab->thr;
+  p.pacc_f = x.d_tab->pacc;
+  p.pacc_cpu = x.d_tab->pacc_cpu;
+  p.float_compare = x.float_cmp;
+  return p;
+}
+
+int check_sweep_args(gasp_grids_t *g, gasp_rng_t *r, int nsweeps, int method) {
+  if (!g || !r) {
+    set_error("NULL grid set or RNG");
+    return GASP_ERR_INVALID;
+  }
+  if (r->ngrids < g->ngrids) {
+    set_error("RNG has %d states for %d grids", r->ngrids, g->ngrids);
+    return GASP_ERR_INVALID;
+  }
+  if (nsweeps < 0) {
+    set_error("nsweeps must be >= 0");
+    return GASP_ERR_INVALID;
+  }
+  if (method < 0 || method > 2) {
+    set_error("gpu_method must be 0, 1 or 2 (got %d)", method);
+    return GASP_ERR_INVALID;
+  }
+  return check_device_of(g->device);
+}
+
+}  // namespace
+
+extern "C" {
+
+int gasp_sweep(gasp_grids_t *g, gasp_rng_t *r, double beta, double h, int nsweeps, int gpu_method) {
+  int rc = check_sweep_args(g, r, nsweeps, gpu_method);
+  if (rc) return rc;
+  if ((rc = ensure_tables(g, beta, h))) return rc;
+  if (nsweeps == 0) return GASP_OK;
+  SweepLaunch p = base_launch(g);
+  p.rng = r->d_state;
+  p.rng_stride = r->stride;
+  p.nsweeps = nsweeps;
+  p.mag_out = g->d_mag;
+  return launch_sweep_exact(p, current_stream());
+}
+
+int gasp_sweep_trace_cpu(gasp_grids_t *g, const double *stream, double beta, double h,
+                         int nsweeps) {
+  if (!g || !stream || nsweeps < 0) return GASP_ERR_INVALID;
+  int rc = check_device_of(g->device);
+  if (rc) return rc;
+  if ((rc = ensure_tables(g, beta, h))) return rc;
+  if (nsweeps == 0) return GASP_OK;
+  GridsExtra &x = impl(g)->x;
+  const size_t n = (size_t)g->ngrids * 3 * (size_t)g->N * nsweeps;
+  cudaPointerAttributes attr;
+  const double *dptr = stream;
+  cudaStream_t s = current_stream();
+  if (cudaPointerGetAttributes(&attr, stream) != cudaSuccess || attr.type != cudaMemoryTypeDevice) {
+    cudaGetLastError();
+    if (x.stream_cap < n) {
+      cudaFree(x.d_stream);
+      x.d_stream = nullptr;
+      x.stream_cap = 0;
+      GASP_CUDA(cudaMalloc(&x.d_stream, n * sizeof(double)));
+      x.stream_cap = n;
+    }
+    GASP_CUDA(cudaMemcpyAsync(x.d_stream, stream, n * sizeof(double), cudaMemcpyHostToDevice, s));
+    dptr = x.d_stream;
+  }
+  SweepLaunch p = base_launch(g);
+  p.stream = dptr;
+  p.nsweeps = nsweeps;
+  p.mag_out = g->d_mag;
+  rc = launch_sweep_trace_cpu(p, s);
+  if (rc) return rc;
+  GASP_CUDA(cudaStreamSynchronize(s));
+  return GASP_OK;
+}
+
+int gasp_magnetisation(gasp_grids_t *g, float *host_mag) {
+  if (!g || !host_mag) return GASP_ERR_INVALID;
+  int rc = check_device_of(g->device);
+  if (rc) return rc;
+  cudaStream_t s = current_stream();
+  rc = launch_measure(g->d_lat, g->L, g->ngrids, g->d_mag, s);
+  if (rc) return rc;
+  GASP_CUDA(cudaMemcpyAsync(host_mag, g->d_mag, (size_t)g->ngrids * sizeof(float),
+                            cudaMemcpyDeviceToHost, s));
+  GASP_CUDA(cudaStreamSynchronize(s));
+  return GASP_OK;
+}
+
+static int ensure_frame(gasp_grids_t *g) {
+  if (!g->d_frame) GASP_CUDA(cudaMalloc(&g->d_frame, (g->frame_bytes + 15) & ~(size_t)15));
+  return GASP_OK;
+}
+
+int gasp_pack_frame(gasp_grids_t *g, uint8_t *host_out) {
+  if (!g || !host_out) return GASP_ERR_INVALID;
+  int rc = check_device_of(g->device);
+  if (rc) return rc;
+  if ((rc = ensure_frame(g))) return rc;
+  cudaStream_t s = current_stream();
+  rc = launch_pack_frame(g->d_lat, g->d_frame, g->L, g->ngrids, s);
+  if (rc) return rc;
+  GASP_CUDA(cudaMemcpyAsync(host_out, g->d_frame, g->frame_bytes, cudaMemcpyDeviceToHost, s));
+  GASP_CUDA(cudaStreamSynchronize(s));
+  return GASP_OK;
+}
+
+}  // extern "C"
+
+// ===========================================================================
+// Driver
+// ===========================================================================
+namespace {
+
+struct PinnedBuf {
+  void *p = nullptr;
+  ~PinnedBuf() {
+    if (p) cudaFreeHost(p);
+  }
+};
+
+void expand_frame(const uint8_t *payload, int *grids, long long nbits) {
+  for (long long i = 0; i < nbits; ++i) grids[i] = ((payload[i >> 3] >> (i & 7)) & 1) ? 1 : -1;
+}
+
+}  // namespace
+
+extern "C" int gasp_mc_driver_gpu_ex(gasp_gpu_grids_t grids, double beta, double h, int *grid_fate,
+                                     gasp_sampler_t samples, gasp_function_t calc,
+                                     gasp_gpu_run_t gpu_state, gasp_grid_output_fn outfunc,
+                                     const gasp_driver_opts_t *opts) {
+  gasp_driver_opts_t o;
+  memset(&o, 0, sizeof o);
+  if (opts) o = *opts;
+  gasp_grids_t *g = grids.d_grids;
+  gasp_rng_t *r = gpu_state.d_state;
+  const int tot = samples.tot_nsweeps, mag_int = samples.mag_output_int,
+            grid_int = samples.grid_output_int;
+  if (!g || !r) {
+    set_error("driver: device grid set and RNG states are required");
+    return GASP_ERR_INVALID;
+  }
+  if (grids.L != g->L || grids.ngrids != g->ngrids) {
+    set_error("driver: grids.L/ngrids (%d, %d) do not match the device set (%d, %d)", grids.L,
+              grids.ngrids, g->L, g->ngrids);
+    return GASP_ERR_INVALID;
+  }
+  if (mag_int <= 0 || grid_int <= 0 || tot < 0) {
+    set_error("driver: output intervals must be positive and tot_nsweeps >= 0");
+    return GASP_ERR_INVALID;
+  }
+  if (calc.itask != 0 && calc.itask != 1) {
+    set_error("Error: itask must be 0 or 1!");
+    return GASP_ERR_INVALID;
+  }
+  const int ninputs = calc.ninputs > 0 ? calc.ninputs : 1;
+  if (g->ngrids % ninputs != 0) {
+    set_error("Error: ngrids must be divisible by ninputs!");
+    return GASP_ERR_INVALID;
+  }
+  if (calc.cv && strcmp(calc.cv, "magnetisation") != 0) {
+    set_error("driver: only cv='magnetisation' is provided (got '%s')", calc.cv);
+    return GASP_ERR_UNSUPPORTED;
+  }
+  if (calc.itask == 1 && !grid_fate) {
+    set_error("driver: itask 1 needs a grid_fate array");
+    return GASP_ERR_INVALID;
+  }
+  if (outfunc && !grids.ising_grids) {
+    set_error("driver: outfunc needs the host grids array (grids.ising_grids)");
+    return GASP_ERR_INVALID;
+  }
+  int rc = check_sweep_args(g, r, 0, gpu_state.gpu_method < 0 ? 0 : gpu_state.gpu_method % 3);
+  if (rc) return rc;
+  if ((rc = ensure_tables(g, beta, h))) return rc;
+
+  GridsExtra &x = impl(g)->x;
+  const int ngrids = g->ngrids, N = g->N, L = g->L;
+  const int itask = calc.itask;
+  const double up = calc.up_thr, dn = calc.dn_thr;
+  const int spc = mag_int < grid_int ? mag_int : grid_int;
+  const int nres = itask == 0 ? tot / mag_int : ninputs;
+  std::vector<float> result((size_t)nres, itask == 0 ? 1.0f : 0.0f);
+  const bool dumps = outfunc != nullptr || o.packed_out != nullptr;
+  const bool compact = o.compact && itask == 1;
+  char *cv = const_cast<char *>(calc.cv ? calc.cv : "magnetisation");
+  char *fname = const_cast<char *>(calc.filename ? calc.filename : "gridstates.bin");
+
+  cudaStream_t s = current_stream();
+  if (!x.d_mag2) GASP_CUDA(cudaMalloc(&x.d_mag2, (size_t)g->ntiles * kTile * sizeof(float)));
+  if (compact && !x.d_active) GASP_CUDA(cudaMalloc(&x.d_active, (size_t)ngrids * sizeof(int)));
+  if (dumps && (rc = ensure_frame(g))) return rc;
+  PinnedBuf hmag_b, hframe_b, hact_b;
+  GASP_CUDA(cudaMallocHost(&hmag_b.p, (size_t)ngrids * sizeof(float)));
+  float *hmag = static_cast<float *>(hmag_b.p);
+  std::vector<float> mag_last((size_t)ngrids, 0.0f);
+  if (dumps) GASP_CUDA(cudaMallocHost(&hframe_b.p, g->frame_bytes));
+  if (compact) GASP_CUDA(cudaMallocHost(&hact_b.p, (size_t)ngrids * sizeof(int)));
+  uint8_t *hframe = static_cast<uint8_t *>(hframe_b.p);
+  int *hact = static_cast<int *>(hact_b.p);
+
+  float *d_mag_cur = g->d_mag, *d_mag_next = x.d_mag2;
+  SweepLaunch p = base_launch(g);
+  p.rng = r->d_state;
+  p.rng_stride = r->stride;
+  p.nsweeps = spc;
+
+  long long attempts = 0;
+  int n_active = ngrids;
+  const auto t0 = std::chrono::steady_clock::now();
+  if ((rc = launch_measure(g->d_lat, L, ngrids, d_mag_cur, s))) return rc;
+
+  int isweep = 0;
+  bool have_frame = false;
+  while (isweep < tot) {
+    const bool dump_now = dumps && (isweep % grid_int == 0);
+    const bool mag_now = isweep % mag_int == 0;
+    if (dump_now) {
+      if ((rc = launch_pack_frame(g->d_lat, g->d_frame, L, ngrids, s))) return rc;
+      GASP_CUDA(cudaMemcpyAsync(hframe, g->d_frame, g->frame_bytes, cudaMemcpyDeviceToHost, s));
+    }
+    if (mag_now)
+      GASP_CUDA(cudaMemcpyAsync(hmag, d_mag_cur, (size_t)ngrids * sizeof(float),
+                                cudaMemcpyDeviceToHost, s));
+    bool fates_done = false;
+    int nA = 0, nB = 0;
+    if (compact && mag_now) {
+      // Fates at this check decide which replicas the next batch simulates.
+      GASP_CUDA(cudaStreamSynchronize(s));
+      memcpy(mag_last.data(), hmag, (size_t)ngrids * sizeof(float));
+      n_active = 0;
+      for (int i = 0; i < ngrids; ++i) {
+        if (grid_fate[i] == -1) {
+          const double m = (double)mag_last[i];
+          if (m > up) grid_fate[i] = 1;
+          else if (m < dn) grid_fate[i] = 0;
+        }
+        if (grid_fate[i] == 0) nA++;
+        else if (grid_fate[i] == 1) nB++;
+        else hact[n_active++] = i;
+      }
+      fates_done = true;
+      if (n_active > 0)
+        GASP_CUDA(cudaMemcpyAsync(x.d_active, hact, (size_t)n_active * sizeof(int),
+                                  cudaMemcpyHostToDevice, s));
+    }
+    // The batch isweep -> isweep+spc; its epilogue measures the state the
+    // next check will read.
+    const int next = isweep + spc;
+    const bool mag_next = next % mag_int == 0;
+    if (n_active > 0) {
+      p.active = compact ? x.d_active : nullptr;
+      p.n_active = n_active;
+      p.mag_out = mag_next ? d_mag_next : nullptr;
+      if (compact && mag_next) {
+        // Resolved replicas are not swept; keep their last magnetisation.
+        GASP_CUDA(cudaMemcpyAsync(d_mag_next, d_mag_cur, (size_t)ngrids * sizeof(float),
+                                  cudaMemcpyDeviceToDevice, s));
+      }
+      if ((rc = launch_sweep_exact(p, s))) return rc;
+      attempts += (long long)n_active * N * spc;
+    }
+    if (dump_now || (dumps && isweep == tot - 1)) {
+      GASP_CUDA(cudaStreamSynchronize(s));
+      if (dump_now) {
+        have_frame = true;
+        if (outfunc) expand_frame(hframe, grids.ising_grids, (long long)N * ngrids);
+      }
+      if (mag_now && !fates_done) memcpy(mag_last.data(), hmag, (size_t)ngrids * sizeof(float));
+      if (have_frame) {
+        if (outfunc && outfunc(L, ngrids, grids.ising_grids, isweep, mag_last.data(), nullptr, cv,
+                               dn, up, fname) != 0) {
+          cudaStreamSynchronize(s);
+          set_error("output callback returned non-zero at isweep %d", isweep);
+          return GASP_ERR_CALLBACK;
+        }
+        if (o.packed_out && o.packed_out(L, ngrids, hframe, g->frame_bytes, isweep,
+                                         mag_last.data(), o.packed_user) != 0) {
+          cudaStreamSynchronize(s);
+          set_error("packed output callback returned non-zero at isweep %d", isweep);
+          return GASP_ERR_CALLBACK;
+        }
+      }
+    }
+    bool stop = false;
+    if (mag_now || isweep == tot - 1) {
+      if (mag_now && !fates_done) {
+        GASP_CUDA(cudaStreamSynchronize(s));
+        memcpy(mag_last.data(), hmag, (size_t)ngrids * sizeof(float));
+      }
+      if (itask == 0) {
+        int nnuc = 0;
+        for (int i = 0; i < ngrids; ++i) nnuc += ((double)mag_last[i] > up) ? 1 : 0;
+        const int idx = isweep / mag_int;
+        if (idx < nres) result[idx] = (float)((double)nnuc / (double)ngrids);
+        if (o.verbosity >= 1) {
+          fprintf(stdout, "%10d  %12.6f\n", isweep, (double)nnuc / (double)ngrids);
+          fflush(stdout);
+        }
+        stop = nnuc == ngrids;
+      } else {
+        if (!fates_done) {
+          nA = nB = 0;
+          for (int i = 0; i < ngrids; ++i) {
+            if (grid_fate[i] == 0) {
+              nA++;
+            } else if (grid_fate[i] == 1) {
+              nB++;
+            } else {
+              const double m = (double)mag_last[i];
+              if (m > up) { grid_fate[i] = 1; nB++; }
+              else if (m < dn) { grid_fate[i] = 0; nA++; }
+            }
+          }
+        }
+        if (o.verbosity >= 1) {
+          fprintf(stdout,
+                  "\r Sweep : %10d, Reached cv = %6.2f : %4d , Reached cv = %6.2f : %4d , "
+                  "Unresolved : %4d",
+                  isweep, dn, nA, up, nB, ngrids - nA - nB);
+          fflush(stdout);
+        }
+        stop = nA + nB == ngrids;
+      }
+    }
+    if (mag_next) {
+      float *t = d_mag_cur;
+      d_mag_cur = d_mag_next;
+      d_mag_next = t;
+    }
+    if (stop) break;
+    isweep = next;
+  }
+  GASP_CUDA(cudaStreamSynchronize(s));
+  // Keep the set's magnetisation buffer pointing at the freshest values.
+  if (d_mag_cur != g->d_mag) {
+    x.d_mag2 = g->d_mag;
+    g->d_mag = d_mag_cur;
+  }
+  const double elapsed =
+      std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  if (itask == 1) {
+    const int sub = ngrids / ninputs;
+    for (int i = 0; i < ninputs; ++i) {
+      int nBb = 0, nF = 0;
+      for (int j = 0; j < sub; ++j) {
+        const int f = grid_fate[i * sub + j];
+        if (f > -1) nBb += f;
+        else nF += 1;
+      }
+      result[i] = (float)nBb / (float)(sub - nF);
+    }
+  }
+  if (o.verbosity >= 1) {
+    fprintf(stdout, "\n# Time taken on GPU = %f seconds\n", elapsed);
+    if (itask == 1) fprintf(stdout, "pB estimate : %10.6f\n", nres > 0 ? (double)result[0] : 0.0);
+    fflush(stdout);
+  }
+  if (calc.result)
+    for (int i = 0; i < nres; ++i) calc.result[i] = result[i];
+  if (o.elapsed_s) *o.elapsed_s = elapsed;
+  if (o.attempts) *o.attempts = attempts;
+  return GASP_OK;
+}
+
+extern "C" int gasp_mc_driver_gpu(gasp_gpu_grids_t grids, double beta, double h, int *grid_fate,
+                                  gasp_sampler_t samples, gasp_function_t calc,
+                                  gasp_gpu_run_t gpu_state, gasp_grid_output_fn outfunc) {
+  return gasp_mc_driver_gpu_ex(grids, beta, h, grid_fate, samples, calc, gpu_state, outfunc,
+                               nullptr);
+}

@@ -1,0 +1,96 @@
+// gasp_internal.h -- shared host-side declarations of the gasp-b200 library.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "gasp.h"
+
+namespace gasp {
+
+// Lattice storage ("lane-interleaved bit planes").  Replicas are grouped in
+// tiles of 32 (one warp, one replica per lane).  A replica's L*L spins are
+// bit-packed row-major into W = ceil(L*L/32) words (site s -> word s>>5,
+// bit s&31, bit 1 == spin +1).  Within a tile, word w of lane l sits at
+// index w*32 + l, so a warp that reads "its own word w" touches 32
+// consecutive words: one coalesced 128 B line in HBM and 32 distinct banks in
+// shared memory whatever site each lane picked.
+constexpr int kTile = 32;
+
+inline int words_per_replica(int L) { return (L * L + 31) / 32; }
+inline int tiles_for(int ngrids) { return (ngrids + kTile - 1) / kTile; }
+
+// Per-replica XORWOW state in structure-of-arrays form: component k of
+// replica r at state[k * stride + r], k = 0 (d), 1..5 (v[0..4]).
+constexpr int kRngWords = 6;
+
+void set_error(const char *fmt, ...);
+int cuda_fail(cudaError_t e, const char *what, const char *file, int line);
+
+#define GASP_CUDA(call)                                                             \
+  do {                                                                              \
+    cudaError_t e_ = (call);                                                        \
+    if (e_ != cudaSuccess) return ::gasp::cuda_fail(e_, #call, __FILE__, __LINE__); \
+  } while (0)
+
+cudaStream_t current_stream();
+
+// Thresholds for the integer acceptance test: replica accepts iff its raw
+// 32-bit XORWOW draw x <= thr[class], class = 5*spin01 + (# up neighbours).
+// Built on the device from the float table so the comparison is exactly
+// "_curand_uniform(x) < P" (see k_build_thresholds).
+struct AcceptTable {
+  float pacc[20];        // reference float table (src/mc_gpu.cu:21-37)
+  double pacc_cpu[20];   // reference double table (src/mc_cpu.c:14-38)
+};
+
+struct SweepLaunch {
+  uint32_t *lat;          // home lattice words [ntiles][W][32]
+  uint32_t *rng;          // SoA XORWOW states
+  int rng_stride;         // component stride of rng (>= ngrids)
+  const int *active;      // optional replica id list (nullptr: identity)
+  int n_active;           // replicas to sweep (slots)
+  int L;
+  int nsweeps;
+  int ngrids;             // replicas in the set
+  const uint32_t *thr;    // 10 device thresholds (exact mode)
+  const float *pacc_f;    // 20 floats (exact mode, float comparison)
+  const double *stream;   // trace mode: per-replica double stream
+  const double *pacc_cpu; // trace mode: 20 doubles (device)
+  float *mag_out;         // optional: magnetisation after the batch [ngrids]
+  int float_compare;      // exact mode: compare in float (thresholds unusable)
+  int warps_per_cta;      // launch shape (0: default)
+};
+
+// kernel launchers (gasp_kernels.cu); each returns a GASP status.
+int launch_rng_init(uint32_t *rng, int ngrids, int stride, unsigned long long seed, cudaStream_t s);
+int launch_build_thresholds(const float *d_pacc20, uint32_t *d_thr10, int *d_flags, cudaStream_t s);
+int launch_sweep_exact(const SweepLaunch &p, cudaStream_t s);
+int launch_sweep_trace_cpu(const SweepLaunch &p, cudaStream_t s);
+int launch_measure(const uint32_t *lat, int L, int ngrids, float *mag, cudaStream_t s);
+int launch_pack_grids(const int *grids32, uint32_t *lat, int L, int ngrids, cudaStream_t s);
+int launch_unpack_grids(const uint32_t *lat, int *grids32, int L, int ngrids, cudaStream_t s);
+int launch_pack_frame(const uint32_t *lat, uint8_t *frame, int L, int ngrids, cudaStream_t s);
+int max_shared_L(int device);
+
+}  // namespace gasp
+
+// Opaque handle definitions.
+struct gasp_grids {
+  int device;
+  int L, N, W;
+  int ngrids, ntiles;
+  uint32_t *d_lat;       // ntiles * W * 32 words
+  float *d_mag;          // ngrids
+  uint8_t *d_frame;      // frame payload buffer (lazily allocated)
+  size_t frame_bytes;
+  int *d_scratch32;      // int32 staging (lazily allocated), ngrids*N
+};
+
+struct gasp_rng {
+  int device;
+  int ngrids, stride;
+  uint32_t *d_state;     // kRngWords * stride
+};

@@ -1,0 +1,404 @@
+// gasp_kernels.cu -- sm_100a device code of gasp-b200.
+//
+// Hot kernel: k_sweep_exact, the reference-exact random-site Metropolis sweep
+// (reproduces mc_sweep_gpu / _bitrep / _bitmap32, src/mc_gpu.cu:88-356).
+// Design (B200 first, not a translation):
+//   * one warp = one tile of 32 replicas, one replica per lane;
+//   * each replica's lattice is a private bitmap in shared memory, stored
+//     lane-interleaved (word w of lane l at w*32+l): every shared load or
+//     store a warp issues hits 32 distinct banks, whatever sites the lanes
+//     drew, so the random-site gathers of the reference (3-4 way bank
+//     conflicts plus an atomicXor per flip) become single-wavefront accesses
+//     and a flip is a plain store to a word only its lane owns;
+//   * the XORWOW state lives in registers for the whole batch and is drawn
+//     with the cuRAND device API (curand / _curand_uniform), so the stream is
+//     the reference's own;
+//   * the acceptance test u2 < P is replaced by an exactly equivalent integer
+//     test x2 <= thr[class] on the raw draw; thresholds are found on the
+//     device by bisection over the same _curand_uniform, which is monotone;
+//   * the magnetisation of the batch's final state is a popcount of the
+//     lane's own words, fused into the epilogue.
+#include <cfloat>
+#include <cstdio>
+
+#include <curand_kernel.h>
+
+#include "gasp_internal.h"
+
+namespace gasp {
+namespace {
+
+constexpr int kHeaderWords = 64;  // per-CTA shared header: tables (256 B)
+
+__device__ __forceinline__ void load_rng(curandStateXORWOW &st, const uint32_t *rng,
+                                         int stride, int rep) {
+  st.d = rng[rep];
+#pragma unroll
+  for (int k = 0; k < 5; ++k) st.v[k] = rng[(k + 1) * stride + rep];
+  st.boxmuller_flag = 0;
+  st.boxmuller_flag_double = 0;
+  st.boxmuller_extra = 0.f;
+  st.boxmuller_extra_double = 0.0;
+}
+
+__device__ __forceinline__ void store_rng(const curandStateXORWOW &st, uint32_t *rng,
+                                          int stride, int rep) {
+  rng[rep] = st.d;
+#pragma unroll
+  for (int k = 0; k < 5; ++k) rng[(k + 1) * stride + rep] = st.v[k];
+}
+
+// Shared-memory staging of one tile (identity order) or of 32 listed replicas.
+__device__ __forceinline__ void stage_in(uint32_t *lat_s, const SweepLaunch &p, int W,
+                                         int tile, int lane, bool live, int rep) {
+  if (p.active == nullptr) {
+    const uint32_t *src = p.lat + (size_t)tile * W * kTile + lane;
+    for (int w = 0; w < W; ++w) lat_s[w * kTile + lane] = src[(size_t)w * kTile];
+  } else {
+    const uint32_t *src = p.lat + (size_t)(rep >> 5) * W * kTile + (rep & 31);
+    for (int w = 0; w < W; ++w) lat_s[w * kTile + lane] = live ? src[(size_t)w * kTile] : 0u;
+  }
+}
+
+__device__ __forceinline__ void stage_out(const uint32_t *lat_s, const SweepLaunch &p, int W,
+                                          int tile, int lane, bool live, int rep) {
+  if (p.active == nullptr) {
+    uint32_t *dst = p.lat + (size_t)tile * W * kTile + lane;
+    for (int w = 0; w < W; ++w) dst[(size_t)w * kTile] = lat_s[w * kTile + lane];
+  } else if (live) {
+    uint32_t *dst = p.lat + (size_t)(rep >> 5) * W * kTile + (rep & 31);
+    for (int w = 0; w < W; ++w) dst[(size_t)w * kTile] = lat_s[w * kTile + lane];
+  }
+}
+
+__device__ __forceinline__ uint32_t bit_at(const uint32_t *my, int s) {
+  return (my[(s >> 5) * kTile] >> (s & 31)) & 1u;
+}
+
+__device__ __forceinline__ void epilogue_mag(const uint32_t *my, const SweepLaunch &p, int N,
+                                             int W, bool live, int rep) {
+  if (p.mag_out != nullptr && live) {
+    int pc = 0;
+    for (int w = 0; w < W; ++w) pc += __popc(my[w * kTile]);
+    // (float)(sum of +-1 spins) / (float)N, the sum being exact in float.
+    p.mag_out[rep] = (float)(2 * pc - N) / (float)N;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Exact sweep.  L_ > 0: compile-time side length; L_ == 0: runtime p.L.
+// ---------------------------------------------------------------------------
+template <int L_, bool kFloatCmp>
+__global__ void __launch_bounds__(256) k_sweep_exact(SweepLaunch p) {
+  const int L = L_ > 0 ? L_ : p.L;
+  const int N = L * L;
+  const int W = (N + 31) >> 5;
+  extern __shared__ __align__(16) uint32_t smem[];
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int nwarps = blockDim.x >> 5;
+
+  uint32_t *thr_s = smem;                                  // [10]
+  float *pacc_s = reinterpret_cast<float *>(smem + 16);    // [20]
+  if (threadIdx.x < 10) thr_s[threadIdx.x] = p.thr[threadIdx.x];
+  if (threadIdx.x < 20) pacc_s[threadIdx.x] = p.pacc_f[threadIdx.x];
+
+  const int tile = blockIdx.x * nwarps + warp;
+  const int slot = tile * kTile + lane;
+  const bool tile_live = tile * kTile < p.n_active;
+  const bool live = slot < p.n_active;
+  const int rep = live ? (p.active ? p.active[slot] : slot) : 0;
+  uint32_t *lat_s = smem + kHeaderWords + warp * (W * kTile);
+  if (tile_live) stage_in(lat_s, p, W, tile, lane, live, rep);
+  __syncthreads();
+  if (!tile_live) return;
+
+  uint32_t *my = lat_s + lane;
+  if (live) {
+    curandStateXORWOW st;
+    load_rng(st, p.rng, p.rng_stride, rep);
+    const float shrink = (1.0f - FLT_EPSILON) * (float)N;
+    for (int sw = 0; sw < p.nsweeps; ++sw) {
+      for (int a = 0; a < N; ++a) {
+        const uint32_t x1 = curand(&st);
+        const int s = __float2int_rd(shrink * _curand_uniform(x1));
+        const int row = s / L;
+        const int col = s - row * L;
+        const int su = row == 0 ? s + N - L : s - L;
+        const int sd = row == L - 1 ? s - N + L : s + L;
+        const int sl = col == 0 ? s + L - 1 : s - 1;
+        const int sr = col == L - 1 ? s - L + 1 : s + 1;
+        const uint32_t wc = my[(s >> 5) * kTile];
+        const uint32_t bs = (wc >> (s & 31)) & 1u;
+        const uint32_t k = bit_at(my, su) + bit_at(my, sd) + bit_at(my, sl) + bit_at(my, sr);
+        const uint32_t cls = 5u * bs + k;
+        const uint32_t x2 = curand(&st);
+        bool acc;
+        if (kFloatCmp) {
+          acc = _curand_uniform(x2) < pacc_s[2 * cls];  // index 10*bs + 2k
+        } else {
+          acc = x2 <= thr_s[cls];
+        }
+        if (acc) my[(s >> 5) * kTile] = wc ^ (1u << (s & 31));
+      }
+    }
+    store_rng(st, p.rng, p.rng_stride, rep);
+  }
+  __syncwarp();
+  epilogue_mag(my, p, N, W, live, rep);
+  stage_out(lat_s, p, W, tile, lane, live, rep);
+}
+
+// ---------------------------------------------------------------------------
+// CPU-trace sweep: mc_sweep_cpu arithmetic (src/mc_cpu.c:41-89) on a replayed
+// stream of doubles (row-u, col-u, xi) per attempt.
+// ---------------------------------------------------------------------------
+template <int L_>
+__global__ void __launch_bounds__(256) k_sweep_trace_cpu(SweepLaunch p) {
+  const int L = L_ > 0 ? L_ : p.L;
+  const int N = L * L;
+  const int W = (N + 31) >> 5;
+  extern __shared__ __align__(16) uint32_t smem[];
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int nwarps = blockDim.x >> 5;
+  double *pacc_s = reinterpret_cast<double *>(smem);  // [20] (160 B < header)
+  if (threadIdx.x < 20) pacc_s[threadIdx.x] = p.pacc_cpu[threadIdx.x];
+  const int tile = blockIdx.x * nwarps + warp;
+  const int slot = tile * kTile + lane;
+  const bool tile_live = tile * kTile < p.n_active;
+  const bool live = slot < p.n_active;
+  const int rep = live ? (p.active ? p.active[slot] : slot) : 0;
+  uint32_t *lat_s = smem + kHeaderWords + warp * (W * kTile);
+  if (tile_live) stage_in(lat_s, p, W, tile, lane, live, rep);
+  __syncthreads();
+  if (!tile_live) return;
+  uint32_t *my = lat_s + lane;
+  if (live) {
+    const double *str = p.stream + (size_t)rep * 3 * (size_t)N * p.nsweeps;
+    const long long total = (long long)N * p.nsweeps;
+    for (long long a = 0; a < total; ++a) {
+      const double ur = str[3 * a + 0], uc = str[3 * a + 1], xi = str[3 * a + 2];
+      const int row = (int)floor(L * ur);
+      const int col = (int)floor(L * uc);
+      const int s = L * row + col;
+      const int su = L * ((row + L - 1) % L) + col;
+      const int sd = L * ((row + 1) % L) + col;
+      const int sr = L * row + (col + 1) % L;
+      const int sl = L * row + (col + L - 1) % L;
+      const uint32_t wc = my[(s >> 5) * kTile];
+      const uint32_t bs = (wc >> (s & 31)) & 1u;
+      const uint32_t k = bit_at(my, su) + bit_at(my, sd) + bit_at(my, sl) + bit_at(my, sr);
+      // reference index 5*(spin+1) + nsum + 4 == 10*bs + 2*k
+      if (xi < pacc_s[10 * bs + 2 * k]) my[(s >> 5) * kTile] = wc ^ (1u << (s & 31));
+    }
+  }
+  __syncwarp();
+  epilogue_mag(my, p, N, W, live, rep);
+  stage_out(lat_s, p, W, tile, lane, live, rep);
+}
+
+// ---------------------------------------------------------------------------
+__global__ void k_rng_init(uint32_t *rng, int ngrids, int stride, unsigned long long seed) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= ngrids) return;
+  curandStateXORWOW st;
+  curand_init(seed, (unsigned long long)r, 0ull, &st);  // as src/gpu_tools.cu:130-133
+  store_rng(st, rng, stride, r);
+}
+
+// thr[c] = T-1 with T = min{x in [0,2^32] : !(_curand_uniform(x) < P[2c])}.
+// _curand_uniform is monotone non-decreasing in x (a rounded conversion then a
+// fused multiply-add by a positive constant), so "x <= thr[c]" is exactly
+// "_curand_uniform(x) < P[2c]" for every 32-bit x.  flags[0] is set when some
+// class can never accept (T == 0); the host then uses the float comparison.
+__global__ void k_build_thresholds(const float *pacc20, uint32_t *thr10, int *flags) {
+  const int c = threadIdx.x;
+  if (c >= 10) return;
+  const float P = pacc20[2 * c];
+  unsigned long long lo = 0ull, hi = 1ull << 32;
+  while (lo < hi) {
+    const unsigned long long mid = (lo + hi) >> 1;
+    if (_curand_uniform((unsigned int)mid) < P) lo = mid + 1;
+    else hi = mid;
+  }
+  if (lo == 0ull) atomicExch(flags, 1);
+  thr10[c] = (uint32_t)(lo - 1ull);
+}
+
+__global__ void k_measure(const uint32_t *lat, int L, int ngrids, float *mag) {
+  const int rep = blockIdx.x * blockDim.x + threadIdx.x;
+  if (rep >= ngrids) return;
+  const int N = L * L, W = (N + 31) >> 5;
+  const uint32_t *src = lat + (size_t)(rep >> 5) * W * kTile + (rep & 31);
+  int pc = 0;
+  for (int w = 0; w < W; ++w) pc += __popc(src[(size_t)w * kTile]);
+  mag[rep] = (float)(2 * pc - N) / (float)N;
+}
+
+// int32 grids [ngrids][N] -> lattice words; one thread per (tile, w, lane).
+__global__ void k_pack_grids(const int *g, uint32_t *lat, int L, int ngrids, long long total) {
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= total) return;
+  const int N = L * L, W = (N + 31) >> 5;
+  const int lane = (int)(idx & 31);
+  const long long tw = idx >> 5;
+  const int w = (int)(tw % W);
+  const long long tile = tw / W;
+  const long long rep = tile * kTile + lane;
+  uint32_t word = 0u;
+  if (rep < ngrids) {
+    const int *src = g + rep * N;
+    const int s0 = w * 32;
+    const int nb = min(32, N - s0);
+    for (int b = 0; b < nb; ++b) word |= (src[s0 + b] == 1 ? 1u : 0u) << b;
+  }
+  lat[idx] = word;
+}
+
+// lattice words -> int32 grids; one thread per (replica, w).
+__global__ void k_unpack_grids(const uint32_t *lat, int *g, int L, int ngrids, long long total) {
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= total) return;
+  const int N = L * L, W = (N + 31) >> 5;
+  const long long rep = idx / W;
+  const int w = (int)(idx % W);
+  const uint32_t word = lat[(rep >> 5) * W * kTile + (size_t)w * kTile + (rep & 31)];
+  int *dst = g + rep * N;
+  const int s0 = w * 32;
+  const int nb = min(32, N - s0);
+  for (int b = 0; b < nb; ++b) dst[s0 + b] = ((word >> b) & 1u) ? 1 : -1;
+}
+
+// gridstates.bin payload, N % 32 == 0: output word k is lattice word
+// (rep = k / W, w = k % W): a per-tile transpose.
+__global__ void k_pack_frame32(const uint32_t *lat, uint32_t *out, int W, long long nwords) {
+  const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nwords) return;
+  const long long rep = k / W;
+  const int w = (int)(k % W);
+  out[k] = lat[(rep >> 5) * W * kTile + (size_t)w * kTile + (rep & 31)];
+}
+
+// General payload: one thread per output byte, bit cursor over all spins.
+__global__ void k_pack_frame8(const uint32_t *lat, uint8_t *out, int L, long long nbits,
+                              long long nbytes) {
+  const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= nbytes) return;
+  const int N = L * L, W = (N + 31) >> 5;
+  uint32_t byte = 0u;
+  for (int b = 0; b < 8; ++b) {
+    const long long pbit = j * 8 + b;
+    if (pbit >= nbits) break;
+    const long long rep = pbit / N;
+    const int s = (int)(pbit % N);
+    const uint32_t word = lat[(rep >> 5) * W * kTile + (size_t)(s >> 5) * kTile + (rep & 31)];
+    byte |= ((word >> (s & 31)) & 1u) << b;
+  }
+  out[j] = (uint8_t)byte;
+}
+
+template <typename Kern>
+int launch_tiles(Kern kern, const SweepLaunch &p, cudaStream_t s) {
+  const int W = words_per_replica(p.L);
+  const int nwarps = p.warps_per_cta > 0 ? p.warps_per_cta : 1;
+  const int tiles = tiles_for(p.n_active);
+  if (tiles == 0) return GASP_OK;
+  const size_t smem = (size_t)(kHeaderWords + nwarps * W * kTile) * sizeof(uint32_t);
+  GASP_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int blocks = (tiles + nwarps - 1) / nwarps;
+  kern<<<blocks, nwarps * 32, smem, s>>>(p);
+  GASP_CUDA(cudaGetLastError());
+  return GASP_OK;
+}
+
+template <bool F>
+int dispatch_exact(const SweepLaunch &p, cudaStream_t s) {
+  switch (p.L) {
+    case 16: return launch_tiles(k_sweep_exact<16, F>, p, s);
+    case 32: return launch_tiles(k_sweep_exact<32, F>, p, s);
+    case 48: return launch_tiles(k_sweep_exact<48, F>, p, s);
+    case 64: return launch_tiles(k_sweep_exact<64, F>, p, s);
+    case 96: return launch_tiles(k_sweep_exact<96, F>, p, s);
+    case 128: return launch_tiles(k_sweep_exact<128, F>, p, s);
+    default: return launch_tiles(k_sweep_exact<0, F>, p, s);
+  }
+}
+
+}  // namespace
+
+int max_shared_L(int device) {
+  int optin = 0;
+  if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device) != cudaSuccess)
+    return 0;
+  const int words = optin / 4 - kHeaderWords;  // one warp per CTA
+  int L = 1;
+  while (words_per_replica(L + 1) * kTile <= words) ++L;
+  return L;
+}
+
+int launch_rng_init(uint32_t *rng, int ngrids, int stride, unsigned long long seed, cudaStream_t s) {
+  if (ngrids <= 0) return GASP_OK;
+  k_rng_init<<<(ngrids + 127) / 128, 128, 0, s>>>(rng, ngrids, stride, seed);
+  GASP_CUDA(cudaGetLastError());
+  return GASP_OK;
+}
+
+int launch_build_thresholds(const float *d_pacc20, uint32_t *d_thr10, int *d_flags, cudaStream_t s) {
+  k_build_thresholds<<<1, 32, 0, s>>>(d_pacc20, d_thr10, d_flags);
+  GASP_CUDA(cudaGetLastError());
+  return GASP_OK;
+}
+
+int launch_sweep_exact(const SweepLaunch &p, cudaStream_t s) {
+  return p.float_compare ? dispatch_exact<true>(p, s) : dispatch_exact<false>(p, s);
+}
+
+int launch_sweep_trace_cpu(const SweepLaunch &p, cudaStream_t s) {
+  switch (p.L) {
+    case 16: return launch_tiles(k_sweep_trace_cpu<16>, p, s);
+    case 64: return launch_tiles(k_sweep_trace_cpu<64>, p, s);
+    default: return launch_tiles(k_sweep_trace_cpu<0>, p, s);
+  }
+}
+
+int launch_measure(const uint32_t *lat, int L, int ngrids, float *mag, cudaStream_t s) {
+  if (ngrids <= 0) return GASP_OK;
+  k_measure<<<(ngrids + 127) / 128, 128, 0, s>>>(lat, L, ngrids, mag);
+  GASP_CUDA(cudaGetLastError());
+  return GASP_OK;
+}
+
+int launch_pack_grids(const int *g, uint32_t *lat, int L, int ngrids, cudaStream_t s) {
+  const long long total = (long long)tiles_for(ngrids) * words_per_replica(L) * kTile;
+  if (total == 0) return GASP_OK;
+  k_pack_grids<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(g, lat, L, ngrids, total);
+  GASP_CUDA(cudaGetLastError());
+  return GASP_OK;
+}
+
+int launch_unpack_grids(const uint32_t *lat, int *g, int L, int ngrids, cudaStream_t s) {
+  const long long total = (long long)ngrids * words_per_replica(L);
+  if (total == 0) return GASP_OK;
+  k_unpack_grids<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(lat, g, L, ngrids, total);
+  GASP_CUDA(cudaGetLastError());
+  return GASP_OK;
+}
+
+int launch_pack_frame(const uint32_t *lat, uint8_t *frame, int L, int ngrids, cudaStream_t s) {
+  const long long N = (long long)L * L;
+  const long long nbits = N * ngrids;
+  if (nbits == 0) return GASP_OK;
+  if (N % 32 == 0) {
+    const long long nwords = nbits / 32;
+    k_pack_frame32<<<(unsigned)((nwords + 255) / 256), 256, 0, s>>>(
+        lat, reinterpret_cast<uint32_t *>(frame), (int)(N / 32), nwords);
+  } else {
+    const long long nbytes = (nbits + 7) / 8;
+    k_pack_frame8<<<(unsigned)((nbytes + 255) / 256), 256, 0, s>>>(lat, frame, L, nbits, nbytes);
+  }
+  GASP_CUDA(cudaGetLastError());
+  return GASP_OK;
+}
+
+}  // namespace gasp

@@ -1,0 +1,191 @@
+"""Python host layer over the gasp-b200 C ABI.
+
+Thin objects owning the native handles: ``DeviceGrids`` (replaces the
+reference's device grid array, src/gpu_tools.cu:143-159), ``RngStates``
+(replaces the curandState array, src/gpu_tools.cu:162-174) and ``run_driver``
+(replaces mc_driver_gpu, src/mc_gpu.cu:530-831).  Every call goes to the CUDA
+library; a missing library or device raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _native as nat
+from ._native import check, lib
+
+
+def init_device(device_index=-1, verbose=False):
+    """Selects a device; returns (device, n_SMs).  src/gpu_tools.cu:18-99."""
+    dev, nsms = C.c_int(), C.c_int()
+    check(lib().gasp_init_device(int(device_index), int(bool(verbose)), C.byref(dev),
+                                 C.byref(nsms)), "gasp_init_device")
+    return dev.value, nsms.value
+
+
+def select_gpu_method(L, ngrids, threads_per_block=32, device=-1):
+    """The reference's method auto-selection rule (src/gpu_tools.cu:205-232)."""
+    m = C.c_int()
+    check(lib().gasp_select_gpu_method(L, ngrids, threads_per_block, device, C.byref(m)),
+          "gasp_select_gpu_method")
+    return m.value
+
+
+def acceptance_table(beta, h):
+    """float32[20] table of preComputeProbs_gpu (src/mc_gpu.cu:21-37)."""
+    out = np.zeros(20, np.float32)
+    check(lib().gasp_acceptance_table(float(beta), float(h), out), "gasp_acceptance_table")
+    return out
+
+
+def max_shared_L(device=-1):
+    v = C.c_int()
+    check(lib().gasp_max_shared_L(device, C.byref(v)), "gasp_max_shared_L")
+    return v.value
+
+
+def set_stream(stream_handle):
+    """Route this thread's device work to a cudaStream_t (int handle or 0)."""
+    check(lib().gasp_set_stream(C.c_void_p(int(stream_handle) if stream_handle else None)))
+
+
+class RngStates:
+    """Per-replica cuRAND XORWOW states, seeded as gpuInitRand."""
+
+    def __init__(self, ngrids, seed, threads_per_block=32):
+        self.ngrids = int(ngrids)
+        self._h = C.c_void_p()
+        check(lib().gasp_init_rand(self.ngrids, threads_per_block, C.c_ulonglong(int(seed)),
+                                   C.byref(self._h)), "gasp_init_rand")
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if self._h:
+            lib().gasp_free_rand(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class DeviceGrids:
+    """A device-resident set of ngrids LxL replicas (bit-packed)."""
+
+    def __init__(self, L, ngrids, host_grids=None, threads_per_block=32):
+        self.L, self.ngrids = int(L), int(ngrids)
+        self._h = C.c_void_p()
+        check(lib().gasp_init_grid(self.L, self.ngrids, threads_per_block, None,
+                                   C.byref(self._h)), "gasp_init_grid")
+        if host_grids is not None:
+            self.upload(host_grids)
+
+    @property
+    def handle(self):
+        return self._h
+
+    def upload(self, grids):
+        g = np.ascontiguousarray(grids, dtype=np.int32).reshape(-1)
+        if g.size != self.L * self.L * self.ngrids:
+            raise ValueError("grid array has the wrong size")
+        check(lib().gasp_grids_upload(self._h, g), "gasp_grids_upload")
+
+    def download(self):
+        out = np.empty(self.L * self.L * self.ngrids, np.int32)
+        check(lib().gasp_grids_download(self._h, out), "gasp_grids_download")
+        return out.reshape(self.ngrids, self.L, self.L)
+
+    def magnetisation(self):
+        out = np.empty(self.ngrids, np.float32)
+        check(lib().gasp_magnetisation(self._h, out), "gasp_magnetisation")
+        return out
+
+    def pack_frame(self):
+        n = lib().gasp_frame_bytes(self.L, self.ngrids)
+        out = np.empty(n, np.uint8)
+        check(lib().gasp_pack_frame(self._h, out), "gasp_pack_frame")
+        return out
+
+    def sweep(self, rng, beta, h, nsweeps, gpu_method=2):
+        check(lib().gasp_sweep(self._h, rng.handle, float(beta), float(h), int(nsweeps),
+                               int(gpu_method)), "gasp_sweep")
+
+    def sweep_trace_cpu(self, stream, beta, h, nsweeps):
+        s = np.ascontiguousarray(stream, np.float64)
+        need = self.ngrids * 3 * self.L * self.L * nsweeps
+        if s.size < need:
+            raise ValueError(f"trace stream too short ({s.size} < {need})")
+        check(lib().gasp_sweep_trace_cpu(self._h, s, float(beta), float(h), int(nsweeps)),
+              "gasp_sweep_trace_cpu")
+
+    def close(self):
+        if self._h:
+            lib().gasp_free_grid(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def run_driver(dgrids, rng, beta, h, tot_nsweeps, mag_output_int, grid_output_int, itask=0,
+               dn_thr=-0.9, up_thr=0.9, ninputs=1, host_grids=None, fates=None,
+               outfunc=None, packed_out=None, verbosity=0, compact=False,
+               threads_per_block=32, gpu_method=2, filename="gridstates.bin"):
+    """Runs gasp_mc_driver_gpu_ex; returns (result, fates, elapsed_s, attempts).
+
+    ``outfunc(L, ngrids, grids_int32[ngrids,L,L], isweep, mag)`` mirrors the
+    reference's GridOutputFunc; ``packed_out(L, ngrids, payload_u8, isweep,
+    mag)`` receives gridstates.bin payloads.  Either returns 0 on success.
+    """
+    L, ngrids = dgrids.L, dgrids.ngrids
+    nres = tot_nsweeps // mag_output_int if itask == 0 else ninputs
+    result = np.zeros(max(nres, 1), np.float32)
+    if host_grids is None and outfunc is not None:
+        host_grids = np.empty((ngrids, L, L), np.int32)
+    hg_ptr = None
+    if host_grids is not None:
+        host_grids = np.ascontiguousarray(host_grids, np.int32)
+        hg_ptr = host_grids.ctypes.data_as(C.POINTER(C.c_int))
+    if itask == 1 and fates is None:
+        fates = np.full(ngrids, -1, np.int32)
+    fate_ptr = fates.ctypes.data_as(C.c_void_p) if fates is not None else None
+
+    def _outfunc(L_, ng_, gptr, isweep, magp, lcp, cv, dn, up, fn):
+        try:
+            g = np.ctypeslib.as_array(gptr, shape=(ng_ * L_ * L_,)).reshape(ng_, L_, L_)
+            m = np.ctypeslib.as_array(magp, shape=(ng_,))
+            return int(outfunc(L_, ng_, g, isweep, m) or 0)
+        except Exception:  # a Python error stops the driver
+            return 1
+
+    def _packed(L_, ng_, payload, nbytes, isweep, magp, user):
+        try:
+            b = np.ctypeslib.as_array(payload, shape=(nbytes,))
+            m = np.ctypeslib.as_array(magp, shape=(ng_,))
+            return int(packed_out(L_, ng_, b, isweep, m) or 0)
+        except Exception:
+            return 1
+
+    cb = nat.GRID_OUTPUT_FN(_outfunc) if outfunc is not None else nat.GRID_OUTPUT_FN()
+    pcb = nat.PACKED_OUTPUT_FN(_packed) if packed_out is not None else nat.PACKED_OUTPUT_FN()
+    elapsed = C.c_double(0.0)
+    attempts = C.c_longlong(0)
+    opts = nat.DriverOptsT(verbosity, int(bool(compact)), pcb, None,
+                           C.pointer(elapsed), C.pointer(attempts))
+    grids_t = nat.GpuGridsT(L, ngrids, hg_ptr, dgrids.handle)
+    samp = nat.SamplerT(tot_nsweeps, mag_output_int, grid_output_int)
+    calc = nat.FunctionT(itask, dn_thr, up_thr, ninputs, -1, b"magnetisation",
+                         result.ctypes.data_as(C.POINTER(C.c_float)), filename.encode())
+    run = nat.GpuRunT(rng.handle, threads_per_block, gpu_method)
+    check(lib().gasp_mc_driver_gpu_ex(grids_t, float(beta), float(h), fate_ptr, samp, calc, run,
+                                      cb, C.byref(opts)), "gasp_mc_driver_gpu")
+    return result[:nres], fates, elapsed.value, attempts.value

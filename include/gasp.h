@@ -1,0 +1,250 @@
+/*
+ * gasp.h -- C ABI of gasp-b200, a B200-native (sm_100a) engine for the
+ * many-replica 2D Ising Metropolis path of GASP (dquigley533/GPU_2DIsing).
+ *
+ * Every entry point is extern "C", takes plain pointers and sizes, and returns
+ * a status code (GASP_OK == 0) instead of calling exit() as the reference
+ * does.  Each declaration names the reference interface it replaces
+ * (file:line inside the reference project).  Host grids use the reference's
+ * layout: int32 spins (+1/-1), [grid][row][col] (src/grid.c:10).
+ *
+ * Threading: calls on one handle must not overlap; different handles may be
+ * used from different host threads.  All device work of a handle is issued on
+ * that handle's CUDA stream (gasp_set_stream).
+ */
+#ifndef GASP_H
+#define GASP_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+enum {
+  GASP_OK = 0,
+  GASP_ERR_INVALID = 1,     /* bad argument: sizes, method, divisibility      */
+  GASP_ERR_CUDA = 2,        /* CUDA runtime error (message via gasp_last_error) */
+  GASP_ERR_NO_DEVICE = 3,   /* no CUDA device (reference returns -1, src/gpu_tools.cu:27-29) */
+  GASP_ERR_ALLOC = 4,       /* host or device allocation failed               */
+  GASP_ERR_IO = 5,          /* file open/read/write failed                    */
+  GASP_ERR_FORMAT = 6,      /* file header does not match (src/io.c:25-28)    */
+  GASP_ERR_CALLBACK = 7,    /* user output callback returned non-zero         */
+  GASP_ERR_UNSUPPORTED = 8, /* e.g. L beyond the shared-memory path            */
+  GASP_ERR_TIMEOUT = 9      /* a bounded device-side wait expired             */
+};
+
+/* Human-readable text for a status code. */
+const char *gasp_status_string(int status);
+/* Detail of the last error raised on the calling host thread. */
+const char *gasp_last_error(void);
+/* Library version string. */
+const char *gasp_version(void);
+
+/* --------------------------------------------------------------- device */
+/* Replaces gpuInitDevice (include/gpu_tools.h:16, src/gpu_tools.cu:18-99):
+ * selects device_index (-1 keeps the current device), reports the device in
+ * use and its SM count.  verbose != 0 prints the reference's device summary. */
+int gasp_init_device(int device_index, int verbose, int *device_out, int *nsms_out);
+
+/* Replaces select_gpu_method (include/gpu_tools.h:38, src/gpu_tools.cu:205-232):
+ * the reference's rule, evaluated against the device's default per-block
+ * shared memory (method 2 if it fits, else 0). */
+int gasp_select_gpu_method(int L, int ngrids, int threads_per_block, int gpu_device,
+                           int *method_out);
+
+/* Replaces preComputeProbs_gpu (include/mc_gpu.h:28, src/mc_gpu.cu:21-37):
+ * the 20-slot float acceptance table exp(-beta*2*s*(nsum+h)) computed with the
+ * host expf exactly as the reference does; index 5*(s+1)+nsum+4. */
+int gasp_acceptance_table(double beta, double h, float table_out[20]);
+
+/* Largest L the shared-memory sweep supports on this device. */
+int gasp_max_shared_L(int device, int *maxL_out);
+
+/* Makes subsequent device work of this thread's handles go to `stream`
+ * (a cudaStream_t; NULL restores the library's own stream). */
+int gasp_set_stream(void *stream);
+
+/* ----------------------------------------------------- device grid sets */
+/* Opaque device-resident replica set: bit-packed lattices, magnetisation,
+ * fates.  Replaces the raw int* d_ising_grids + d_neighbour_list pair of
+ * mc_gpu_grids_t (include/mc_gpu.h:12-18). */
+typedef struct gasp_grids gasp_grids_t;
+
+/* Replaces gpuInitGrid (include/gpu_tools.h:19, src/gpu_tools.cu:143-159):
+ * allocates the device set for ngrids LxL replicas and uploads host_grids
+ * (may be NULL: all spins -1).  threads_per_block is accepted for signature
+ * parity; the kernels choose their own launch shape. */
+int gasp_init_grid(int L, int ngrids, int threads_per_block, const int *host_grids,
+                   gasp_grids_t **grids_out);
+/* Frees a grid set (replaces the cudaFree calls of src/ising.cu:191-193). */
+int gasp_free_grid(gasp_grids_t *grids);
+/* Host <-> device copies of all replicas in the reference's int32 layout. */
+int gasp_grids_upload(gasp_grids_t *grids, const int *host_grids);
+int gasp_grids_download(gasp_grids_t *grids, int *host_grids);
+/* Replica count / side length of a set. */
+int gasp_grids_shape(const gasp_grids_t *grids, int *L_out, int *ngrids_out);
+
+/* ------------------------------------------------------------ RNG states */
+/* Opaque per-replica XORWOW states (cuRAND device API), replaces curandState*. */
+typedef struct gasp_rng gasp_rng_t;
+
+/* Replaces gpuInitRand (include/gpu_tools.h:22, src/gpu_tools.cu:162-174):
+ * curand_init(seed, subsequence = replica index, offset 0) per replica, so a
+ * replica's stream is independent of the launch shape, exactly as the
+ * reference. */
+int gasp_init_rand(int ngrids, int threads_per_block, unsigned long long seed,
+                   gasp_rng_t **rng_out);
+int gasp_free_rand(gasp_rng_t *rng);
+
+/* ------------------------------------------------------------ kernels */
+/* Sweep modes. */
+enum {
+  /* Reference-exact: per-replica cuRAND XORWOW stream, two draws per attempt,
+   * site = floor(fl((1-FLT_EPSILON)*L*L) * u1), accept iff u2 < P (float).
+   * Bit-identical to mc_sweep_gpu (method 0), mc_sweep_gpu_bitrep (method 1)
+   * and mc_sweep_gpu_bitmap32 (method 2) for the same seed. */
+  GASP_MODE_EXACT = 0,
+  /* CPU-trace: consumes a caller-supplied stream of doubles (row-u, col-u, xi
+   * per attempt) with mc_sweep_cpu's arithmetic (src/mc_cpu.c:41-89).
+   * Bit-identical to the reference CPU path fed the same stream. */
+  GASP_MODE_TRACE_CPU = 1
+};
+
+/* One sweep batch: every replica does L*L*nsweeps attempted flips
+ * (replaces one launch of the mc_sweep_gpu* kernels, include/mc_gpu.h:35-38,
+ * launched from src/mc_gpu.cu:679-706).  gpu_method (0, 1, 2) is accepted for
+ * parity; all three map to the exact kernel, which reproduces each of them.
+ * mag_out (device or NULL) receives each replica's magnetisation after the
+ * batch.  Asynchronous on the handle's stream. */
+int gasp_sweep(gasp_grids_t *grids, gasp_rng_t *rng, double beta, double h, int nsweeps,
+               int gpu_method);
+
+/* CPU-trace sweep: stream holds, for replica r, 3*L*L*nsweeps doubles starting
+ * at stream[r * 3*L*L*nsweeps] (host or device pointer; host is copied). */
+int gasp_sweep_trace_cpu(gasp_grids_t *grids, const double *stream, double beta, double h,
+                         int nsweeps);
+
+/* Replaces compute_magnetisation_gpu (include/mc_gpu.h:41, src/mc_gpu.cu:437-455):
+ * m = (float)(sum of spins) / (float)(L*L) per replica, bit-identical.
+ * host_mag receives ngrids floats (synchronous). */
+int gasp_magnetisation(gasp_grids_t *grids, float *host_mag);
+
+/* gridstates.bin frame payload (src/io.c:89-117): ceil(L*L*ngrids/8) bytes,
+ * grid-major, row-major, LSB-first, bit 1 iff spin +1.  Packed on the device;
+ * host_out receives the bytes (synchronous). */
+int gasp_pack_frame(gasp_grids_t *grids, uint8_t *host_out);
+size_t gasp_frame_bytes(int L, int ngrids);
+
+/* ----------------------------------------------------------- the driver */
+/* Mirrors mc_sampler_t (include/mc_cpu.h:13-17). */
+typedef struct {
+  int tot_nsweeps;
+  int mag_output_int;
+  int grid_output_int;
+} gasp_sampler_t;
+
+/* Mirrors mc_function_t (include/mc_cpu.h:19-28). cv must be "magnetisation"
+ * (the largest_cluster CV is not provided by this library). */
+typedef struct {
+  int itask;           /* 0 nucleation swarm, 1 committor                  */
+  double dn_thr;       /* below: basin A (strict <)                        */
+  double up_thr;       /* above: basin B / nucleated (strict >)            */
+  int ninputs;         /* committor input blocks (ngrids % ninputs == 0)   */
+  int initial_spin;
+  const char *cv;
+  float *result;       /* itask 0: tot/mag_int floats; itask 1: ninputs    */
+  const char *filename;
+} gasp_function_t;
+
+/* Mirrors gpu_run_t (include/mc_gpu.h:20-24). */
+typedef struct {
+  gasp_rng_t *d_state;
+  int threadsPerBlock;
+  int gpu_method;
+} gasp_gpu_run_t;
+
+/* Mirrors mc_gpu_grids_t (include/mc_gpu.h:12-18): ising_grids is the host
+ * copy the output callback receives. */
+typedef struct {
+  int L;
+  int ngrids;
+  int *ising_grids;
+  gasp_grids_t *d_grids;
+} gasp_gpu_grids_t;
+
+/* Same signature as GridOutputFunc (include/mc_cpu.h:31).  Non-zero return
+ * stops the driver with GASP_ERR_CALLBACK. */
+typedef int (*gasp_grid_output_fn)(int L, int ngrids, int *grid_data, int isweep,
+                                   float *magnetisation, float *lclus_size, char *cv,
+                                   double dn_thr, double up_thr, char *filename);
+
+/* Faster alternative callback: receives the packed gridstates.bin payload of
+ * the frame (gasp_frame_bytes bytes) instead of expanded int32 grids. */
+typedef int (*gasp_packed_output_fn)(int L, int ngrids, const uint8_t *payload,
+                                     size_t nbytes, int isweep,
+                                     const float *magnetisation, void *user);
+
+/* Driver options beyond the reference's arguments. */
+typedef struct {
+  int verbosity;        /* 0 silent; 1 the reference CLI's stdout lines    */
+  int compact;          /* itask 1: stop simulating resolved replicas      */
+  gasp_packed_output_fn packed_out; /* if set, used instead of outfunc     */
+  void *packed_user;
+  double *elapsed_s;    /* if set, receives the driver's wall time          */
+  long long *attempts;  /* if set, receives attempted flips simulated       */
+} gasp_driver_opts_t;
+
+/* Replaces mc_driver_gpu (include/mc_gpu.h:47, src/mc_gpu.cu:530-831): the
+ * sweep / magnetisation / threshold-check / dump loop with the reference's
+ * timing: checks at isweep % mag_output_int == 0 or isweep == tot-1, dumps at
+ * isweep % grid_output_int == 0 or isweep == tot-1, sweeps_per_call =
+ * min(mag_output_int, grid_output_int); itask 0 fills result with the
+ * nucleated fraction (pre-filled with 1.0) and stops when all replicas are
+ * above up_thr; itask 1 records absorbing fates (-1 pending, 0 A, 1 B) in
+ * grid_fate and writes pB per input block.  outfunc may be NULL. */
+int gasp_mc_driver_gpu(gasp_gpu_grids_t grids, double beta, double h, int *grid_fate,
+                       gasp_sampler_t samples, gasp_function_t calc, gasp_gpu_run_t gpu_state,
+                       gasp_grid_output_fn outfunc);
+int gasp_mc_driver_gpu_ex(gasp_gpu_grids_t grids, double beta, double h, int *grid_fate,
+                          gasp_sampler_t samples, gasp_function_t calc,
+                          gasp_gpu_run_t gpu_state, gasp_grid_output_fn outfunc,
+                          const gasp_driver_opts_t *opts);
+
+/* ---------------------------------------------------- host-side helpers */
+/* Replace init_grids_uniform / init_grids_from_file / init_grids_from_array /
+ * init_fates (include/grid.h:5-9, src/grid.c:5-87); caller owns the memory
+ * (ngrids*L*L ints, or ngrids ints for fates). */
+int gasp_init_grids_uniform(int L, int ngrids, int spin, int *out);
+int gasp_init_grids_from_file(const char *path, int L, int ngrids, int *out);
+int gasp_init_grids_from_array(int L, int ngrids, int ninputs, const int *array, int *out);
+int gasp_init_fates(int ngrids, int *out);
+
+/* Replaces read_input_grid (include/io.h:8, src/io.c:4-65): gridinput.bin
+ * (int32 L + ceil(L*L/8) LSB-first bytes) copied into all ngrids grids.
+ * GASP_ERR_FORMAT if the file's L differs. */
+int gasp_read_input_grid(const char *path, int L, int ngrids, int *out);
+
+/* Replaces write_ising_grids (include/io.h:11, src/io.c:67-130) and has its
+ * GridOutputFunc signature: appends one gridstates.bin frame to filename. */
+int gasp_write_ising_grids(int L, int ngrids, int *ising_grids, int isweep,
+                           float *magnetisation, float *lclus_size, char *cv,
+                           double dn_thr, double up_thr, char *filename);
+/* Appends a frame from an already packed payload. */
+int gasp_write_packed_frame(const char *path, int L, int ngrids, int isweep,
+                            const uint8_t *payload, size_t nbytes);
+
+/* Replaces bootstrap_errbar (include/bootstrap.h:5, src/bootstrap.c:6-65):
+ * m resamples with libc rand()%ngrids, population standard deviation.
+ * Negative return on allocation failure, as the reference. */
+double gasp_bootstrap_errbar(int ngrids, int m, const int *grid_fate);
+
+/* pB per contiguous input block from fates (src/mc_gpu.cu:812-826). */
+int gasp_committor_from_fates(int ngrids, int ninputs, const int *grid_fate, float *pB);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GASP_H */

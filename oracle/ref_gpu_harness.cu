@@ -1,0 +1,172 @@
+// ref_gpu_harness.cu -- project-written glue around the reference's GPU code
+// (src/mc_gpu.cu, src/gpu_tools.cu), which oracle/Makefile compiles UNMODIFIED
+// for sm_100a into oracle/_ref/libref_gpu.so.  TEST INFRASTRUCTURE ONLY: the
+// GPU parity tests use it as the oracle for bit-exact trajectories.
+//
+// Safety: the reference's method-2 staging reads 32 grids per block even when
+// ngrids % 32 != 0 (src/mc_gpu.cu:293-300).  Every device grid buffer this
+// harness hands to reference code is therefore padded to a whole number of
+// 64-grid blocks, so those reads stay inside the allocation.
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "mc_gpu.h"
+#include "gpu_tools.h"
+
+namespace {
+
+int padded_ngrids(int ngrids) { return ((ngrids + 63) / 64) * 64; }
+
+#define HCHECK(x)                                                              \
+  do {                                                                         \
+    cudaError_t e_ = (x);                                                      \
+    if (e_ != cudaSuccess) {                                                   \
+      fprintf(stderr, "ref harness: %s at %s:%d\n", cudaGetErrorString(e_),    \
+              __FILE__, __LINE__);                                             \
+      return -1;                                                               \
+    }                                                                          \
+  } while (0)
+
+// Same launch configuration as the reference driver (src/mc_gpu.cu:679-706).
+int launch_reference_sweep(int method, int L, int ngrids, int tpb, curandState *d_state,
+                           int *d_grids, int *d_nbr, double beta, double h, int nsweeps) {
+  int blocks = ngrids / tpb + (ngrids % tpb != 0);
+  if (method == 0) {
+    mc_sweep_gpu<<<blocks, tpb>>>(L, d_state, ngrids, d_grids, d_nbr, (float)beta, (float)h, nsweeps);
+  } else if (method == 1) {
+    size_t shmem = (size_t)(L * L / 8) * tpb;
+    if ((L * L) % 8 != 0) shmem = (size_t)(L * L / 8 + 1) * tpb;  // see note below
+    cudaFuncSetAttribute(mc_sweep_gpu_bitrep, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    cudaFuncSetAttribute(mc_sweep_gpu_bitrep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem);
+    mc_sweep_gpu_bitrep<<<blocks, tpb, shmem>>>(L, d_state, ngrids, d_grids, d_nbr, (float)beta, (float)h, nsweeps);
+  } else if (method == 2 && tpb == 32) {
+    // The reference sizes this as ceil(L*L/8)*tpb with integer division
+    // first (src/mc_gpu.cu:688); for L*L % 8 != 0 that is smaller than the
+    // L*L words the kernel indexes, so the harness gives L*L*4 bytes.
+    size_t shmem = (size_t)L * L * 4;
+    cudaFuncSetAttribute(mc_sweep_gpu_bitmap32, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    cudaFuncSetAttribute(mc_sweep_gpu_bitmap32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem);
+    mc_sweep_gpu_bitmap32<<<blocks, tpb, shmem>>>(L, d_state, ngrids, d_grids, d_nbr, (float)beta, (float)h, nsweeps);
+  } else {
+    return -2;
+  }
+  HCHECK(cudaGetLastError());
+  HCHECK(cudaDeviceSynchronize());
+  return 0;
+}
+
+__global__ void record_uniforms(int ngrids, int n, curandState *state, float *out) {
+  int idx = threadIdx.x + blockIdx.x * blockDim.x;
+  if (idx >= ngrids) return;
+  curandState local = state[idx];
+  for (int i = 0; i < n; ++i) out[(size_t)idx * n + i] = curand_uniform(&local);
+  state[idx] = local;
+}
+
+}  // namespace
+
+extern "C" {
+
+// Runs `ncalls` launches of the reference sweep kernel `method` (0, 1, or 2
+// with tpb 32), nsweeps each, from caller grids, seeding exactly as
+// gpuInitRand (src/gpu_tools.cu:162-174).  mags receives (ncalls+1)*ngrids
+// floats from the reference magnetisation kernel before the first and after
+// every call; grids_inout receives the final grids.
+int refgpu_run_kernels(int L, int ngrids, int tpb, int method, unsigned long long seed,
+                       double beta, double h, int nsweeps, int ncalls,
+                       int *grids_inout, float *mags) {
+  int npad = padded_ngrids(ngrids);
+  size_t n = (size_t)L * L;
+  int *d_grids = nullptr, *d_nbr = nullptr;
+  float *d_mag = nullptr;
+  curandState *d_state = nullptr;
+  HCHECK(cudaMalloc(&d_grids, n * npad * sizeof(int)));
+  HCHECK(cudaMemset(d_grids, 0, n * npad * sizeof(int)));
+  HCHECK(cudaMemcpy(d_grids, grids_inout, n * ngrids * sizeof(int), cudaMemcpyHostToDevice));
+  HCHECK(cudaMalloc(&d_nbr, n * 4 * sizeof(int)));
+  HCHECK(cudaMalloc(&d_mag, (size_t)npad * sizeof(float)));
+  preComputeNeighbours_gpu(L, d_grids, d_nbr);
+  gpuInitRand(ngrids, tpb, (unsigned long)seed, &d_state);
+  preComputeProbs_gpu(beta, h);
+  int blocks = ngrids / tpb + (ngrids % tpb != 0);
+  for (int c = 0; c <= ncalls; ++c) {
+    compute_magnetisation_gpu<<<blocks, tpb>>>(L, ngrids, d_grids, d_mag);
+    HCHECK(cudaGetLastError());
+    HCHECK(cudaMemcpy(mags + (size_t)c * ngrids, d_mag, ngrids * sizeof(float), cudaMemcpyDeviceToHost));
+    if (c == ncalls) break;
+    int rc = launch_reference_sweep(method, L, ngrids, tpb, d_state, d_grids, d_nbr, beta, h, nsweeps);
+    if (rc != 0) return rc;
+  }
+  HCHECK(cudaMemcpy(grids_inout, d_grids, n * ngrids * sizeof(int), cudaMemcpyDeviceToHost));
+  cudaFree(d_grids); cudaFree(d_nbr); cudaFree(d_mag); cudaFree(d_state);
+  return 0;
+}
+
+// The first n curand_uniform draws of each replica's stream, seeded as
+// gpuInitRand does (subsequence = replica index).  out: [ngrids][n].
+int refgpu_uniform_stream(unsigned long long seed, int ngrids, int n, float *out) {
+  curandState *d_state = nullptr;
+  float *d_out = nullptr;
+  gpuInitRand(ngrids, 32, (unsigned long)seed, &d_state);
+  HCHECK(cudaMalloc(&d_out, (size_t)ngrids * n * sizeof(float)));
+  record_uniforms<<<(ngrids + 31) / 32, 32>>>(ngrids, n, d_state, d_out);
+  HCHECK(cudaGetLastError());
+  HCHECK(cudaMemcpy(out, d_out, (size_t)ngrids * n * sizeof(float), cudaMemcpyDeviceToHost));
+  cudaFree(d_out); cudaFree(d_state);
+  return 0;
+}
+
+static int *g_cap_grids = nullptr, *g_cap_isweep = nullptr;
+static float *g_cap_mag = nullptr;
+static int g_cap_max = 0, g_cap_n = 0;
+
+static int capture_outfunc(int L, int ngrids, int *grid_data, int isweep, float *magnetisation,
+                           float *, char *, double, double, char *) {
+  if (g_cap_n < g_cap_max) {
+    size_t n = (size_t)L * L * ngrids;
+    if (g_cap_grids) memcpy(g_cap_grids + (size_t)g_cap_n * n, grid_data, n * sizeof(int));
+    if (g_cap_mag) memcpy(g_cap_mag + (size_t)g_cap_n * ngrids, magnetisation, ngrids * sizeof(float));
+    if (g_cap_isweep) g_cap_isweep[g_cap_n] = isweep;
+  }
+  g_cap_n++;
+  return 0;
+}
+
+// Runs the reference driver mc_driver_gpu (src/mc_gpu.cu:530-831) end to end
+// with a capturing output callback.  Returns the number of callback calls.
+int refgpu_run_driver(int L, int ngrids, int tpb, int method, unsigned long long seed,
+                      double beta, double h, int tot_nsweeps, int mag_output_int,
+                      int grid_output_int, int itask, double dn_thr, double up_thr,
+                      int ninputs, int *grids_inout, int *fates_inout, float *result,
+                      int max_frames, int *frame_grids, int *frame_isweep, float *frame_mag) {
+  int npad = padded_ngrids(ngrids);
+  size_t n = (size_t)L * L;
+  int *d_grids = nullptr, *d_nbr = nullptr;
+  curandState *d_state = nullptr;
+  HCHECK(cudaMalloc(&d_grids, n * npad * sizeof(int)));
+  HCHECK(cudaMemset(d_grids, 0, n * npad * sizeof(int)));
+  HCHECK(cudaMemcpy(d_grids, grids_inout, n * ngrids * sizeof(int), cudaMemcpyHostToDevice));
+  HCHECK(cudaMalloc(&d_nbr, n * 4 * sizeof(int)));
+  preComputeNeighbours_gpu(L, d_grids, d_nbr);
+  gpuInitRand(ngrids, tpb, (unsigned long)seed, &d_state);
+  preComputeProbs_gpu(beta, h);
+  g_cap_grids = frame_grids; g_cap_isweep = frame_isweep; g_cap_mag = frame_mag;
+  g_cap_max = max_frames; g_cap_n = 0;
+  mc_gpu_grids_t grids; grids.L = L; grids.ngrids = ngrids; grids.ising_grids = grids_inout;
+  grids.d_ising_grids = d_grids; grids.d_neighbour_list = d_nbr;
+  mc_sampler_t samples; samples.tot_nsweeps = tot_nsweeps;
+  samples.mag_output_int = mag_output_int; samples.grid_output_int = grid_output_int;
+  mc_function_t calc; memset(&calc, 0, sizeof calc);
+  calc.itask = itask; calc.dn_thr = dn_thr; calc.up_thr = up_thr; calc.ninputs = ninputs;
+  calc.initial_spin = -1; calc.cv = (char *)"magnetisation"; calc.result = result;
+  calc.filename = (char *)"gridstates.bin";
+  gpu_run_t gs; gs.d_state = d_state; gs.threadsPerBlock = tpb; gs.gpu_method = method;
+  mc_driver_gpu(grids, beta, h, fates_inout, samples, calc, gs, capture_outfunc);
+  fflush(stdout);
+  HCHECK(cudaMemcpy(grids_inout, d_grids, n * ngrids * sizeof(int), cudaMemcpyDeviceToHost));
+  cudaFree(d_grids); cudaFree(d_nbr); cudaFree(d_state);
+  return g_cap_n;
+}
+
+}  // extern "C"
