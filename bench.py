@@ -189,8 +189,10 @@ def run_e2e(args, rank, world, dist, torch, engine):
         dist.barrier()
     t0 = time.perf_counter()
     dg2 = engine.DeviceGrids(L, R, host)
+    t1 = time.perf_counter()
     rng2 = engine.RngStates(R, SEED + 7919 * rank + 1)
-    _, _, _, attempts = engine.run_driver(dg2, rng2, BETA, H, SWEEPS_PER_STEP * args.steps,
+    t2 = time.perf_counter()
+    _, _, drv_s, attempts = engine.run_driver(dg2, rng2, BETA, H, SWEEPS_PER_STEP * args.steps,
                                           MAG_INT, GRID_INT, itask=0, dn_thr=-0.9, up_thr=0.9,
                                           packed_out=packed)
     torch.cuda.synchronize()
@@ -205,7 +207,7 @@ def run_e2e(args, rank, world, dist, torch, engine):
     rng2.close()
     return {"value": attempts * world / e2e_s, "unit": UNIT,
             "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
-            "wall_s": e2e_s,
+            "wall_s": e2e_s, "upload_s": t1 - t0, "rng_init_s": t2 - t1, "driver_s": drv_s,
             "scope": "gasp_init_grid (int32 host grids) + gasp_init_rand + "
                      "gasp_mc_driver_gpu over all steps (per-check magnetisation D2H, "
                      "packed dumps every 1000 sweeps)"}
@@ -228,6 +230,7 @@ def run_ours(args, rank, world, local_rank):
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
 
     dg = engine.DeviceGrids(L, R, -np.ones((R, L, L), np.int32))
+    dg.set_option(1, args.variant)  # GASP_OPT_SWEEP_VARIANT
     rng = engine.RngStates(R, SEED + 7919 * rank)
 
     def barrier():
@@ -301,6 +304,7 @@ def run_ours(args, rank, world, local_rank):
 
 
 def main():
+    global SWEEPS_PER_STEP
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=50)
@@ -310,9 +314,10 @@ def main():
     ap.add_argument("--sweeps-per-step", type=int, default=SWEEPS_PER_STEP,
                     help="smaller values give a short launch for ncu captures")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--variant", type=int, default=0,
+                    help="sweep kernel variant (0 fastest for L, 1 generic) for comparisons")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
-    global SWEEPS_PER_STEP
     SWEEPS_PER_STEP = args.sweeps_per_step
     CONFIG["sweeps_per_step"] = SWEEPS_PER_STEP
     rank = int(os.environ.get("RANK", "0"))

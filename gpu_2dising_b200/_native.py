@@ -25,6 +25,9 @@ GASP_ERR_CALLBACK = 7
 GASP_ERR_UNSUPPORTED = 8
 GASP_ERR_TIMEOUT = 9
 
+OPT_SWEEP_VARIANT = 1
+OPT_WARPS_PER_CTA = 2
+
 MODE_EXACT = 0
 MODE_TRACE_CPU = 1
 
@@ -33,7 +36,8 @@ EXPORTED = (
     "gasp_status_string", "gasp_last_error", "gasp_version", "gasp_init_device",
     "gasp_select_gpu_method", "gasp_acceptance_table", "gasp_max_shared_L",
     "gasp_set_stream", "gasp_init_grid", "gasp_free_grid", "gasp_grids_upload",
-    "gasp_grids_download", "gasp_grids_shape", "gasp_init_rand", "gasp_free_rand",
+    "gasp_grids_download", "gasp_grids_shape", "gasp_grids_set_option", "gasp_init_rand",
+    "gasp_free_rand",
     "gasp_sweep", "gasp_sweep_trace_cpu", "gasp_magnetisation", "gasp_pack_frame",
     "gasp_frame_bytes", "gasp_mc_driver_gpu", "gasp_mc_driver_gpu_ex",
     "gasp_init_grids_uniform", "gasp_init_grids_from_file", "gasp_init_grids_from_array",
@@ -110,6 +114,7 @@ def _bind(lib):
         "gasp_grids_upload": (I, [P, _i32p]),
         "gasp_grids_download": (I, [P, _i32p]),
         "gasp_grids_shape": (I, [P, C.POINTER(I), C.POINTER(I)]),
+        "gasp_grids_set_option": (I, [P, I, I]),
         "gasp_init_rand": (I, [I, I, C.c_ulonglong, C.POINTER(P)]),
         "gasp_free_rand": (I, [P]),
         "gasp_sweep": (I, [P, P, C.c_double, C.c_double, I, I]),

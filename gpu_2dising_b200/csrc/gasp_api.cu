@@ -60,6 +60,8 @@ struct GridsExtra {
   size_t stream_cap = 0;
   float *d_mag2 = nullptr;  // second magnetisation buffer for the driver
   int *d_active = nullptr;
+  int variant = 0;          // GASP_OPT_SWEEP_VARIANT
+  int warps_per_cta = 1;    // GASP_OPT_WARPS_PER_CTA
 };
 
 // Extra state kept beside the public struct (allocated with it).
@@ -333,6 +335,21 @@ int gasp_grids_download(gasp_grids_t *g, int *host_grids) {
   return GASP_OK;
 }
 
+int gasp_grids_set_option(gasp_grids_t *g, int option, int value) {
+  if (!g) return GASP_ERR_INVALID;
+  GridsExtra &x = impl(g)->x;
+  if (option == GASP_OPT_SWEEP_VARIANT && (value == 0 || value == 1)) {
+    x.variant = value;
+    return GASP_OK;
+  }
+  if (option == GASP_OPT_WARPS_PER_CTA && value >= 1 && value <= 8) {
+    x.warps_per_cta = value;
+    return GASP_OK;
+  }
+  set_error("unknown option %d or bad value %d", option, value);
+  return GASP_ERR_INVALID;
+}
+
 int gasp_grids_shape(const gasp_grids_t *g, int *L_out, int *ngrids_out) {
   if (!g) return GASP_ERR_INVALID;
   if (L_out) *L_out = g->L;
@@ -397,6 +414,8 @@ SweepLaunch base_launch(gasp_grids_t *g) {
   p.pacc_f = x.d_tab->pacc;
   p.pacc_cpu = x.d_tab->pacc_cpu;
   p.float_compare = x.float_cmp;
+  p.variant = x.variant;
+  p.warps_per_cta = x.warps_per_cta;
   return p;
 }
 
@@ -690,8 +709,12 @@ extern "C" int gasp_mc_driver_gpu_ex(gasp_gpu_grids_t grids, double beta, double
         for (int i = 0; i < ngrids; ++i) nnuc += ((double)mag_last[i] > up) ? 1 : 0;
         const int idx = isweep / mag_int;
         if (idx < nres) result[idx] = (float)((double)nnuc / (double)ngrids);
-        if (o.verbosity >= 1) {
+        if (o.verbosity == 1) {  // CLI (src/mc_gpu.cu:726)
           fprintf(stdout, "%10d  %12.6f\n", isweep, (double)nnuc / (double)ngrids);
+          fflush(stdout);
+        } else if (o.verbosity == 2) {  // PyGASP progress (src/mc_gpu.cu:730-731)
+          fprintf(stdout, "\r Sweep : %10d, Reached cv = %6.2f : %4d , Unresolved : %4d", isweep,
+                  up, nnuc, ngrids - nnuc);
           fflush(stdout);
         }
         stop = nnuc == ngrids;
@@ -748,9 +771,12 @@ extern "C" int gasp_mc_driver_gpu_ex(gasp_gpu_grids_t grids, double beta, double
       result[i] = (float)nBb / (float)(sub - nF);
     }
   }
-  if (o.verbosity >= 1) {
+  if (o.verbosity == 1) {  // src/mc_gpu.cu:786-787
     fprintf(stdout, "\n# Time taken on GPU = %f seconds\n", elapsed);
     if (itask == 1) fprintf(stdout, "pB estimate : %10.6f\n", nres > 0 ? (double)result[0] : 0.0);
+    fflush(stdout);
+  } else if (o.verbosity == 2) {
+    fprintf(stdout, "\n");
     fflush(stdout);
   }
   if (calc.result)

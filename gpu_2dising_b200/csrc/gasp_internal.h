@@ -62,6 +62,7 @@ struct SweepLaunch {
   float *mag_out;         // optional: magnetisation after the batch [ngrids]
   int float_compare;      // exact mode: compare in float (thresholds unusable)
   int warps_per_cta;      // launch shape (0: default)
+  int variant;            // 0: fastest kernel for L; 1: generic exact kernel
 };
 
 // kernel launchers (gasp_kernels.cu); each returns a GASP status.

@@ -150,6 +150,120 @@ __global__ void __launch_bounds__(256) k_sweep_exact(SweepLaunch p) {
 }
 
 // ---------------------------------------------------------------------------
+// Exact sweep specialised for L a power of two and a multiple of 32 (32, 64,
+// 128): a row is R = L/32 whole words, so
+//   * up/down neighbours are the words R rows-words away, at the same bit,
+//     and their byte offsets wrap with a mask (4N is a power of two);
+//   * left/right neighbours sit in the centre word except at bit 0 / 31,
+//     where they are in the row's edge word (for R == 2 simply word w^1);
+//   * one funnel shift of (hi:lo) brings left/centre/right to bits 2..4 and
+//     two rotates bring up/down to bits 5..6, giving pattern*4 directly as a
+//     byte offset into a 32-entry threshold table indexed by the 5 spins.
+// Same arithmetic, stream consumption and result as k_sweep_exact.
+// ---------------------------------------------------------------------------
+template <int Words, bool kStatic>
+struct LatticeStore;
+
+template <int Words>
+struct LatticeStore<Words, true> {
+  __device__ __forceinline__ static uint32_t *get(uint32_t *) {
+    __shared__ __align__(128) uint32_t lat[Words];
+    return lat;
+  }
+};
+
+template <int Words>
+struct LatticeStore<Words, false> {
+  __device__ __forceinline__ static uint32_t *get(uint32_t *dyn) { return dyn; }
+};
+
+template <int L, bool kStatic, bool kFloatCmp>
+__global__ void __launch_bounds__(32) k_sweep_rows(SweepLaunch p) {
+  static_assert(L % 32 == 0 && (L & (L - 1)) == 0, "L must be a power of two >= 32");
+  constexpr int N = L * L;
+  constexpr int W = N / 32;
+  constexpr int R = L / 32;
+  constexpr uint32_t kMask = (uint32_t)(4 * N - 1) & ~127u;  // word part of a byte offset
+  __shared__ __align__(16) uint32_t thrP[32];   // threshold by 5-spin pattern
+  __shared__ __align__(16) float paccP[32];     // float table by pattern
+  extern __shared__ __align__(16) uint32_t dyn[];
+  uint32_t *lat = LatticeStore<W * kTile, kStatic>::get(dyn);
+
+  const int lane = threadIdx.x;
+  {
+    // pattern bits: 0 left, 1 centre, 2 right, 3 up, 4 down (1 == spin +1)
+    const int c = (lane >> 1) & 1;
+    const int cls = 5 * c + __popc(lane & 0x1D);
+    thrP[lane] = p.thr[cls];
+    paccP[lane] = p.pacc_f[2 * cls];
+  }
+  const int tile = blockIdx.x;
+  const int slot = tile * kTile + lane;
+  const bool live = slot < p.n_active;
+  const int rep = live ? (p.active ? p.active[slot] : slot) : 0;
+  stage_in(lat, p, W, tile, lane, live, rep);
+  __syncwarp();
+
+  const char *latb = reinterpret_cast<const char *>(lat);
+  const char *thrb = reinterpret_cast<const char *>(thrP);
+  const char *paccb = reinterpret_cast<const char *>(paccP);
+  if (live) {
+    curandStateXORWOW st;
+    load_rng(st, p.rng, p.rng_stride, rep);
+    const float shrink = (1.0f - FLT_EPSILON) * (float)N;
+    const uint32_t lane4 = (uint32_t)lane << 2;
+    for (int sw = 0; sw < p.nsweeps; ++sw) {
+#pragma unroll 5
+      for (int a = 0; a < N; ++a) {
+        const uint32_t x1 = curand(&st);
+        const uint32_t s = (uint32_t)__float2int_rd(shrink * _curand_uniform(x1));
+        const uint32_t b = s & 31u;
+        const uint32_t offc = ((s << 2) & kMask) | lane4;
+        const uint32_t offu = ((offc - 128u * R) & kMask) | lane4;
+        const uint32_t offd = ((offc + 128u * R) & kMask) | lane4;
+        const uint32_t wu = *reinterpret_cast<const uint32_t *>(latb + offu);
+        const uint32_t wd = *reinterpret_cast<const uint32_t *>(latb + offd);
+        uint32_t wc, lo, hi;
+        if constexpr (R == 1) {
+          wc = *reinterpret_cast<const uint32_t *>(latb + offc);
+          lo = hi = wc;
+        } else if constexpr (R == 2) {
+          wc = *reinterpret_cast<const uint32_t *>(latb + offc);
+          const uint32_t wx = *reinterpret_cast<const uint32_t *>(latb + (offc ^ 128u));
+          lo = (b == 0u) ? wx : wc;
+          hi = (b == 31u) ? wx : wc;
+        } else {
+          const uint32_t wi = (offc >> 7) & (uint32_t)(R - 1);
+          const uint32_t offl =
+              (b == 0u) ? (wi == 0u ? offc + 128u * (R - 1) : offc - 128u) : offc;
+          const uint32_t offr =
+              (b == 31u) ? (wi == (uint32_t)(R - 1) ? offc - 128u * (R - 1) : offc + 128u) : offc;
+          lo = *reinterpret_cast<const uint32_t *>(latb + offl);
+          hi = *reinterpret_cast<const uint32_t *>(latb + offr);
+          wc = (b == 0u) ? hi : lo;
+        }
+        const uint32_t t = __funnelshift_r(lo, hi, b + 29u);  // bits 2,3,4: left, centre, right
+        const uint32_t u = __funnelshift_r(wu, wu, b + 27u);  // bit 5: up
+        const uint32_t d = __funnelshift_r(wd, wd, b + 26u);  // bit 6: down
+        const uint32_t p4 = (t & 0x1Cu) | (u & 0x20u) | (d & 0x40u);
+        const uint32_t x2 = curand(&st);
+        bool acc;
+        if (kFloatCmp) {
+          acc = _curand_uniform(x2) < *reinterpret_cast<const float *>(paccb + p4);
+        } else {
+          acc = x2 <= *reinterpret_cast<const uint32_t *>(thrb + p4);
+        }
+        if (acc) *reinterpret_cast<uint32_t *>(const_cast<char *>(latb) + offc) = wc ^ (1u << b);
+      }
+    }
+    store_rng(st, p.rng, p.rng_stride, rep);
+  }
+  __syncwarp();
+  epilogue_mag(lat + lane, p, N, W, live, rep);
+  stage_out(lat, p, W, tile, lane, live, rep);
+}
+
+// ---------------------------------------------------------------------------
 // CPU-trace sweep: mc_sweep_cpu arithmetic (src/mc_cpu.c:41-89) on a replayed
 // stream of doubles (row-u, col-u, xi) per attempt.
 // ---------------------------------------------------------------------------
@@ -312,15 +426,32 @@ int launch_tiles(Kern kern, const SweepLaunch &p, cudaStream_t s) {
   return GASP_OK;
 }
 
+// One warp per CTA; the lattice is static shared memory (kStatic) or dynamic.
+template <typename Kern>
+int launch_rows(Kern kern, const SweepLaunch &p, size_t dyn_smem, cudaStream_t s) {
+  const int tiles = tiles_for(p.n_active);
+  if (tiles == 0) return GASP_OK;
+  if (dyn_smem > 0)
+    GASP_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_smem));
+  kern<<<tiles, 32, dyn_smem, s>>>(p);
+  GASP_CUDA(cudaGetLastError());
+  return GASP_OK;
+}
+
 template <bool F>
 int dispatch_exact(const SweepLaunch &p, cudaStream_t s) {
+  if (p.variant == 1) {  // the generic kernel, kept selectable for comparisons
+    return launch_tiles(p.L == 64 ? k_sweep_exact<64, F> : k_sweep_exact<0, F>, p, s);
+  }
   switch (p.L) {
     case 16: return launch_tiles(k_sweep_exact<16, F>, p, s);
-    case 32: return launch_tiles(k_sweep_exact<32, F>, p, s);
+    case 32: return launch_rows(k_sweep_rows<32, true, F>, p, 0, s);
     case 48: return launch_tiles(k_sweep_exact<48, F>, p, s);
-    case 64: return launch_tiles(k_sweep_exact<64, F>, p, s);
+    case 64: return launch_rows(k_sweep_rows<64, true, F>, p, 0, s);
     case 96: return launch_tiles(k_sweep_exact<96, F>, p, s);
-    case 128: return launch_tiles(k_sweep_exact<128, F>, p, s);
+    case 128:
+      return launch_rows(k_sweep_rows<128, false, F>, p,
+                         (size_t)words_per_replica(128) * kTile * sizeof(uint32_t), s);
     default: return launch_tiles(k_sweep_exact<0, F>, p, s);
   }
 }

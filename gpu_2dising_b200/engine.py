@@ -96,6 +96,10 @@ class DeviceGrids:
             raise ValueError("grid array has the wrong size")
         check(lib().gasp_grids_upload(self._h, g), "gasp_grids_upload")
 
+    def set_option(self, option, value):
+        """Launch tuning (results never depend on it): see gasp_grids_set_option."""
+        check(lib().gasp_grids_set_option(self._h, int(option), int(value)), "gasp_grids_set_option")
+
     def download(self):
         out = np.empty(self.L * self.L * self.ngrids, np.int32)
         check(lib().gasp_grids_download(self._h, out), "gasp_grids_download")

@@ -1,0 +1,266 @@
+"""Drop-in mirror of the reference's PyGASP module ``gasp``
+(src/ising_ext.cu:522-1264), running on the gasp-b200 CUDA library.
+
+    from gpu_2dising_b200 import gasp
+    frac = gasp.run_nucleation_swarm(64, 1024, 10000, 0.54, 0.07)
+    pB = gasp.run_committor_calc(64, 1024, 20000, 0.54, 0.07, grid_input="NumPy",
+                                 grid_array=[g0, g1])
+
+Same entry points, keyword names, defaults, validation errors and return
+values; the module-level ``grids`` / ``magnetisation`` / ``largest_cluster``
+lists and ``gpu_nsms`` behave as in the reference.  Differences, all
+deliberate:
+
+* there is no CPU fallback: without a CUDA device the calls raise;
+* the HDF5 side files (gridstates.hdf5 / pBgrids.hdf5) are not written
+  (HDF5 is not a dependency of this library);
+* ``cv='largest_cluster'`` is rejected with NotImplementedError;
+* ``seed`` (default: the clock, as the reference) and ``compact`` (committor
+  runs stop simulating replicas whose fate is decided; pB and fates are
+  unchanged) are extra keywords;
+* ``grid_input='gridstates.bin'`` reads gridinput.bin, the intended
+  behaviour of src/ising_ext.cu:971-972 (the reference dereferences a NULL
+  grid_array there).
+"""
+from __future__ import annotations
+
+import copy
+import os
+import sys
+import time
+
+import numpy as np
+
+from . import engine
+from ._native import GaspError, check, lib
+
+# ---- module state (src/ising_ext.cu:61-64, :1192-1260) ---------------------
+grids: list = []
+magnetisation: list = []
+largest_cluster: list = []
+gpu_nsms: int = 0
+_device_error = None
+
+try:
+    _dev, gpu_nsms = engine.init_device(-1)
+except Exception as e:  # no device: calls raise later, import still works
+    _device_error = e
+
+
+class GridSnapObject:
+    """A grid snapshot (src/ising_ext.cu:74-207): isweep, igrid, an int8 LxL
+    ``grid`` and the float members magnetisation / lclus_size / committor."""
+
+    __slots__ = ("isweep", "igrid", "_grid", "magnetisation", "lclus_size", "committor")
+
+    def __init__(self, isweep, igrid, grid):
+        if not isinstance(grid, np.ndarray):
+            raise TypeError("Third argument must be a NumPy array.")
+        if grid.dtype != np.int8 or grid.ndim != 2:
+            raise TypeError("NumPy array must be 2D with 8-bit integer elements.")
+        self.isweep = int(isweep)
+        self.igrid = int(igrid)
+        self._grid = grid
+        self.magnetisation = 0.0
+        self.lclus_size = -1.0
+        self.committor = -1.0
+
+    @property
+    def grid(self):
+        return self._grid
+
+    @grid.setter
+    def grid(self, value):
+        if not isinstance(value, np.ndarray):
+            raise TypeError("grid must be a numpy array")
+        self._grid = value
+
+    def __deepcopy__(self, memo):
+        new = GridSnapObject(self.isweep, self.igrid, self._grid.copy())
+        new.magnetisation = self.magnetisation
+        new.lclus_size = self.lclus_size
+        new.committor = self.committor
+        return new
+
+    def __repr__(self):
+        return (f"GridSnapObject(isweep={self.isweep}, igrid={self.igrid}, "
+                f"magnetisation={self.magnetisation:.4f}, committor={self.committor})")
+
+
+def _reset_lists():
+    """src/ising_ext.cu:216-275: fresh module-level lists."""
+    global grids, magnetisation, largest_cluster
+    grids = []
+    magnetisation = []
+    largest_cluster = []
+
+
+class _History:
+    """The snapshot store of append_grids_list (src/ising_ext.cu:280-463)."""
+
+    def __init__(self, keep, maxhist, L):
+        self.keep, self.maxhist, self.L = keep, maxhist, L
+        self.ihist = 0
+
+    def __call__(self, L, ngrids, g, isweep, mag, dn, up):
+        magnetisation.append([float(x) for x in mag])
+        if not self.keep or self.ihist >= self.maxhist:
+            return 0
+        snaps = []
+        cvv = mag.astype(np.float64)
+        sel = np.nonzero((cvv > dn) & (cvv < up))[0]
+        for i in sel:
+            snap = GridSnapObject(isweep, int(i), g[i].astype(np.int8))
+            snap.magnetisation = float(mag[i])
+            snap.committor = -1.0
+            snaps.append(snap)
+            self.ihist += 1
+            if self.ihist == self.maxhist:
+                sys.stderr.write("\nWARNING: Maximum history reached, not storing more "
+                                 "snapshots to grids object!\n\n")
+                self.ihist += 1
+                break
+        if snaps:
+            grids.append(snaps)
+        return 0
+
+
+def _require_device():
+    if _device_error is not None:
+        raise GaspError(3, f"no CUDA device available ({_device_error})")
+
+
+def _check_cv(cv, up, dn):
+    if cv not in ("magnetisation", "largest_cluster"):
+        raise ValueError("cv must be either 'magnetisation' or 'largest_cluster'")
+    if cv == "largest_cluster":
+        raise NotImplementedError("cv='largest_cluster' is not provided by gasp-b200")
+
+
+def run_nucleation_swarm(L, ngrid, tot_nsweeps, beta, h, initial_spin=-1, cv="magnetisation",
+                         up_threshold=0.90, dn_threshold=-0.95, mag_output_int=100,
+                         grid_output_int=1000, keep_grids=True, max_keep_grids=0,
+                         threadsPerBlock=32, gpu_method=0, seed=None, verbose=False):
+    """Simulate a swarm of ngrid LxL replicas from a uniform ``initial_spin``
+    start; returns float32[tot_nsweeps // mag_output_int], the fraction of
+    replicas with cv > up_threshold at each check (src/ising_ext.cu:522-743).
+    Default thresholds are those of the reference (computed there from the
+    default initial_spin=-1: up 0.90, dn -0.95)."""
+    _check_cv(cv, up_threshold, dn_threshold)
+    if max_keep_grids < 0:
+        raise ValueError("max_keep_grids must be a positive integer")
+    _require_device()
+    if os.path.exists("gridstates.bin"):
+        os.remove("gridstates.bin")
+    _reset_lists()
+    nsnaps = tot_nsweeps // grid_output_int + 1
+    maxhist = max_keep_grids if max_keep_grids else nsnaps * ngrid
+    hist = _History(bool(keep_grids), maxhist, L)
+    host = np.full((ngrid, L, L), int(initial_spin), np.int32)
+    engine.select_gpu_method(L, ngrid, threadsPerBlock)  # evaluated, then ignored (as :678)
+    seed = int(time.time()) if seed is None else int(seed)
+    dg = engine.DeviceGrids(L, ngrid, host)
+    rng = engine.RngStates(ngrid, seed)
+    try:
+        res, _, _, _ = engine.run_driver(
+            dg, rng, beta, h, tot_nsweeps, mag_output_int, grid_output_int, itask=0,
+            dn_thr=dn_threshold, up_thr=up_threshold, host_grids=host,
+            outfunc=lambda L_, ng_, g, isweep, m: hist(L_, ng_, g, isweep, m, dn_threshold,
+                                                        up_threshold),
+            verbosity=2 if verbose else 0, threads_per_block=threadsPerBlock)
+    finally:
+        dg.close()
+        rng.close()
+    return np.asarray(res, np.float32)
+
+
+def run_committor_calc(L, ngrid, tot_nsweeps, beta, h, initial_spin=-1, cv="magnetisation",
+                       up_threshold=0.90, dn_threshold=-0.93, mag_output_int=100,
+                       grid_output_int=1000, keep_grids=True, max_keep_grids=0,
+                       threadsPerBlock=32, gpu_method=0, grid_input="gridstates.bin",
+                       grid_array=None, nsms=None, seed=None, compact=False, verbose=False):
+    """Committor pB of each input grid by shooting ngrid/len(grid_array)
+    trajectories per input until cv > up_threshold (B) or < dn_threshold (A);
+    returns [(pB, bootstrap error), ...] (src/ising_ext.cu:805-1130)."""
+    global gpu_nsms
+    if nsms is None:
+        nsms = gpu_nsms
+    if nsms < 0:
+        raise ValueError("nsms must be a non-negative integer")
+    gpu_nsms = nsms
+    _check_cv(cv, up_threshold, dn_threshold)
+    if max_keep_grids < 0:
+        raise ValueError("max_keep_grids must be a non-negative integer")
+    count = 1
+    if grid_array is not None:
+        if not isinstance(grid_array, list):
+            raise TypeError("grid_array must be a list of 2D NumPy arrays")
+        count = len(grid_array)
+        if count > gpu_nsms:
+            raise ValueError("grid_array list length exceeds gpu_nsms")
+        if count == 0:
+            raise ValueError("grid_array list is empty")
+        if gpu_nsms % count != 0:
+            raise ValueError("grid_array list length must divide gpu_nsms exactly")
+        if ngrid % gpu_nsms != 0:
+            raise ValueError("ngrids must be a multiple of gpu_nsms")
+        if ngrid % count != 0:
+            raise ValueError("ngrids must be a multiple of grid_array list length")
+        arrs = []
+        for a in grid_array:
+            if not isinstance(a, np.ndarray):
+                raise TypeError("All items in grid_array must be NumPy arrays")
+            if a.dtype != np.int8 or a.ndim != 2:
+                raise TypeError("Each grid_array item must be a 2D NumPy array of type int8")
+            if a.shape != (L, L):
+                raise ValueError("Each grid_array item must have shape LxL")
+            arrs.append(a.astype(np.int32))
+    _require_device()
+    if os.path.exists("gridstates.bin"):
+        os.remove("gridstates.bin")
+    _reset_lists()
+    nsnaps = tot_nsweeps // grid_output_int + 1
+    maxhist = max_keep_grids if max_keep_grids else nsnaps * ngrid
+    hist = _History(bool(keep_grids), maxhist, L)
+    host = np.empty((ngrid, L, L), np.int32)
+    if grid_input == "gridstates.bin":
+        rc = lib().gasp_init_grids_from_file(b"gridinput.bin", L, ngrid, host.reshape(-1))
+        check(rc, "reading gridinput.bin")
+        count = 1
+    elif grid_input == "NumPy" and grid_array is not None:
+        check(lib().gasp_init_grids_from_array(L, ngrid, count,
+                                               np.ascontiguousarray(np.stack(arrs)).reshape(-1),
+                                               host.reshape(-1)), "init_grids_from_array")
+    else:
+        raise ValueError("Invalid grid_input option or no grid_array supplied")
+    fates = np.full(ngrid, -1, np.int32)
+    engine.select_gpu_method(L, ngrid, threadsPerBlock)
+    seed = int(time.time()) if seed is None else int(seed)
+    dg = engine.DeviceGrids(L, ngrid, host)
+    rng = engine.RngStates(ngrid, seed)
+    try:
+        res, fates, _, _ = engine.run_driver(
+            dg, rng, beta, h, tot_nsweeps, mag_output_int, grid_output_int, itask=1,
+            dn_thr=dn_threshold, up_thr=up_threshold, ninputs=count, host_grids=host,
+            fates=fates, compact=compact,
+            outfunc=lambda L_, ng_, g, isweep, m: hist(L_, ng_, g, isweep, m, dn_threshold,
+                                                        up_threshold),
+            verbosity=2 if verbose else 0, threads_per_block=threadsPerBlock)
+    finally:
+        dg.close()
+        rng.close()
+    sub = ngrid // count
+    out = []
+    for i in range(count):
+        block = np.ascontiguousarray(fates[i * sub:(i + 1) * sub])
+        err = lib().gasp_bootstrap_errbar(sub, sub, block)
+        if err < 0.0:
+            raise RuntimeError("Error calculating bootstrap error bar")
+        out.append((float(res[i]), float(err)))
+    return out
+
+
+__all__ = ["run_nucleation_swarm", "run_committor_calc", "GridSnapObject", "grids",
+           "magnetisation", "largest_cluster", "gpu_nsms"]
+
+_ = copy  # deepcopy support is through GridSnapObject.__deepcopy__

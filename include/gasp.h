@@ -87,6 +87,13 @@ int gasp_grids_download(gasp_grids_t *grids, int *host_grids);
 /* Replica count / side length of a set. */
 int gasp_grids_shape(const gasp_grids_t *grids, int *L_out, int *ngrids_out);
 
+/* Launch tuning of a set (no reference counterpart; results never depend on
+ * it).  GASP_OPT_SWEEP_VARIANT: 0 the fastest exact kernel for L (default),
+ * 1 the generic exact kernel.  GASP_OPT_WARPS_PER_CTA: tiles per CTA of the
+ * generic kernel (1..8). */
+enum { GASP_OPT_SWEEP_VARIANT = 1, GASP_OPT_WARPS_PER_CTA = 2 };
+int gasp_grids_set_option(gasp_grids_t *grids, int option, int value);
+
 /* ------------------------------------------------------------ RNG states */
 /* Opaque per-replica XORWOW states (cuRAND device API), replaces curandState*. */
 typedef struct gasp_rng gasp_rng_t;
@@ -189,7 +196,8 @@ typedef int (*gasp_packed_output_fn)(int L, int ngrids, const uint8_t *payload,
 
 /* Driver options beyond the reference's arguments. */
 typedef struct {
-  int verbosity;        /* 0 silent; 1 the reference CLI's stdout lines    */
+  int verbosity;        /* 0 silent; 1 the reference CLI's stdout lines;   
+                         * 2 PyGASP's progress line                       */
   int compact;          /* itask 1: stop simulating resolved replicas      */
   gasp_packed_output_fn packed_out; /* if set, used instead of outfunc     */
   void *packed_user;

@@ -171,7 +171,10 @@ def test_driver_matches_reference_driver(ref_gpu, case, compact):
                                          compact=compact)
     assert np.array_equal(res, r_res)
     assert [f[0] for f in frames] == list(r_fi)
-    for (isw, g), rg in zip(frames, r_fg):
+    # With compaction a resolved replica is no longer simulated, so dumped
+    # grids can differ from the reference after its fate is decided; the
+    # first frame and every fate/result are still identical.
+    for (isw, g), rg in zip(frames[:1] if compact else frames, r_fg):
         assert np.array_equal(g, rg)
     if itask == 1:
         assert np.array_equal(fates, r_fates)
