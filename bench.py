@@ -190,7 +190,7 @@ def run_e2e(args, rank, world, dist, torch, engine):
     t0 = time.perf_counter()
     dg2 = engine.DeviceGrids(L, R, host)
     t1 = time.perf_counter()
-    rng2 = engine.RngStates(R, SEED + 7919 * rank + 1)
+    rng2 = engine.RngStates(R, SEED + 7919 * rank + 1, kind=args.rng)
     t2 = time.perf_counter()
     _, _, drv_s, attempts = engine.run_driver(dg2, rng2, BETA, H, SWEEPS_PER_STEP * args.steps,
                                           MAG_INT, GRID_INT, itask=0, dn_thr=-0.9, up_thr=0.9,
@@ -231,7 +231,7 @@ def run_ours(args, rank, world, local_rank):
 
     dg = engine.DeviceGrids(L, R, -np.ones((R, L, L), np.int32))
     dg.set_option(1, args.variant)  # GASP_OPT_SWEEP_VARIANT
-    rng = engine.RngStates(R, SEED + 7919 * rank)
+    rng = engine.RngStates(R, SEED + 7919 * rank, kind=args.rng)
 
     def barrier():
         torch.cuda.synchronize()
@@ -281,6 +281,9 @@ def run_ours(args, rank, world, local_rank):
             if c is not None:
                 cpu = {"value": c[0], "unit": UNIT, "cores": c[1], "kind": "reference",
                        "sample": c[2]}
+        if args.rng != "xorwow":
+            CONFIG["rng"] = "MWC64X production stream (statistically equivalent, not bit-exact)"
+            CONFIG["workload"] = CONFIG["workload"].replace("gpu_method 2 exact", "production RNG")
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max / args.steps,
@@ -314,6 +317,8 @@ def main():
     ap.add_argument("--sweeps-per-step", type=int, default=SWEEPS_PER_STEP,
                     help="smaller values give a short launch for ncu captures")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--rng", default="xorwow", choices=["xorwow", "mwc64x"],
+                    help="xorwow: the reference stream (bit-exact); mwc64x: production stream")
     ap.add_argument("--variant", type=int, default=0,
                     help="sweep kernel variant (0 fastest for L, 1 generic) for comparisons")
     args = ap.parse_args()

@@ -28,6 +28,9 @@ GASP_ERR_TIMEOUT = 9
 OPT_SWEEP_VARIANT = 1
 OPT_WARPS_PER_CTA = 2
 
+RNG_XORWOW = 0
+RNG_MWC64X = 1
+
 MODE_EXACT = 0
 MODE_TRACE_CPU = 1
 
@@ -37,7 +40,7 @@ EXPORTED = (
     "gasp_select_gpu_method", "gasp_acceptance_table", "gasp_max_shared_L",
     "gasp_set_stream", "gasp_init_grid", "gasp_free_grid", "gasp_grids_upload",
     "gasp_grids_download", "gasp_grids_shape", "gasp_grids_set_option", "gasp_init_rand",
-    "gasp_free_rand",
+    "gasp_init_rand_mode", "gasp_mwc64x_seed_states", "gasp_free_rand",
     "gasp_sweep", "gasp_sweep_trace_cpu", "gasp_magnetisation", "gasp_pack_frame",
     "gasp_frame_bytes", "gasp_mc_driver_gpu", "gasp_mc_driver_gpu_ex",
     "gasp_init_grids_uniform", "gasp_init_grids_from_file", "gasp_init_grids_from_array",
@@ -88,7 +91,8 @@ PACKED_OUTPUT_FN = C.CFUNCTYPE(C.c_int, C.c_int, C.c_int, C.POINTER(C.c_uint8), 
 class DriverOptsT(C.Structure):
     _fields_ = [("verbosity", C.c_int), ("compact", C.c_int),
                 ("packed_out", PACKED_OUTPUT_FN), ("packed_user", C.c_void_p),
-                ("elapsed_s", C.POINTER(C.c_double)), ("attempts", C.POINTER(C.c_longlong))]
+                ("elapsed_s", C.POINTER(C.c_double)), ("attempts", C.POINTER(C.c_longlong)),
+                ("first_up", C.POINTER(C.c_int))]
 
 
 _i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
@@ -116,6 +120,9 @@ def _bind(lib):
         "gasp_grids_shape": (I, [P, C.POINTER(I), C.POINTER(I)]),
         "gasp_grids_set_option": (I, [P, I, I]),
         "gasp_init_rand": (I, [I, I, C.c_ulonglong, C.POINTER(P)]),
+        "gasp_init_rand_mode": (I, [I, I, C.c_ulonglong, I, C.POINTER(P)]),
+        "gasp_mwc64x_seed_states": (I, [C.c_ulonglong, I, I,
+                                        np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")]),
         "gasp_free_rand": (I, [P]),
         "gasp_sweep": (I, [P, P, C.c_double, C.c_double, I, I]),
         "gasp_sweep_trace_cpu": (I, [P, _f64p, C.c_double, C.c_double, I]),

@@ -357,11 +357,62 @@ int gasp_grids_shape(const gasp_grids_t *g, int *L_out, int *ngrids_out) {
   return GASP_OK;
 }
 
-int gasp_init_rand(int ngrids, int threads_per_block, unsigned long long seed,
-                   gasp_rng_t **rng_out) {
+}  // extern "C"
+
+namespace {
+
+uint64_t splitmix64(uint64_t &z) {
+  // Steele, Lea & Flood (2014) SplitMix64 finaliser, used only to spread the
+  // user's seed over the MWC64X state space.
+  uint64_t v = (z += 0x9E3779B97F4A7C15ull);
+  v = (v ^ (v >> 30)) * 0xBF58476D1CE4E5B9ull;
+  v = (v ^ (v >> 27)) * 0x94D049BB133111EBull;
+  return v ^ (v >> 31);
+}
+
+uint64_t mulmod64(uint64_t a, uint64_t b, uint64_t m) {
+  return (uint64_t)((unsigned __int128)a * b % m);
+}
+
+uint64_t powmod64(uint64_t a, uint64_t e, uint64_t m) {
+  uint64_t r = 1 % m;
+  a %= m;
+  while (e) {
+    if (e & 1) r = mulmod64(r, a, m);
+    a = mulmod64(a, a, m);
+    e >>= 1;
+  }
+  return r;
+}
+
+// MWC64X states for ngrids replicas: the seed picks a base state X0 in
+// [1, M-1]; replica r starts at X0 * A^(r * 2^40) mod M, i.e. 2^40 draws
+// after replica r-1 (a run uses < 2^32 draws per replica, so streams never
+// overlap).  Layout: x at [r], c at [stride + r].
+void mwc_seed_states(uint64_t seed, int ngrids, int stride, std::vector<uint32_t> &out) {
+  const uint64_t A = kMwcA;
+  const uint64_t M = (A << 32) - 1;
+  uint64_t z = seed;
+  const uint64_t X0 = 1 + splitmix64(z) % (M - 1);
+  const uint64_t P = powmod64(A, 1ull << 40, M);
+  out.assign((size_t)kMwcWords * stride, 0u);
+  uint64_t X = X0;
+  for (int r = 0; r < ngrids; ++r) {
+    out[r] = (uint32_t)(X / A);
+    out[(size_t)stride + r] = (uint32_t)(X % A);
+    X = mulmod64(X, P, M);
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int gasp_init_rand_mode(int ngrids, int threads_per_block, unsigned long long seed, int kind,
+                        gasp_rng_t **rng_out) {
   (void)threads_per_block;
-  if (!rng_out || ngrids <= 0) {
-    set_error("gasp_init_rand: ngrids must be positive and rng_out non-NULL");
+  if (!rng_out || ngrids <= 0 || (kind != GASP_RNG_XORWOW && kind != GASP_RNG_MWC64X)) {
+    set_error("gasp_init_rand: ngrids must be positive, kind valid and rng_out non-NULL");
     return GASP_ERR_INVALID;
   }
   *rng_out = nullptr;
@@ -370,14 +421,25 @@ int gasp_init_rand(int ngrids, int threads_per_block, unsigned long long seed,
   cudaError_t e = cudaGetDevice(&r->device);
   r->ngrids = ngrids;
   r->stride = tiles_for(ngrids) * kTile;
+  r->kind = kind == GASP_RNG_MWC64X ? kRngMwc : kRngXorwow;
+  const int words = r->kind == kRngMwc ? kMwcWords : kRngWords;
   if (e == cudaSuccess)
-    e = cudaMalloc(&r->d_state, (size_t)kRngWords * r->stride * sizeof(uint32_t));
+    e = cudaMalloc(&r->d_state, (size_t)words * r->stride * sizeof(uint32_t));
   if (e != cudaSuccess) {
     delete r;
     return cuda_fail(e, "gasp_init_rand allocation", __FILE__, __LINE__);
   }
   cudaStream_t s = current_stream();
-  int rc = launch_rng_init(r->d_state, ngrids, r->stride, seed, s);
+  int rc = GASP_OK;
+  std::vector<uint32_t> host;
+  if (r->kind == kRngMwc) {
+    mwc_seed_states(seed, ngrids, r->stride, host);
+    e = cudaMemcpyAsync(r->d_state, host.data(), host.size() * sizeof(uint32_t),
+                        cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) rc = cuda_fail(e, "gasp_init_rand upload", __FILE__, __LINE__);
+  } else {
+    rc = launch_rng_init(r->d_state, ngrids, r->stride, seed, s);
+  }
   if (rc == GASP_OK) {
     e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) rc = cuda_fail(e, "gasp_init_rand", __FILE__, __LINE__);
@@ -389,6 +451,19 @@ int gasp_init_rand(int ngrids, int threads_per_block, unsigned long long seed,
   }
   *rng_out = r;
   return GASP_OK;
+}
+
+int gasp_mwc64x_seed_states(unsigned long long seed, int ngrids, int stride, uint32_t *out) {
+  if (!out || ngrids <= 0 || stride < ngrids) return GASP_ERR_INVALID;
+  std::vector<uint32_t> host;
+  mwc_seed_states(seed, ngrids, stride, host);
+  memcpy(out, host.data(), host.size() * sizeof(uint32_t));
+  return GASP_OK;
+}
+
+int gasp_init_rand(int ngrids, int threads_per_block, unsigned long long seed,
+                   gasp_rng_t **rng_out) {
+  return gasp_init_rand_mode(ngrids, threads_per_block, seed, GASP_RNG_XORWOW, rng_out);
 }
 
 int gasp_free_rand(gasp_rng_t *r) {
@@ -451,6 +526,7 @@ int gasp_sweep(gasp_grids_t *g, gasp_rng_t *r, double beta, double h, int nsweep
   SweepLaunch p = base_launch(g);
   p.rng = r->d_state;
   p.rng_stride = r->stride;
+  p.rng_kind = r->kind;
   p.nsweeps = nsweeps;
   p.mag_out = g->d_mag;
   return launch_sweep_exact(p, current_stream());
@@ -619,6 +695,7 @@ extern "C" int gasp_mc_driver_gpu_ex(gasp_gpu_grids_t grids, double beta, double
   SweepLaunch p = base_launch(g);
   p.rng = r->d_state;
   p.rng_stride = r->stride;
+  p.rng_kind = r->kind;
   p.nsweeps = spc;
 
   long long attempts = 0;
@@ -626,6 +703,8 @@ extern "C" int gasp_mc_driver_gpu_ex(gasp_gpu_grids_t grids, double beta, double
   const auto t0 = std::chrono::steady_clock::now();
   if ((rc = launch_measure(g->d_lat, L, ngrids, d_mag_cur, s))) return rc;
 
+  if (o.first_up)
+    for (int i = 0; i < ngrids; ++i) o.first_up[i] = -1;
   int isweep = 0;
   bool have_frame = false;
   while (isweep < tot) {
@@ -707,6 +786,9 @@ extern "C" int gasp_mc_driver_gpu_ex(gasp_gpu_grids_t grids, double beta, double
       if (itask == 0) {
         int nnuc = 0;
         for (int i = 0; i < ngrids; ++i) nnuc += ((double)mag_last[i] > up) ? 1 : 0;
+        if (o.first_up)
+          for (int i = 0; i < ngrids; ++i)
+            if (o.first_up[i] < 0 && (double)mag_last[i] > up) o.first_up[i] = isweep;
         const int idx = isweep / mag_int;
         if (idx < nres) result[idx] = (float)((double)nnuc / (double)ngrids);
         if (o.verbosity == 1) {  // CLI (src/mc_gpu.cu:726)

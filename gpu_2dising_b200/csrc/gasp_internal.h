@@ -26,6 +26,15 @@ inline int tiles_for(int ngrids) { return (ngrids + kTile - 1) / kTile; }
 // replica r at state[k * stride + r], k = 0 (d), 1..5 (v[0..4]).
 constexpr int kRngWords = 6;
 
+// Production RNG: MWC64X (D. B. Thomas, "The MWC64X random number generator",
+// 2011): state (x, c), step t = A*x + c, x' = t mod 2^32, c' = t >> 32,
+// output x ^ c.  Equivalent to X -> X*A mod M with X = x*A + c and
+// M = A*2^32 - 1, which gives the skip-ahead used to start replica r's stream
+// r * 2^40 draws after the seed's base state (non-overlapping substreams).
+constexpr uint32_t kMwcA = 4294883355u;
+constexpr int kMwcWords = 2;  // SoA: x at [0*stride + r], c at [1*stride + r]
+enum RngKind { kRngXorwow = 0, kRngMwc = 1 };
+
 void set_error(const char *fmt, ...);
 int cuda_fail(cudaError_t e, const char *what, const char *file, int line);
 
@@ -63,6 +72,7 @@ struct SweepLaunch {
   int float_compare;      // exact mode: compare in float (thresholds unusable)
   int warps_per_cta;      // launch shape (0: default)
   int variant;            // 0: fastest kernel for L; 1: generic exact kernel
+  int rng_kind;           // RngKind of p.rng
 };
 
 // kernel launchers (gasp_kernels.cu); each returns a GASP status.
@@ -93,5 +103,6 @@ struct gasp_grids {
 struct gasp_rng {
   int device;
   int ngrids, stride;
-  uint32_t *d_state;     // kRngWords * stride
+  int kind;              // gasp::RngKind
+  uint32_t *d_state;     // kRngWords (XORWOW) or kMwcWords (MWC64X) * stride
 };

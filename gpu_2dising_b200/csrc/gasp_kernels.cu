@@ -48,6 +48,59 @@ __device__ __forceinline__ void store_rng(const curandStateXORWOW &st, uint32_t 
   for (int k = 0; k < 5; ++k) rng[(k + 1) * stride + rep] = st.v[k];
 }
 
+// RNG policies of the sweep kernels.
+//   RngXorwow: the reference stream (cuRAND XORWOW, curand_uniform site
+//              arithmetic of src/mc_gpu.cu:311,317).
+//   RngMwc:    the production stream (MWC64X, two instructions per 32-bit
+//              draw; site = the draw's top bits scaled to [0, N)).
+template <int kKind>
+struct RngPolicy;
+
+template <>
+struct RngPolicy<kRngXorwow> {
+  curandStateXORWOW st;
+  __device__ __forceinline__ void load(const uint32_t *rng, int stride, int rep) {
+    load_rng(st, rng, stride, rep);
+  }
+  __device__ __forceinline__ void store(uint32_t *rng, int stride, int rep) const {
+    store_rng(st, rng, stride, rep);
+  }
+  __device__ __forceinline__ uint32_t next() { return curand(&st); }
+  template <int N>
+  __device__ __forceinline__ uint32_t site(float shrink, int /*n_runtime*/) {
+    return (uint32_t)__float2int_rd(shrink * _curand_uniform(curand(&st)));
+  }
+};
+
+template <>
+struct RngPolicy<kRngMwc> {
+  uint32_t x, c;
+  __device__ __forceinline__ void load(const uint32_t *rng, int stride, int rep) {
+    x = rng[rep];
+    c = rng[stride + rep];
+  }
+  __device__ __forceinline__ void store(uint32_t *rng, int stride, int rep) const {
+    rng[rep] = x;
+    rng[stride + rep] = c;
+  }
+  __device__ __forceinline__ uint32_t next() {
+    const uint32_t r = x ^ c;
+    const unsigned long long t = (unsigned long long)x * kMwcA + c;
+    x = (uint32_t)t;
+    c = (uint32_t)(t >> 32);
+    return r;
+  }
+  template <int N>
+  __device__ __forceinline__ uint32_t site(float, int n_runtime) {
+    const uint32_t r = next();
+    if constexpr (N > 0 && (N & (N - 1)) == 0) {
+      return r >> (32 - __builtin_ctz((unsigned)N));
+    } else {
+      return __umulhi(r, (uint32_t)(N > 0 ? N : n_runtime));
+    }
+  }
+};
+
 // Shared-memory staging of one tile (identity order) or of 32 listed replicas.
 __device__ __forceinline__ void stage_in(uint32_t *lat_s, const SweepLaunch &p, int W,
                                          int tile, int lane, bool live, int rep) {
@@ -88,7 +141,7 @@ __device__ __forceinline__ void epilogue_mag(const uint32_t *my, const SweepLaun
 // ---------------------------------------------------------------------------
 // Exact sweep.  L_ > 0: compile-time side length; L_ == 0: runtime p.L.
 // ---------------------------------------------------------------------------
-template <int L_, bool kFloatCmp>
+template <int L_, bool kFloatCmp, int kRng>
 __global__ void __launch_bounds__(256) k_sweep_exact(SweepLaunch p) {
   const int L = L_ > 0 ? L_ : p.L;
   const int N = L * L;
@@ -115,13 +168,12 @@ __global__ void __launch_bounds__(256) k_sweep_exact(SweepLaunch p) {
 
   uint32_t *my = lat_s + lane;
   if (live) {
-    curandStateXORWOW st;
-    load_rng(st, p.rng, p.rng_stride, rep);
+    RngPolicy<kRng> rg;
+    rg.load(p.rng, p.rng_stride, rep);
     const float shrink = (1.0f - FLT_EPSILON) * (float)N;
     for (int sw = 0; sw < p.nsweeps; ++sw) {
       for (int a = 0; a < N; ++a) {
-        const uint32_t x1 = curand(&st);
-        const int s = __float2int_rd(shrink * _curand_uniform(x1));
+        const int s = (int)rg.template site<(L_ > 0 ? L_ * L_ : 0)>(shrink, N);
         const int row = s / L;
         const int col = s - row * L;
         const int su = row == 0 ? s + N - L : s - L;
@@ -132,7 +184,7 @@ __global__ void __launch_bounds__(256) k_sweep_exact(SweepLaunch p) {
         const uint32_t bs = (wc >> (s & 31)) & 1u;
         const uint32_t k = bit_at(my, su) + bit_at(my, sd) + bit_at(my, sl) + bit_at(my, sr);
         const uint32_t cls = 5u * bs + k;
-        const uint32_t x2 = curand(&st);
+        const uint32_t x2 = rg.next();
         bool acc;
         if (kFloatCmp) {
           acc = _curand_uniform(x2) < pacc_s[2 * cls];  // index 10*bs + 2k
@@ -142,7 +194,7 @@ __global__ void __launch_bounds__(256) k_sweep_exact(SweepLaunch p) {
         if (acc) my[(s >> 5) * kTile] = wc ^ (1u << (s & 31));
       }
     }
-    store_rng(st, p.rng, p.rng_stride, rep);
+    rg.store(p.rng, p.rng_stride, rep);
   }
   __syncwarp();
   epilogue_mag(my, p, N, W, live, rep);
@@ -177,13 +229,62 @@ struct LatticeStore<Words, false> {
   __device__ __forceinline__ static uint32_t *get(uint32_t *dyn) { return dyn; }
 };
 
-template <int L, bool kStatic, bool kFloatCmp>
+// One attempt of k_sweep_rows on site s.  kLookahead: also draw the next
+// attempt's site (after this attempt's acceptance draw, as the reference's
+// stream order requires) so its conversion overlaps this attempt's
+// shared-memory round trips.
+template <int L, bool kFloatCmp, bool kLookahead, typename Rng>
+__device__ __forceinline__ void row_attempt(uint32_t &s, Rng &rg, const char *latb,
+                                            const char *thrb, const char *paccb, uint32_t lane4,
+                                            float shrink) {
+  constexpr int N = L * L;
+  constexpr int R = L / 32;
+  constexpr uint32_t kMask = (uint32_t)(4 * N - 1) & ~127u;  // word part of a byte offset
+  const uint32_t b = s & 31u;
+  const uint32_t offc = ((s << 2) & kMask) | lane4;
+  const uint32_t offu = ((offc - 128u * R) & kMask) | lane4;
+  const uint32_t offd = ((offc + 128u * R) & kMask) | lane4;
+  const uint32_t wu = *reinterpret_cast<const uint32_t *>(latb + offu);
+  const uint32_t wd = *reinterpret_cast<const uint32_t *>(latb + offd);
+  uint32_t wc, lo, hi;
+  if constexpr (R == 1) {
+    wc = *reinterpret_cast<const uint32_t *>(latb + offc);
+    lo = hi = wc;
+  } else if constexpr (R == 2) {
+    wc = *reinterpret_cast<const uint32_t *>(latb + offc);
+    const uint32_t wx = *reinterpret_cast<const uint32_t *>(latb + (offc ^ 128u));
+    lo = (b == 0u) ? wx : wc;
+    hi = (b == 31u) ? wx : wc;
+  } else {
+    const uint32_t wi = (offc >> 7) & (uint32_t)(R - 1);
+    const uint32_t offl = (b == 0u) ? (wi == 0u ? offc + 128u * (R - 1) : offc - 128u) : offc;
+    const uint32_t offr =
+        (b == 31u) ? (wi == (uint32_t)(R - 1) ? offc - 128u * (R - 1) : offc + 128u) : offc;
+    lo = *reinterpret_cast<const uint32_t *>(latb + offl);
+    hi = *reinterpret_cast<const uint32_t *>(latb + offr);
+    wc = (b == 0u) ? hi : lo;
+  }
+  const uint32_t t = __funnelshift_r(lo, hi, b + 29u);  // bits 2,3,4: left, centre, right
+  const uint32_t u = __funnelshift_r(wu, wu, b + 27u);  // bit 5: up
+  const uint32_t d = __funnelshift_r(wd, wd, b + 26u);  // bit 6: down
+  const uint32_t p4 = (t & 0x1Cu) | (u & 0x20u) | (d & 0x40u);
+  const uint32_t x2 = rg.next();
+  const uint32_t sc = s;
+  if constexpr (kLookahead) s = rg.template site<N>(shrink, N);
+  bool acc;
+  if constexpr (kFloatCmp) {
+    acc = _curand_uniform(x2) < *reinterpret_cast<const float *>(paccb + p4);
+  } else {
+    acc = x2 <= *reinterpret_cast<const uint32_t *>(thrb + p4);
+  }
+  if (acc) *reinterpret_cast<uint32_t *>(const_cast<char *>(latb) + offc) = wc ^ (1u << (sc & 31u));
+}
+
+template <int L, bool kStatic, bool kFloatCmp, int kRng>
 __global__ void __launch_bounds__(32) k_sweep_rows(SweepLaunch p) {
   static_assert(L % 32 == 0 && (L & (L - 1)) == 0, "L must be a power of two >= 32");
   constexpr int N = L * L;
   constexpr int W = N / 32;
-  constexpr int R = L / 32;
-  constexpr uint32_t kMask = (uint32_t)(4 * N - 1) & ~127u;  // word part of a byte offset
   __shared__ __align__(16) uint32_t thrP[32];   // threshold by 5-spin pattern
   __shared__ __align__(16) float paccP[32];     // float table by pattern
   extern __shared__ __align__(16) uint32_t dyn[];
@@ -207,56 +308,20 @@ __global__ void __launch_bounds__(32) k_sweep_rows(SweepLaunch p) {
   const char *latb = reinterpret_cast<const char *>(lat);
   const char *thrb = reinterpret_cast<const char *>(thrP);
   const char *paccb = reinterpret_cast<const char *>(paccP);
-  if (live) {
-    curandStateXORWOW st;
-    load_rng(st, p.rng, p.rng_stride, rep);
+  if (live && p.nsweeps > 0) {
+    RngPolicy<kRng> rg;
+    rg.load(p.rng, p.rng_stride, rep);
     const float shrink = (1.0f - FLT_EPSILON) * (float)N;
     const uint32_t lane4 = (uint32_t)lane << 2;
-    for (int sw = 0; sw < p.nsweeps; ++sw) {
+    // Software pipeline over the batch's attempts; draw order x1(a), x2(a),
+    // x1(a+1), ... as in the reference.  The host keeps N*nsweeps < 2^31.
+    uint32_t s = rg.template site<N>(shrink, N);
+    const int total = N * p.nsweeps;
 #pragma unroll 5
-      for (int a = 0; a < N; ++a) {
-        const uint32_t x1 = curand(&st);
-        const uint32_t s = (uint32_t)__float2int_rd(shrink * _curand_uniform(x1));
-        const uint32_t b = s & 31u;
-        const uint32_t offc = ((s << 2) & kMask) | lane4;
-        const uint32_t offu = ((offc - 128u * R) & kMask) | lane4;
-        const uint32_t offd = ((offc + 128u * R) & kMask) | lane4;
-        const uint32_t wu = *reinterpret_cast<const uint32_t *>(latb + offu);
-        const uint32_t wd = *reinterpret_cast<const uint32_t *>(latb + offd);
-        uint32_t wc, lo, hi;
-        if constexpr (R == 1) {
-          wc = *reinterpret_cast<const uint32_t *>(latb + offc);
-          lo = hi = wc;
-        } else if constexpr (R == 2) {
-          wc = *reinterpret_cast<const uint32_t *>(latb + offc);
-          const uint32_t wx = *reinterpret_cast<const uint32_t *>(latb + (offc ^ 128u));
-          lo = (b == 0u) ? wx : wc;
-          hi = (b == 31u) ? wx : wc;
-        } else {
-          const uint32_t wi = (offc >> 7) & (uint32_t)(R - 1);
-          const uint32_t offl =
-              (b == 0u) ? (wi == 0u ? offc + 128u * (R - 1) : offc - 128u) : offc;
-          const uint32_t offr =
-              (b == 31u) ? (wi == (uint32_t)(R - 1) ? offc - 128u * (R - 1) : offc + 128u) : offc;
-          lo = *reinterpret_cast<const uint32_t *>(latb + offl);
-          hi = *reinterpret_cast<const uint32_t *>(latb + offr);
-          wc = (b == 0u) ? hi : lo;
-        }
-        const uint32_t t = __funnelshift_r(lo, hi, b + 29u);  // bits 2,3,4: left, centre, right
-        const uint32_t u = __funnelshift_r(wu, wu, b + 27u);  // bit 5: up
-        const uint32_t d = __funnelshift_r(wd, wd, b + 26u);  // bit 6: down
-        const uint32_t p4 = (t & 0x1Cu) | (u & 0x20u) | (d & 0x40u);
-        const uint32_t x2 = curand(&st);
-        bool acc;
-        if (kFloatCmp) {
-          acc = _curand_uniform(x2) < *reinterpret_cast<const float *>(paccb + p4);
-        } else {
-          acc = x2 <= *reinterpret_cast<const uint32_t *>(thrb + p4);
-        }
-        if (acc) *reinterpret_cast<uint32_t *>(const_cast<char *>(latb) + offc) = wc ^ (1u << b);
-      }
-    }
-    store_rng(st, p.rng, p.rng_stride, rep);
+    for (int a = 0; a < total - 1; ++a)
+      row_attempt<L, kFloatCmp, true>(s, rg, latb, thrb, paccb, lane4, shrink);
+    row_attempt<L, kFloatCmp, false>(s, rg, latb, thrb, paccb, lane4, shrink);
+    rg.store(p.rng, p.rng_stride, rep);
   }
   __syncwarp();
   epilogue_mag(lat + lane, p, N, W, live, rep);
@@ -438,22 +503,28 @@ int launch_rows(Kern kern, const SweepLaunch &p, size_t dyn_smem, cudaStream_t s
   return GASP_OK;
 }
 
-template <bool F>
-int dispatch_exact(const SweepLaunch &p, cudaStream_t s) {
+template <bool F, int K>
+int dispatch_kind(const SweepLaunch &p, cudaStream_t s) {
   if (p.variant == 1) {  // the generic kernel, kept selectable for comparisons
-    return launch_tiles(p.L == 64 ? k_sweep_exact<64, F> : k_sweep_exact<0, F>, p, s);
+    return launch_tiles(p.L == 64 ? k_sweep_exact<64, F, K> : k_sweep_exact<0, F, K>, p, s);
   }
   switch (p.L) {
-    case 16: return launch_tiles(k_sweep_exact<16, F>, p, s);
-    case 32: return launch_rows(k_sweep_rows<32, true, F>, p, 0, s);
-    case 48: return launch_tiles(k_sweep_exact<48, F>, p, s);
-    case 64: return launch_rows(k_sweep_rows<64, true, F>, p, 0, s);
-    case 96: return launch_tiles(k_sweep_exact<96, F>, p, s);
+    case 16: return launch_tiles(k_sweep_exact<16, F, K>, p, s);
+    case 32: return launch_rows(k_sweep_rows<32, true, F, K>, p, 0, s);
+    case 48: return launch_tiles(k_sweep_exact<48, F, K>, p, s);
+    case 64: return launch_rows(k_sweep_rows<64, true, F, K>, p, 0, s);
+    case 96: return launch_tiles(k_sweep_exact<96, F, K>, p, s);
     case 128:
-      return launch_rows(k_sweep_rows<128, false, F>, p,
+      return launch_rows(k_sweep_rows<128, false, F, K>, p,
                          (size_t)words_per_replica(128) * kTile * sizeof(uint32_t), s);
-    default: return launch_tiles(k_sweep_exact<0, F>, p, s);
+    default: return launch_tiles(k_sweep_exact<0, F, K>, p, s);
   }
+}
+
+template <bool F>
+int dispatch_exact(const SweepLaunch &p, cudaStream_t s) {
+  return p.rng_kind == kRngMwc ? dispatch_kind<F, kRngMwc>(p, s)
+                               : dispatch_kind<F, kRngXorwow>(p, s);
 }
 
 }  // namespace
@@ -482,7 +553,19 @@ int launch_build_thresholds(const float *d_pacc20, uint32_t *d_thr10, int *d_fla
 }
 
 int launch_sweep_exact(const SweepLaunch &p, cudaStream_t s) {
-  return p.float_compare ? dispatch_exact<true>(p, s) : dispatch_exact<false>(p, s);
+  // Kernels count a batch's attempts in 32-bit integers: split long batches.
+  const int N = p.L * p.L;
+  const int max_chunk = (1 << 30) / N;
+  SweepLaunch q = p;
+  int left = p.nsweeps;
+  while (left > 0) {
+    q.nsweeps = left < max_chunk ? left : max_chunk;
+    left -= q.nsweeps;
+    q.mag_out = left == 0 ? p.mag_out : nullptr;
+    const int rc = p.float_compare ? dispatch_exact<true>(q, s) : dispatch_exact<false>(q, s);
+    if (rc) return rc;
+  }
+  return GASP_OK;
 }
 
 int launch_sweep_trace_cpu(const SweepLaunch &p, cudaStream_t s) {

@@ -53,11 +53,15 @@ def set_stream(stream_handle):
 class RngStates:
     """Per-replica cuRAND XORWOW states, seeded as gpuInitRand."""
 
-    def __init__(self, ngrids, seed, threads_per_block=32):
+    def __init__(self, ngrids, seed, threads_per_block=32, kind="xorwow"):
+        """kind: "xorwow" (the reference's cuRAND stream, bit-exact) or
+        "mwc64x" (the production stream, statistically equivalent)."""
         self.ngrids = int(ngrids)
+        self.kind = kind
+        k = {"xorwow": nat.RNG_XORWOW, "mwc64x": nat.RNG_MWC64X}[kind]
         self._h = C.c_void_p()
-        check(lib().gasp_init_rand(self.ngrids, threads_per_block, C.c_ulonglong(int(seed)),
-                                   C.byref(self._h)), "gasp_init_rand")
+        check(lib().gasp_init_rand_mode(self.ngrids, threads_per_block, C.c_ulonglong(int(seed)),
+                                        k, C.byref(self._h)), "gasp_init_rand")
 
     @property
     def handle(self):
@@ -143,9 +147,11 @@ class DeviceGrids:
 def run_driver(dgrids, rng, beta, h, tot_nsweeps, mag_output_int, grid_output_int, itask=0,
                dn_thr=-0.9, up_thr=0.9, ninputs=1, host_grids=None, fates=None,
                outfunc=None, packed_out=None, verbosity=0, compact=False,
-               threads_per_block=32, gpu_method=2, filename="gridstates.bin"):
+               threads_per_block=32, gpu_method=2, filename="gridstates.bin", first_up=None):
     """Runs gasp_mc_driver_gpu_ex; returns (result, fates, elapsed_s, attempts).
 
+    ``first_up`` (int32[ngrids], optional) receives each replica's first check
+    isweep with magnetisation above up_thr (-1: never).
     ``outfunc(L, ngrids, grids_int32[ngrids,L,L], isweep, mag)`` mirrors the
     reference's GridOutputFunc; ``packed_out(L, ngrids, payload_u8, isweep,
     mag)`` receives gridstates.bin payloads.  Either returns 0 on success.
@@ -183,8 +189,12 @@ def run_driver(dgrids, rng, beta, h, tot_nsweeps, mag_output_int, grid_output_in
     pcb = nat.PACKED_OUTPUT_FN(_packed) if packed_out is not None else nat.PACKED_OUTPUT_FN()
     elapsed = C.c_double(0.0)
     attempts = C.c_longlong(0)
+    fu_ptr = None
+    if first_up is not None:
+        assert first_up.dtype == np.int32 and first_up.size >= ngrids and first_up.flags.c_contiguous
+        fu_ptr = first_up.ctypes.data_as(C.POINTER(C.c_int))
     opts = nat.DriverOptsT(verbosity, int(bool(compact)), pcb, None,
-                           C.pointer(elapsed), C.pointer(attempts))
+                           C.pointer(elapsed), C.pointer(attempts), fu_ptr)
     grids_t = nat.GpuGridsT(L, ngrids, hg_ptr, dgrids.handle)
     samp = nat.SamplerT(tot_nsweeps, mag_output_int, grid_output_int)
     calc = nat.FunctionT(itask, dn_thr, up_thr, ninputs, -1, b"magnetisation",

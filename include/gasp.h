@@ -104,6 +104,18 @@ typedef struct gasp_rng gasp_rng_t;
  * reference. */
 int gasp_init_rand(int ngrids, int threads_per_block, unsigned long long seed,
                    gasp_rng_t **rng_out);
+
+/* RNG kinds.  GASP_RNG_XORWOW is the reference's stream (gpuInitRand);
+ * GASP_RNG_MWC64X is the production stream (no reference counterpart): per
+ * replica an MWC64X generator, non-overlapping substreams 2^40 draws apart,
+ * integer site selection.  Sweeps with an MWC64X state are statistically,
+ * not bitwise, equivalent to the reference and about twice as fast. */
+enum { GASP_RNG_XORWOW = 0, GASP_RNG_MWC64X = 1 };
+int gasp_init_rand_mode(int ngrids, int threads_per_block, unsigned long long seed, int kind,
+                        gasp_rng_t **rng_out);
+/* Host-only: the MWC64X start states gasp_init_rand_mode uploads, x of
+ * replica r at out[r] and carry at out[stride + r] (2*stride words). */
+int gasp_mwc64x_seed_states(unsigned long long seed, int ngrids, int stride, uint32_t *out);
 int gasp_free_rand(gasp_rng_t *rng);
 
 /* ------------------------------------------------------------ kernels */
@@ -203,6 +215,8 @@ typedef struct {
   void *packed_user;
   double *elapsed_s;    /* if set, receives the driver's wall time          */
   long long *attempts;  /* if set, receives attempted flips simulated       */
+  int *first_up;        /* if set (ngrids ints): first check isweep with
+                         * cv > up_thr per replica, -1 if never            */
 } gasp_driver_opts_t;
 
 /* Replaces mc_driver_gpu (include/mc_gpu.h:47, src/mc_gpu.cu:530-831): the

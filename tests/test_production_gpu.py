@@ -1,0 +1,89 @@
+"""Production RNG mode (MWC64X streams, integer site selection) on a B200:
+statistically equivalent to the reference stream.  The reference-exact mode is
+bit-identical to the reference kernels (test_parity_gpu.py), so it serves as
+the reference sample here.  Tolerances are 4 combined standard errors."""
+import numpy as np
+import pytest
+
+from gpu_2dising_b200 import analysis, engine
+
+pytestmark = pytest.mark.gpu
+
+L, R, BETA, H, TOT, MAG, UP = 32, 16384, 0.54, 0.10, 1500, 5, 0.9
+
+
+@pytest.fixture(scope="module", autouse=True)
+def device():
+    return engine.init_device(0)
+
+
+def _swarm(kind, seed):
+    dg = engine.DeviceGrids(L, R, -np.ones((R, L, L), np.int32))
+    rng = engine.RngStates(R, seed, kind=kind)
+    fu = np.full(R, -1, np.int32)
+    res, _, _, _ = engine.run_driver(dg, rng, BETA, H, TOT, MAG, TOT, itask=0, dn_thr=-0.95,
+                                     up_thr=UP, first_up=fu)
+    return res, fu
+
+
+@pytest.fixture(scope="module")
+def swarms():
+    return {k: _swarm(k, 31337 if k == "xorwow" else 27182) for k in ("xorwow", "mwc64x")}
+
+
+def test_production_is_deterministic_and_distinct(swarms):
+    res2, fu2 = _swarm("mwc64x", 27182)
+    assert np.array_equal(fu2, swarms["mwc64x"][1])
+    assert not np.array_equal(swarms["mwc64x"][1], swarms["xorwow"][1])
+
+
+def test_first_passage_consistent_with_fraction(swarms):
+    for res, fu in swarms.values():
+        frac = analysis.fraction_from_first_passage(fu, TOT, MAG)
+        # the driver's fraction counts replicas above up at each check; for
+        # this field a nucleated replica does not return, so both agree
+        assert np.max(np.abs(frac - res)) <= 2.0 / R
+
+
+def test_rate_and_lag_agree_within_bootstrap_error(swarms):
+    fits = {k: analysis.bootstrap_rate(fu, TOT, MAG, nboot=100, L=L) for k, (_, fu) in swarms.items()}
+    a, b = fits["xorwow"], fits["mwc64x"]
+    assert a["k"] > 0 and b["k"] > 0
+    assert abs(a["k"] - b["k"]) < 4 * np.hypot(a["k_se"], b["k_se"]), (a, b)
+    assert abs(a["t0"] - b["t0"]) < 4 * np.hypot(a["t0_se"], b["t0_se"]), (a, b)
+
+
+def test_first_passage_distributions_agree(swarms):
+    fa = swarms["xorwow"][1]
+    fb = swarms["mwc64x"][1]
+    na, nb = np.count_nonzero(fa >= 0), np.count_nonzero(fb >= 0)
+    # fraction nucleated by the end: binomial error
+    pa, pb = na / R, nb / R
+    se = np.sqrt(pa * (1 - pa) / R + pb * (1 - pb) / R)
+    assert abs(pa - pb) < 4 * se + 1e-12
+    # two-sample Kolmogorov-Smirnov on the first-passage sweeps of nucleated replicas
+    from scipy.stats import ks_2samp
+    assert ks_2samp(fa[fa >= 0], fb[fb >= 0]).pvalue > 1e-4
+
+
+def test_committor_agrees_within_binomial_error():
+    """pB of four droplets around the critical size, both streams."""
+    Lc, n, radii = 32, 4096, (3.5, 4.5, 5.5, 6.5)
+    yy, xx = np.mgrid[0:Lc, 0:Lc]
+    inputs = [np.where((yy - Lc / 2) ** 2 + (xx - Lc / 2) ** 2 <= r * r, 1, -1).astype(np.int32)
+              for r in radii]
+    g = np.concatenate([np.repeat(x[None], n, axis=0) for x in inputs])
+    out = {}
+    for kind, seed in (("xorwow", 11), ("mwc64x", 12)):
+        dg = engine.DeviceGrids(Lc, n * len(radii), g)
+        rng = engine.RngStates(n * len(radii), seed, kind=kind)
+        res, fates, _, _ = engine.run_driver(dg, rng, BETA, H, 6000, 5, 6000, itask=1,
+                                             dn_thr=-0.9, up_thr=0.5, ninputs=len(radii),
+                                             compact=True)
+        assert np.count_nonzero(fates == -1) == 0
+        out[kind] = np.asarray(res, np.float64)
+    pa, pb = out["xorwow"], out["mwc64x"]
+    informative = (pa > 0.03) & (pa < 0.97)
+    assert informative.any(), out
+    se = np.sqrt(pa * (1 - pa) / n + pb * (1 - pb) / n)
+    assert np.all(np.abs(pa - pb)[informative] < 4 * se[informative]), out
