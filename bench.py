@@ -306,6 +306,104 @@ def run_ours(args, rank, world, local_rank):
         dist.destroy_process_group()
 
 
+BATCH_GROUPS_L = (32, 48, 64, 96, 128)
+BATCH_GROUPS_R = (16384, 8192, 4096, 2048, 512)
+
+
+def batched_groups(seed=2024):
+    """The uneven-batch workload: five groups, beta ~ U[0.45, 0.60] and
+    h ~ U[0.03, 0.12] drawn per group from a seed."""
+    rs = np.random.default_rng(seed)
+    return [(L, R_, float(rs.uniform(0.45, 0.60)), float(rs.uniform(0.03, 0.12)))
+            for L, R_ in zip(BATCH_GROUPS_L, BATCH_GROUPS_R)]
+
+
+def run_batched(args):
+    """One JSON line for the uneven batched launch vs one plain launch per
+    group, both counting only attempts of not-yet-nucleated replicas."""
+    import ctypes as C
+    from gpu_2dising_b200 import _native as nat, engine
+    engine.init_device(0)
+    groups = batched_groups()
+    arr = (nat.GroupT * len(groups))(*[nat.GroupT(L, n, b, h) for L, n, b, h in groups])
+    h = C.c_void_p()
+    kind = nat.RNG_MWC64X if args.rng == "mwc64x" else nat.RNG_XORWOW
+    nat.check(nat.lib().gasp_batch_create(arr, len(groups), SEED, kind, C.byref(h)))
+    choice = np.zeros(2 * len(groups), np.int32)
+    nat.check(nat.lib().gasp_batch_autotune(h, 2, choice))
+    tot, chk, up = args.batched_sweeps, 50, 0.9
+    res = {}
+    for name, mode in (("plain", nat.BATCH_PLAIN), ("graph", nat.BATCH_GRAPH)):
+        counts = np.zeros((tot // chk) * len(groups), np.int32)
+        att, el = C.c_longlong(), C.c_double()
+        nat.check(nat.lib().gasp_batch_swarm(h, tot, chk, up, mode, counts, C.byref(att),
+                                             C.byref(el)))
+        res[name] = {"attempts": att.value, "seconds": el.value, "value": att.value / el.value,
+                     "nucleated": counts.reshape(-1, len(groups))[-1].tolist()}
+    nat.lib().gasp_batch_free(h)
+    line = {
+        "metric": "spin-flip attempts/s, uneven batched launch vs plain per-group launches",
+        "value": res["graph"]["value"], "unit": UNIT, "n_gpus": 1,
+        "speedup_vs_plain": res["graph"]["value"] / res["plain"]["value"],
+        "plain": res["plain"], "graph": res["graph"],
+        "config": {"workload": "5 groups L=32/48/64/96/128, replicas 16384/8192/4096/2048/512, "
+                               "all-down, nucleated replicas (m > 0.9 at a check) finished",
+                   "groups": [{"L": L, "replicas": n, "beta": b, "h": hh}
+                              for L, n, b, hh in groups],
+                   "sweeps": tot, "check_int": chk, "rng": args.rng,
+                   "autotune": choice.reshape(-1, 2).tolist()},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def committor_inputs(n=64, L_=L, seed=7):
+    """Seeded committor inputs: all -1, a centred +1 disc of radius
+    r ~ U[4, 12] (dist <= r from (L/2, L/2)), then 2% of sites flipped."""
+    rs = np.random.default_rng(seed)
+    yy, xx = np.mgrid[0:L_, 0:L_]
+    out, radii = [], []
+    for _ in range(n):
+        r = rs.uniform(4.0, 12.0)
+        g = np.where((yy - L_ / 2) ** 2 + (xx - L_ / 2) ** 2 <= r * r, 1, -1).astype(np.int32)
+        flip = rs.random((L_, L_)) < 0.02
+        g[flip] *= -1
+        out.append(g)
+        radii.append(r)
+    return np.stack(out), np.array(radii)
+
+
+def run_committor(args):
+    """Committor shooting of 64 seeded droplet grids, 4096 replicas each,
+    until every replica reaches A (m < -0.93) or B (m > 0.9), cap 20000 sweeps."""
+    from gpu_2dising_b200 import analysis, engine
+    engine.init_device(0)
+    ngrid_in, shots = args.committor_inputs, args.committor_shots
+    inputs, radii = committor_inputs(ngrid_in)
+    host = np.repeat(inputs, shots, axis=0)
+    n = host.shape[0]
+    t0 = time.perf_counter()
+    dg = engine.DeviceGrids(L, n, host)
+    rng = engine.RngStates(n, SEED, kind=args.rng)
+    res, fates, drv_s, attempts = engine.run_driver(
+        dg, rng, BETA, H, 20000, args.committor_check, 20000, itask=1, dn_thr=-0.93,
+        up_thr=0.90, ninputs=ngrid_in, compact=True)
+    wall = time.perf_counter() - t0
+    errs = [analysis.committor_errbar(fates[i * shots:(i + 1) * shots]) for i in range(ngrid_in)]
+    line = {
+        "metric": "committor evaluations/s (shooting)", "value": ngrid_in / wall,
+        "unit": "grids/s", "n_gpus": 1, "attempts_per_s": attempts / drv_s,
+        "wall_s": wall, "driver_s": drv_s, "attempts": attempts,
+        "unresolved": int(np.count_nonzero(fates == -1)),
+        "pB": [round(float(x), 5) for x in res], "pB_err": [round(e, 5) for e in errs],
+        "radii": [round(float(r), 3) for r in radii],
+        "config": {"workload": f"{ngrid_in} droplet grids L=64 (r~U[4,12], 2% flips), "
+                               f"{shots} shots each, beta=0.54, h=0.07, dn=-0.93, up=0.9, "
+                               "cap 20000 sweeps, compaction on",
+                   "check_int": args.committor_check, "rng": args.rng},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     global SWEEPS_PER_STEP
     ap = argparse.ArgumentParser()
@@ -317,6 +415,13 @@ def main():
     ap.add_argument("--sweeps-per-step", type=int, default=SWEEPS_PER_STEP,
                     help="smaller values give a short launch for ncu captures")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--workload", default="swarm", choices=["swarm", "batched", "committor"],
+                    help="swarm: the headline single-group swarm; batched: uneven groups; "
+                         "committor: seeded droplet shooting")
+    ap.add_argument("--committor-inputs", type=int, default=64)
+    ap.add_argument("--committor-shots", type=int, default=4096)
+    ap.add_argument("--committor-check", type=int, default=10)
+    ap.add_argument("--batched-sweeps", type=int, default=1000)
     ap.add_argument("--rng", default="xorwow", choices=["xorwow", "mwc64x"],
                     help="xorwow: the reference stream (bit-exact); mwc64x: production stream")
     ap.add_argument("--variant", type=int, default=0,
@@ -330,6 +435,12 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank)
+    elif args.workload == "batched":
+        if rank == 0:
+            run_batched(args)
+    elif args.workload == "committor":
+        if rank == 0:
+            run_committor(args)
     else:
         run_ours(args, rank, world, local_rank)
 

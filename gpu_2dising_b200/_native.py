@@ -28,6 +28,9 @@ GASP_ERR_TIMEOUT = 9
 OPT_SWEEP_VARIANT = 1
 OPT_WARPS_PER_CTA = 2
 
+BATCH_PLAIN = 0
+BATCH_GRAPH = 1
+
 RNG_XORWOW = 0
 RNG_MWC64X = 1
 
@@ -46,6 +49,7 @@ EXPORTED = (
     "gasp_init_grids_uniform", "gasp_init_grids_from_file", "gasp_init_grids_from_array",
     "gasp_init_fates", "gasp_read_input_grid", "gasp_write_ising_grids",
     "gasp_write_packed_frame", "gasp_bootstrap_errbar", "gasp_committor_from_fates",
+    "gasp_batch_create", "gasp_batch_free", "gasp_batch_swarm", "gasp_batch_autotune",
 )
 
 
@@ -79,6 +83,10 @@ class GpuRunT(C.Structure):
 class GpuGridsT(C.Structure):
     _fields_ = [("L", C.c_int), ("ngrids", C.c_int), ("ising_grids", C.POINTER(C.c_int)),
                 ("d_grids", C.c_void_p)]
+
+
+class GroupT(C.Structure):
+    _fields_ = [("L", C.c_int), ("ngrids", C.c_int), ("beta", C.c_double), ("h", C.c_double)]
 
 
 GRID_OUTPUT_FN = C.CFUNCTYPE(C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int), C.c_int,
@@ -144,6 +152,11 @@ def _bind(lib):
         "gasp_write_packed_frame": (I, [C.c_char_p, I, I, I, _u8p, C.c_size_t]),
         "gasp_bootstrap_errbar": (C.c_double, [I, I, _i32p]),
         "gasp_committor_from_fates": (I, [I, I, _i32p, _f32p]),
+        "gasp_batch_create": (I, [C.POINTER(GroupT), I, C.c_ulonglong, I, C.POINTER(P)]),
+        "gasp_batch_free": (I, [P]),
+        "gasp_batch_swarm": (I, [P, I, I, C.c_double, I, _i32p, C.POINTER(C.c_longlong),
+                                 C.POINTER(C.c_double)]),
+        "gasp_batch_autotune": (I, [P, I, _i32p]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

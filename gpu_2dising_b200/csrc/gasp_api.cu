@@ -338,7 +338,7 @@ int gasp_grids_download(gasp_grids_t *g, int *host_grids) {
 int gasp_grids_set_option(gasp_grids_t *g, int option, int value) {
   if (!g) return GASP_ERR_INVALID;
   GridsExtra &x = impl(g)->x;
-  if (option == GASP_OPT_SWEEP_VARIANT && (value == 0 || value == 1)) {
+  if (option == GASP_OPT_SWEEP_VARIANT && value >= 0 && value <= 2) {
     x.variant = value;
     return GASP_OK;
   }
@@ -515,6 +515,20 @@ int check_sweep_args(gasp_grids_t *g, gasp_rng_t *r, int nsweeps, int method) {
 }
 
 }  // namespace
+
+namespace gasp {
+
+SweepLaunch launch_for(gasp_grids_t *g, gasp_rng_t *r) {
+  SweepLaunch p = base_launch(g);
+  p.rng = r->d_state;
+  p.rng_stride = r->stride;
+  p.rng_kind = r->kind;
+  return p;
+}
+
+int prepare_tables(gasp_grids_t *g, double beta, double h) { return ensure_tables(g, beta, h); }
+
+}  // namespace gasp
 
 extern "C" {
 

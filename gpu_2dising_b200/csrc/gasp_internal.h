@@ -71,9 +71,20 @@ struct SweepLaunch {
   float *mag_out;         // optional: magnetisation after the batch [ngrids]
   int float_compare;      // exact mode: compare in float (thresholds unusable)
   int warps_per_cta;      // launch shape (0: default)
-  int variant;            // 0: fastest kernel for L; 1: generic exact kernel
+  int variant;            // 0: fastest kernel for L; 1: generic; 2: row kernel, no pairing
   int rng_kind;           // RngKind of p.rng
+  const int *n_active_dev;// optional device count overriding n_active (graph replays)
 };
+
+// Sweep parameters of a replica set + RNG whose tables are ready
+// (prepare_tables called for the set's beta, h); gasp_api.cu.
+SweepLaunch launch_for(gasp_grids_t *g, gasp_rng_t *r);
+int prepare_tables(gasp_grids_t *g, double beta, double h);
+
+// Device-side check + compaction of one replica group (gasp_batch.cu).
+int launch_check_compact(const float *mag, int *active, int *n_active, int ngrids,
+                         double up_thr, int *counts, int *interval, int max_intervals,
+                         cudaStream_t s);
 
 // kernel launchers (gasp_kernels.cu); each returns a GASP status.
 int launch_rng_init(uint32_t *rng, int ngrids, int stride, unsigned long long seed, cudaStream_t s);

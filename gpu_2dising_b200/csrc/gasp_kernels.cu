@@ -156,10 +156,11 @@ __global__ void __launch_bounds__(256) k_sweep_exact(SweepLaunch p) {
   if (threadIdx.x < 10) thr_s[threadIdx.x] = p.thr[threadIdx.x];
   if (threadIdx.x < 20) pacc_s[threadIdx.x] = p.pacc_f[threadIdx.x];
 
+  const int n_act = p.n_active_dev ? *p.n_active_dev : p.n_active;
   const int tile = blockIdx.x * nwarps + warp;
   const int slot = tile * kTile + lane;
-  const bool tile_live = tile * kTile < p.n_active;
-  const bool live = slot < p.n_active;
+  const bool tile_live = tile * kTile < n_act;
+  const bool live = slot < n_act;
   const int rep = live ? (p.active ? p.active[slot] : slot) : 0;
   uint32_t *lat_s = smem + kHeaderWords + warp * (W * kTile);
   if (tile_live) stage_in(lat_s, p, W, tile, lane, live, rep);
@@ -280,6 +281,161 @@ __device__ __forceinline__ void row_attempt(uint32_t &s, Rng &rg, const char *la
   if (acc) *reinterpret_cast<uint32_t *>(const_cast<char *>(latb) + offc) = wc ^ (1u << (sc & 31u));
 }
 
+// The shared-memory words one attempt reads, and its 5-spin pattern.
+struct Probe {
+  uint32_t offc;  // byte offset of the centre word
+  uint32_t wc;    // centre word as loaded
+  uint32_t p4;    // pattern * 4 (left, centre, right, up, down at bits 2..6)
+  uint32_t bit;   // 1 << (site & 31)
+};
+
+template <int L>
+__device__ __forceinline__ Probe row_probe(uint32_t s, const char *latb, uint32_t lane4) {
+  constexpr int N = L * L;
+  constexpr int R = L / 32;
+  constexpr uint32_t kMask = (uint32_t)(4 * N - 1) & ~127u;
+  Probe q;
+  const uint32_t b = s & 31u;
+  q.bit = 1u << b;
+  q.offc = ((s << 2) & kMask) | lane4;
+  const uint32_t offu = ((q.offc - 128u * R) & kMask) | lane4;
+  const uint32_t offd = ((q.offc + 128u * R) & kMask) | lane4;
+  const uint32_t wu = *reinterpret_cast<const uint32_t *>(latb + offu);
+  const uint32_t wd = *reinterpret_cast<const uint32_t *>(latb + offd);
+  uint32_t lo, hi;
+  if constexpr (R == 1) {
+    q.wc = *reinterpret_cast<const uint32_t *>(latb + q.offc);
+    lo = hi = q.wc;
+  } else if constexpr (R == 2) {
+    q.wc = *reinterpret_cast<const uint32_t *>(latb + q.offc);
+    const uint32_t wx = *reinterpret_cast<const uint32_t *>(latb + (q.offc ^ 128u));
+    lo = (b == 0u) ? wx : q.wc;
+    hi = (b == 31u) ? wx : q.wc;
+  } else {
+    const uint32_t wi = (q.offc >> 7) & (uint32_t)(R - 1);
+    const uint32_t offl =
+        (b == 0u) ? (wi == 0u ? q.offc + 128u * (R - 1) : q.offc - 128u) : q.offc;
+    const uint32_t offr =
+        (b == 31u) ? (wi == (uint32_t)(R - 1) ? q.offc - 128u * (R - 1) : q.offc + 128u) : q.offc;
+    lo = *reinterpret_cast<const uint32_t *>(latb + offl);
+    hi = *reinterpret_cast<const uint32_t *>(latb + offr);
+    q.wc = (b == 0u) ? hi : lo;
+  }
+  const uint32_t t = __funnelshift_r(lo, hi, b + 29u);
+  const uint32_t u = __funnelshift_r(wu, wu, b + 27u);
+  const uint32_t d = __funnelshift_r(wd, wd, b + 26u);
+  q.p4 = (t & 0x1Cu) | (u & 0x20u) | (d & 0x40u);
+  return q;
+}
+
+template <bool kFloatCmp>
+__device__ __forceinline__ bool row_accept(uint32_t x2, uint32_t p4, const char *thrb,
+                                           const char *paccb) {
+  if constexpr (kFloatCmp) return _curand_uniform(x2) < *reinterpret_cast<const float *>(paccb + p4);
+  else return x2 <= *reinterpret_cast<const uint32_t *>(thrb + p4);
+}
+
+// Could site sa be one of the five sites attempt sb reads (sb, its left,
+// right, up, down neighbours, rows and columns periodic)?  Conservative: also
+// true for the two diagonal offsets L-1 and N-L+1.
+template <int L>
+__device__ __forceinline__ bool row_collide(uint32_t sa, uint32_t sb) {
+  constexpr uint32_t N = (uint32_t)(L * L);
+  const uint32_t e = (sa - sb + 1u) & (N - 1u);  // (sa - sb) + 1 mod N
+  return (e <= 2u) | ((e - (uint32_t)L) <= 1u) | ((e - (N - (uint32_t)L + 1u)) <= 1u);
+}
+
+// Two consecutive attempts (a, b) of every lane.  Unless some lane's attempt
+// a touches a site attempt b reads, both are evaluated on the lattice as it
+// was before the pair and their flips applied in order (b's store forwards a's
+// flip when both flip the same word); otherwise the warp runs them in order.
+// Either way each replica sees exactly the sequential result.
+template <int L, bool kFloatCmp>
+__device__ __forceinline__ void row_pair(uint32_t sa, uint32_t x2a, uint32_t sb, uint32_t x2b,
+                                         const char *latb, const char *thrb, const char *paccb,
+                                         uint32_t lane4) {
+  char *latw = const_cast<char *>(latb);
+  const bool coll = row_collide<L>(sa, sb);
+  const Probe A = row_probe<L>(sa, latb, lane4);
+  if (!__any_sync(__activemask(), coll)) {
+    const Probe B = row_probe<L>(sb, latb, lane4);
+    const bool acc_a = row_accept<kFloatCmp>(x2a, A.p4, thrb, paccb);
+    const bool acc_b = row_accept<kFloatCmp>(x2b, B.p4, thrb, paccb);
+    const uint32_t fa = acc_a ? A.bit : 0u;
+    if (acc_a) *reinterpret_cast<uint32_t *>(latw + A.offc) = A.wc ^ A.bit;
+    const uint32_t wcb = B.wc ^ ((B.offc == A.offc) ? fa : 0u);
+    if (acc_b) *reinterpret_cast<uint32_t *>(latw + B.offc) = wcb ^ B.bit;
+  } else {
+    if (row_accept<kFloatCmp>(x2a, A.p4, thrb, paccb))
+      *reinterpret_cast<uint32_t *>(latw + A.offc) = A.wc ^ A.bit;
+    const Probe B = row_probe<L>(sb, latb, lane4);
+    if (row_accept<kFloatCmp>(x2b, B.p4, thrb, paccb))
+      *reinterpret_cast<uint32_t *>(latw + B.offc) = B.wc ^ B.bit;
+  }
+}
+
+// k_sweep_rows with pairwise speculation (see row_pair).  The four draws of
+// the next pair are made during the current pair, in the reference's order.
+template <int L, bool kStatic, bool kFloatCmp, int kRng>
+__global__ void __launch_bounds__(32) k_sweep_rows_pair(SweepLaunch p) {
+  static_assert(L % 32 == 0 && (L & (L - 1)) == 0, "L must be a power of two >= 32");
+  constexpr int N = L * L;
+  constexpr int W = N / 32;
+  __shared__ __align__(16) uint32_t thrP[32];
+  __shared__ __align__(16) float paccP[32];
+  extern __shared__ __align__(16) uint32_t dyn[];
+  uint32_t *lat = LatticeStore<W * kTile, kStatic>::get(dyn);
+
+  const int lane = threadIdx.x;
+  {
+    const int c = (lane >> 1) & 1;
+    const int cls = 5 * c + __popc(lane & 0x1D);
+    thrP[lane] = p.thr[cls];
+    paccP[lane] = p.pacc_f[2 * cls];
+  }
+  const int n_act = p.n_active_dev ? *p.n_active_dev : p.n_active;
+  const int tile = blockIdx.x;
+  if (tile * kTile >= n_act) return;  // whole CTA (one warp) idle this batch
+  const int slot = tile * kTile + lane;
+  const bool live = slot < n_act;
+  const int rep = live ? (p.active ? p.active[slot] : slot) : 0;
+  stage_in(lat, p, W, tile, lane, live, rep);
+  __syncwarp();
+
+  const char *latb = reinterpret_cast<const char *>(lat);
+  const char *thrb = reinterpret_cast<const char *>(thrP);
+  const char *paccb = reinterpret_cast<const char *>(paccP);
+  if (live && p.nsweeps > 0) {
+    RngPolicy<kRng> rg;
+    rg.load(p.rng, p.rng_stride, rep);
+    const float shrink = (1.0f - FLT_EPSILON) * (float)N;
+    const uint32_t lane4 = (uint32_t)lane << 2;
+    // N is even, so a batch is a whole number of pairs.
+    uint32_t sa = rg.template site<N>(shrink, N);
+    uint32_t x2a = rg.next();
+    uint32_t sb = rg.template site<N>(shrink, N);
+    uint32_t x2b = rg.next();
+    const int pairs = (N / 2) * p.nsweeps;
+#pragma unroll 2
+    for (int k = 0; k < pairs - 1; ++k) {
+      const uint32_t na = rg.template site<N>(shrink, N);
+      const uint32_t nxa = rg.next();
+      const uint32_t nb = rg.template site<N>(shrink, N);
+      const uint32_t nxb = rg.next();
+      row_pair<L, kFloatCmp>(sa, x2a, sb, x2b, latb, thrb, paccb, lane4);
+      sa = na;
+      x2a = nxa;
+      sb = nb;
+      x2b = nxb;
+    }
+    row_pair<L, kFloatCmp>(sa, x2a, sb, x2b, latb, thrb, paccb, lane4);
+    rg.store(p.rng, p.rng_stride, rep);
+  }
+  __syncwarp();
+  epilogue_mag(lat + lane, p, N, W, live, rep);
+  stage_out(lat, p, W, tile, lane, live, rep);
+}
+
 template <int L, bool kStatic, bool kFloatCmp, int kRng>
 __global__ void __launch_bounds__(32) k_sweep_rows(SweepLaunch p) {
   static_assert(L % 32 == 0 && (L & (L - 1)) == 0, "L must be a power of two >= 32");
@@ -298,9 +454,11 @@ __global__ void __launch_bounds__(32) k_sweep_rows(SweepLaunch p) {
     thrP[lane] = p.thr[cls];
     paccP[lane] = p.pacc_f[2 * cls];
   }
+  const int n_act = p.n_active_dev ? *p.n_active_dev : p.n_active;
   const int tile = blockIdx.x;
+  if (tile * kTile >= n_act) return;  // whole CTA (one warp) idle this batch
   const int slot = tile * kTile + lane;
-  const bool live = slot < p.n_active;
+  const bool live = slot < n_act;
   const int rep = live ? (p.active ? p.active[slot] : slot) : 0;
   stage_in(lat, p, W, tile, lane, live, rep);
   __syncwarp();
@@ -343,10 +501,11 @@ __global__ void __launch_bounds__(256) k_sweep_trace_cpu(SweepLaunch p) {
   const int nwarps = blockDim.x >> 5;
   double *pacc_s = reinterpret_cast<double *>(smem);  // [20] (160 B < header)
   if (threadIdx.x < 20) pacc_s[threadIdx.x] = p.pacc_cpu[threadIdx.x];
+  const int n_act = p.n_active_dev ? *p.n_active_dev : p.n_active;
   const int tile = blockIdx.x * nwarps + warp;
   const int slot = tile * kTile + lane;
-  const bool tile_live = tile * kTile < p.n_active;
-  const bool live = slot < p.n_active;
+  const bool tile_live = tile * kTile < n_act;
+  const bool live = slot < n_act;
   const int rep = live ? (p.active ? p.active[slot] : slot) : 0;
   uint32_t *lat_s = smem + kHeaderWords + warp * (W * kTile);
   if (tile_live) stage_in(lat_s, p, W, tile, lane, live, rep);
@@ -508,15 +667,22 @@ int dispatch_kind(const SweepLaunch &p, cudaStream_t s) {
   if (p.variant == 1) {  // the generic kernel, kept selectable for comparisons
     return launch_tiles(p.L == 64 ? k_sweep_exact<64, F, K> : k_sweep_exact<0, F, K>, p, s);
   }
+  const size_t dyn128 = (size_t)words_per_replica(128) * kTile * sizeof(uint32_t);
+  if (p.variant == 2) {  // row kernel without pairwise speculation
+    switch (p.L) {
+      case 32: return launch_rows(k_sweep_rows<32, true, F, K>, p, 0, s);
+      case 64: return launch_rows(k_sweep_rows<64, true, F, K>, p, 0, s);
+      case 128: return launch_rows(k_sweep_rows<128, false, F, K>, p, dyn128, s);
+      default: break;
+    }
+  }
   switch (p.L) {
     case 16: return launch_tiles(k_sweep_exact<16, F, K>, p, s);
-    case 32: return launch_rows(k_sweep_rows<32, true, F, K>, p, 0, s);
+    case 32: return launch_rows(k_sweep_rows_pair<32, true, F, K>, p, 0, s);
     case 48: return launch_tiles(k_sweep_exact<48, F, K>, p, s);
-    case 64: return launch_rows(k_sweep_rows<64, true, F, K>, p, 0, s);
+    case 64: return launch_rows(k_sweep_rows_pair<64, true, F, K>, p, 0, s);
     case 96: return launch_tiles(k_sweep_exact<96, F, K>, p, s);
-    case 128:
-      return launch_rows(k_sweep_rows<128, false, F, K>, p,
-                         (size_t)words_per_replica(128) * kTile * sizeof(uint32_t), s);
+    case 128: return launch_rows(k_sweep_rows_pair<128, false, F, K>, p, dyn128, s);
     default: return launch_tiles(k_sweep_exact<0, F, K>, p, s);
   }
 }

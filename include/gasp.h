@@ -235,6 +235,40 @@ int gasp_mc_driver_gpu_ex(gasp_gpu_grids_t grids, double beta, double h, int *gr
                           gasp_gpu_run_t gpu_state, gasp_grid_output_fn outfunc,
                           const gasp_driver_opts_t *opts);
 
+/* ------------------------------------------ batched groups of uneven L */
+/* Several replica groups with their own L, beta and h driven together (no
+ * reference counterpart: the reference runs one (L, beta, h) per process). */
+typedef struct {
+  int L;
+  int ngrids;
+  double beta;
+  double h;
+} gasp_group_t;
+typedef struct gasp_batch gasp_batch_t;
+
+int gasp_batch_create(const gasp_group_t *groups, int ngroups, unsigned long long seed,
+                      int rng_kind, gasp_batch_t **out);
+int gasp_batch_free(gasp_batch_t *batch);
+
+enum { GASP_BATCH_PLAIN = 0, GASP_BATCH_GRAPH = 1 };
+/* Nucleation swarm of every group from all spins -1, re-seeded each call:
+ * every check_int sweeps a replica whose magnetisation exceeds up_thr is
+ * finished (absorbing).  GASP_BATCH_GRAPH: each interval is one CUDA graph
+ * running all groups concurrently, finished replicas compacted out on the
+ * device, no host synchronisation until the end.  GASP_BATCH_PLAIN: one launch
+ * per group per interval over all its replicas, groups in turn, checks on the
+ * host (the comparison path).  Both modes give identical counts.
+ * counts_out[i*ngroups + g] (tot_nsweeps/check_int rows): finished replicas
+ * of group g after interval i.  attempts_out: attempted flips credited to
+ * unfinished replicas only (the same workload for both modes). */
+int gasp_batch_swarm(gasp_batch_t *batch, int tot_nsweeps, int check_int, double up_thr,
+                     int mode, int *counts_out, long long *attempts_out, double *elapsed_out);
+/* Autotuner: times the candidate kernels (row kernel with or without pairwise
+ * speculation; tiles per CTA of the generic kernel) for each group on an
+ * nsweeps run and keeps the fastest.  choice_out (2*ngroups ints, may be
+ * NULL): (variant, warps per CTA) chosen per group. */
+int gasp_batch_autotune(gasp_batch_t *batch, int nsweeps, int *choice_out);
+
 /* ---------------------------------------------------- host-side helpers */
 /* Replace init_grids_uniform / init_grids_from_file / init_grids_from_array /
  * init_fates (include/grid.h:5-9, src/grid.c:5-87); caller owns the memory

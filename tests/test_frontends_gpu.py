@@ -154,16 +154,22 @@ def test_cli_committor_reads_gridinput(ref_gpu, tmp_path):
     assert "does not match L" in r.stderr
 
 
-def test_kernel_variants_agree():
-    """The generic and row-specialised exact kernels give identical results."""
-    L, ng, seed = 64, 96, 31
+@pytest.mark.parametrize("L", [32, 64, 128])
+@pytest.mark.parametrize("kind", ["xorwow", "mwc64x"])
+def test_kernel_variants_agree(L, kind):
+    """The pairwise-speculative, plain row and generic kernels give identical
+    results for both RNG kinds (the speculation never changes a trajectory)."""
+    ng, seed = 96, 31 + L
     g0 = np.where(np.random.default_rng(seed).random((ng, L, L)) < 0.3, 1, -1).astype(np.int32)
     outs = []
-    for variant in (0, 1):
+    for variant in (0, 1, 2):
         dg = engine.DeviceGrids(L, ng, g0)
         dg.set_option(1, variant)
-        r = engine.RngStates(ng, seed)
-        dg.sweep(r, 0.5, 0.1, 3)
+        r = engine.RngStates(ng, seed, kind=kind)
+        dg.sweep(r, 0.45, 0.1, 3)
+        dg.sweep(r, 0.45, 0.1, 2)
         outs.append((dg.download(), dg.magnetisation()))
-    assert np.array_equal(outs[0][0], outs[1][0])
-    assert np.array_equal(outs[0][1], outs[1][1])
+    for o in outs[1:]:
+        assert np.array_equal(outs[0][0], o[0])
+        assert np.array_equal(outs[0][1], o[1])
+    assert not np.array_equal(outs[0][0], g0)

@@ -40,9 +40,11 @@ def test_production_is_deterministic_and_distinct(swarms):
 def test_first_passage_consistent_with_fraction(swarms):
     for res, fu in swarms.values():
         frac = analysis.fraction_from_first_passage(fu, TOT, MAG)
-        # the driver's fraction counts replicas above up at each check; for
-        # this field a nucleated replica does not return, so both agree
-        assert np.max(np.abs(frac - res)) <= 2.0 / R
+        # the driver's fraction counts replicas above up at each check (not
+        # absorbing): at L=32 a nucleated replica can dip back below up, so
+        # it is at most the first-passage fraction and close to it
+        assert np.all(res <= frac + 1e-12)
+        assert np.max(frac - res) < 0.01
 
 
 def test_rate_and_lag_agree_within_bootstrap_error(swarms):
