@@ -50,6 +50,8 @@ EXPORTED = (
     "gasp_init_fates", "gasp_read_input_grid", "gasp_write_ising_grids",
     "gasp_write_packed_frame", "gasp_bootstrap_errbar", "gasp_committor_from_fates",
     "gasp_batch_create", "gasp_batch_free", "gasp_batch_swarm", "gasp_batch_autotune",
+    "gasp_cnn_param_count", "gasp_cnn_create", "gasp_cnn_free", "gasp_cnn_set_params",
+    "gasp_cnn_get_params", "gasp_cnn_predict", "gasp_cnn_gradients", "gasp_cnn_train_step",
 )
 
 
@@ -107,6 +109,7 @@ _i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
 _f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
 _f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 _u8p = np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")
+_i8p = np.ctypeslib.ndpointer(dtype=np.int8, flags="C_CONTIGUOUS")
 
 
 def _bind(lib):
@@ -157,6 +160,14 @@ def _bind(lib):
         "gasp_batch_swarm": (I, [P, I, I, C.c_double, I, _i32p, C.POINTER(C.c_longlong),
                                  C.POINTER(C.c_double)]),
         "gasp_batch_autotune": (I, [P, I, _i32p]),
+        "gasp_cnn_param_count": (I, []),
+        "gasp_cnn_create": (I, [I, I, C.POINTER(P)]),
+        "gasp_cnn_free": (I, [P]),
+        "gasp_cnn_set_params": (I, [P, _f32p]),
+        "gasp_cnn_get_params": (I, [P, _f32p]),
+        "gasp_cnn_predict": (I, [P, _i8p, I, _f32p]),
+        "gasp_cnn_gradients": (I, [P, _i8p, _f32p, I, C.POINTER(C.c_float), _f32p]),
+        "gasp_cnn_train_step": (I, [P, _i8p, _f32p, I, C.c_float, C.POINTER(C.c_float)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -127,12 +127,18 @@ struct gasp_batch {
   int max_intervals = 0;
   std::vector<cudaStream_t> streams;
   std::vector<cudaEvent_t> events;  // fork + one join per group
+  cudaStream_t origin = nullptr;    // capture/launch stream (never the legacy default)
   cudaGraphExec_t exec = nullptr;
   int graph_check_int = -1;
   double graph_up = 0.0;
 };
 
 namespace {
+
+struct StreamRestore {
+  cudaStream_t prev = current_stream();
+  ~StreamRestore() { gasp_set_stream(prev); }
+};
 
 int batch_release(gasp_batch *b) {
   if (!b) return GASP_OK;
@@ -143,6 +149,7 @@ int batch_release(gasp_batch *b) {
   cudaFree(b->d_small);
   cudaFree(b->d_counts);
   for (auto s : b->streams) cudaStreamDestroy(s);
+  if (b->origin) cudaStreamDestroy(b->origin);
   for (auto e : b->events) cudaEventDestroy(e);
   delete b;
   return GASP_OK;
@@ -242,6 +249,8 @@ int gasp_batch_create(const gasp_group_t *groups, int ngroups, unsigned long lon
     if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) rc = GASP_ERR_CUDA;
     else b->events.push_back(ev);
   }
+  if (rc == GASP_OK && cudaStreamCreateWithFlags(&b->origin, cudaStreamNonBlocking) != cudaSuccess)
+    rc = GASP_ERR_CUDA;
   if (rc == GASP_OK && cudaMalloc(&b->d_small, (size_t)2 * ngroups * sizeof(int)) != cudaSuccess)
     rc = GASP_ERR_ALLOC;
   if (rc) {
@@ -261,7 +270,11 @@ int gasp_batch_swarm(gasp_batch_t *b, int tot_nsweeps, int check_int, double up_
     return GASP_ERR_INVALID;
   const int nint = tot_nsweeps / check_int;
   int rc;
-  cudaStream_t s = current_stream();
+  // All batch work runs on the batch's own stream; the caller's stream
+  // choice is restored on return.
+  const StreamRestore restore_stream;
+  cudaStream_t s = b->origin;
+  GASP_CUDA(cudaStreamSynchronize(restore_stream.prev));
   if (nint > b->max_intervals) {
     cudaFree(b->d_counts);
     b->d_counts = nullptr;
@@ -353,7 +366,11 @@ int gasp_batch_swarm(gasp_batch_t *b, int tot_nsweeps, int check_int, double up_
 
 int gasp_batch_autotune(gasp_batch_t *b, int nsweeps, int *choice_out) {
   if (!b || nsweeps <= 0) return GASP_ERR_INVALID;
-  cudaStream_t s = current_stream();
+  // All batch work runs on the batch's own stream; the caller's stream
+  // choice is restored on return.
+  const StreamRestore restore_stream;
+  cudaStream_t s = b->origin;
+  GASP_CUDA(cudaStreamSynchronize(restore_stream.prev));
   cudaEvent_t e0, e1;
   GASP_CUDA(cudaEventCreate(&e0));
   GASP_CUDA(cudaEventCreate(&e1));

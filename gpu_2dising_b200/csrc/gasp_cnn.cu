@@ -1,0 +1,621 @@
+// gasp_cnn.cu -- the committor surrogate network on sm_100a (no reference
+// counterpart).  4 circular 3x3 convolutions (1->32, 32->32 x3) + ReLU,
+// global average pool, 32->1 linear, sigmoid; binomial cross-entropy; Adam.
+//
+// Convolutions (forward, and the data gradient of the backward pass) are
+// implicit GEMMs on the 5th-generation tensor cores: per CTA a 128-pixel tile,
+// D[128 x 32] (FP32, in TMEM) = A[128 x K] (im2col, BF16) * B[32 x K]^T
+// (weights, BF16), K = 9 taps * 32 channels = 288 (16 for the first layer).
+// Both operands are staged K-major in shared memory in the no-swizzle
+// interleaved layout (8x8 core matrices, leading-byte offset 128 B between
+// k-chunks, stride-byte offset K*16 B between 8-row groups); one thread
+// issues K/16 tcgen05.mma (kind::f16, M=128, N=32), a tcgen05.commit arrives
+// on an mbarrier, and every warp reads its 32 rows of D with tcgen05.ld.
+// Weight gradients are FP32 reductions over pixels on the CUDA cores.
+//
+// Activations: BF16, [image][pixel][32 channels] (pixel = row*L + col).
+#include <cuda_bf16.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "gasp_internal.h"
+
+namespace gasp {
+namespace {
+
+constexpr int kC = 32;
+constexpr int kTileM = 128;
+constexpr int kWaitLimit = 1 << 26;  // bounded mbarrier wait (iterations)
+
+// Flat FP32 parameter offsets (same order as the CPU oracle).
+constexpr int kOffW1 = 0, kOffB1 = 288, kOffW2 = 320, kOffB2 = 320 + 9216;
+constexpr int kOffW3 = kOffB2 + 32, kOffB3 = kOffW3 + 9216;
+constexpr int kOffW4 = kOffB3 + 32, kOffB4 = kOffW4 + 9216;
+constexpr int kOffWf = kOffB4 + 32, kOffBf = kOffWf + 32;
+constexpr int kNParam = kOffBf + 1;  // 28097
+static_assert(kNParam == 28097, "parameter count");
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// UMMA shared-memory descriptor: no swizzle, K-major interleaved layout.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1u << 46;  // descriptor version for sm_100
+  return d;                 // base offset 0, layout type 0 (no swizzle)
+}
+
+// Instruction descriptor: D F32, A/B BF16, both K-major, N=32, M=128.
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((32u >> 3) << 17) |
+                            ((128u >> 4) << 24);
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db,
+                                          uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+      "l"(da), "l"(db), "r"(kIdesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t mbar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   mbar)
+               : "memory");
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t mbar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar), "r"(count) : "memory");
+}
+
+// Bounded wait for phase `parity` of an mbarrier; false on timeout.
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
+  for (int it = 0; it < kWaitLimit; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred P1;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, P1;\n\t}\n"
+        : "=r"(done)
+        : "r"(mbar), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
+      "%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+        "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]),
+        "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]),
+        "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// Byte offset of element (row, k) in the interleaved K-major layout.
+__device__ __forceinline__ uint32_t il_off(int row, int k, int sbo) {
+  return (uint32_t)((row >> 3) * sbo + (k >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2);
+}
+
+__device__ __forceinline__ int nbr(int p, int tap, int L) {
+  const int y = p / L, x = p - y * L;
+  const int dy = tap / 3 - 1, dx = tap % 3 - 1;
+  const int yy = (y + dy + L) % L, xx = (x + dx + L) % L;
+  return yy * L + xx;
+}
+
+enum { kFwd1 = 0, kFwd = 1, kBwd = 2 };
+
+struct ConvArgs {
+  int L;
+  const int8_t *spins;           // kFwd1: [B][N]
+  const __nv_bfloat16 *x;        // kFwd: activations in; kBwd: dZ of this layer
+  const __nv_bfloat16 *w;        // [32][K] (kBwd: transposed weights)
+  const float *bias;             // kFwd1/kFwd
+  __nv_bfloat16 *y;              // kFwd: activations out; kBwd: dZ of the previous layer
+  const __nv_bfloat16 *mask_src; // kBwd: activations of the previous layer (ReLU mask)
+  float *pool;                   // layer 4 forward: per-image channel sums [B][32]
+  int *err;                      // set on a timed-out wait
+};
+
+template <int MODE>
+__global__ void __launch_bounds__(128) k_conv_tc(ConvArgs a) {
+  constexpr int K = (MODE == kFwd1) ? 16 : 9 * kC;
+  constexpr int SBO = K * 16;  // bytes between 8-row groups
+  extern __shared__ __align__(1024) unsigned char smem[];
+  unsigned char *sA = smem;                               // 128 x K bf16
+  unsigned char *sB = smem + kTileM * K * 2;              // 32 x K bf16
+  uint64_t *mbar = reinterpret_cast<uint64_t *>(sB + kC * K * 2);
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(mbar + 1);
+  float *red = reinterpret_cast<float *>(tslot + 4);     // [128][33] (pool)
+
+  const int L = a.L, N = L * L;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int tiles_per_img = N / kTileM;
+  const int img = blockIdx.x / tiles_per_img;
+  const int p = (blockIdx.x % tiles_per_img) * kTileM + tid;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(tslot)),
+                 "r"(32)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    mbar_init(smem_u32(mbar), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+
+  // ---- stage A (im2col row of this thread's pixel) ----
+  if constexpr (MODE == kFwd1) {
+    const int8_t *s = a.spins + (size_t)img * N;
+    __align__(16) __nv_bfloat16 v[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k)
+      v[k] = __float2bfloat16_rn(k < 9 ? (float)s[nbr(p, k, L)] : 0.0f);
+    *reinterpret_cast<uint4 *>(sA + il_off(tid, 0, SBO)) = *reinterpret_cast<uint4 *>(&v[0]);
+    *reinterpret_cast<uint4 *>(sA + il_off(tid, 8, SBO)) = *reinterpret_cast<uint4 *>(&v[8]);
+  } else {
+    const __nv_bfloat16 *x = a.x + (size_t)img * N * kC;
+#pragma unroll 1
+    for (int tap = 0; tap < 9; ++tap) {
+      // forward reads the tap's neighbour; the data gradient the opposite one
+      const int q = nbr(p, MODE == kBwd ? 8 - tap : tap, L);
+      const uint4 *src = reinterpret_cast<const uint4 *>(x + (size_t)q * kC);
+#pragma unroll
+      for (int c = 0; c < 4; ++c)
+        *reinterpret_cast<uint4 *>(sA + il_off(tid, tap * kC + 8 * c, SBO)) = src[c];
+    }
+  }
+  // ---- stage B (32 x K weights) ----
+  for (int i = tid; i < kC * (K / 8); i += blockDim.x) {
+    const int n = i / (K / 8), kc = i % (K / 8);
+    *reinterpret_cast<uint4 *>(sB + il_off(n, kc * 8, SBO)) =
+        *reinterpret_cast<const uint4 *>(a.w + (size_t)n * K + kc * 8);
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t taddr = *tslot;
+
+  if (tid == 0) {
+    const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
+#pragma unroll
+    for (int j = 0; j < K / 16; ++j)
+      umma_bf16(taddr, umma_desc(a0 + j * 256, 128, SBO), umma_desc(b0 + j * 256, 128, SBO),
+                j > 0 ? 1u : 0u);
+    umma_commit(smem_u32(mbar));
+  }
+  const bool ok = mbar_wait(smem_u32(mbar), 0);
+  if (!ok && a.err) atomicExch(a.err, 1);
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  float acc[32];
+  tmem_ld32(taddr + ((uint32_t)(warp * 32) << 16), acc);
+
+  // ---- epilogue: this thread owns pixel p's 32 channels ----
+  if (ok) {
+    __align__(16) __nv_bfloat16 o[32];
+    if constexpr (MODE == kBwd) {
+      const __nv_bfloat16 *m = a.mask_src + ((size_t)img * N + p) * kC;
+#pragma unroll
+      for (int c = 0; c < 32; ++c)
+        o[c] = __float2bfloat16_rn(__bfloat162float(m[c]) > 0.0f ? acc[c] : 0.0f);
+    } else {
+#pragma unroll
+      for (int c = 0; c < 32; ++c) {
+        const float z = acc[c] + a.bias[c];
+        acc[c] = z > 0.0f ? z : 0.0f;
+        o[c] = __float2bfloat16_rn(acc[c]);
+      }
+    }
+    uint4 *dst = reinterpret_cast<uint4 *>(a.y + ((size_t)img * N + p) * kC);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) dst[c] = reinterpret_cast<uint4 *>(o)[c];
+    if (MODE == kFwd && a.pool != nullptr) {
+      // channel sums of the rounded activations over the tile
+#pragma unroll
+      for (int c = 0; c < 32; ++c) red[tid * 33 + c] = __bfloat162float(o[c]);
+    }
+  }
+  if (MODE == kFwd && a.pool != nullptr) {
+    __syncthreads();
+    if (ok && tid < 32) {
+      float sum = 0.f;
+      for (int r = 0; r < kTileM; ++r) sum += red[r * 33 + tid];
+      atomicAdd(&a.pool[img * kC + tid], sum);
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(32)
+                 : "memory");
+  }
+}
+
+size_t conv_smem(int mode) {
+  const int K = mode == kFwd1 ? 16 : 9 * kC;
+  return (size_t)kTileM * K * 2 + (size_t)kC * K * 2 + 64 + (size_t)kTileM * 33 * 4;
+}
+
+// FP32 weight gradient of one layer: dW[co][k] += sum_p dZ[p][co] * X[p, k]
+// with X[p, tap*Cin + ci] = input[nbr(p, tap)][ci]; db[co] += sum_p dZ[p][co].
+// Thread t accumulates co = t/8 and k = (t%8) + 8j.  CTAs stride over 32-pixel
+// chunks of the whole batch, then add their partial sums atomically.
+template <int CIN>
+__global__ void __launch_bounds__(256) k_conv_dw(int L, int B, const __nv_bfloat16 *dz,
+                                                 const __nv_bfloat16 *xin, const int8_t *spins,
+                                                 float *dW, float *db) {
+  constexpr int K = 9 * CIN;
+  constexpr int KPT = (K + 7) / 8;  // k values per thread
+  constexpr int P = 32;             // pixels per chunk (static shared memory < 48 KB)
+  __shared__ float s_dz[P][kC + 1];
+  __shared__ float s_x[P][K + 1];
+  const int N = L * L;
+  const int tid = threadIdx.x;
+  const int co = tid >> 3, k0 = tid & 7;
+  float acc[KPT];
+#pragma unroll
+  for (int j = 0; j < KPT; ++j) acc[j] = 0.f;
+  float accb = 0.f;
+  const long long nchunks = (long long)B * N / P;
+  for (long long ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
+    const long long pix0 = ch * P;
+    const int img = (int)(pix0 / N);
+    const int p0 = (int)(pix0 % N);
+    for (int i = tid; i < P * kC; i += blockDim.x) {
+      const int r = i / kC, c = i % kC;
+      s_dz[r][c] = __bfloat162float(dz[((size_t)img * N + p0 + r) * kC + c]);
+    }
+    for (int i = tid; i < P * K; i += blockDim.x) {
+      const int r = i / K, k = i % K;
+      const int tap = k / CIN, ci = k % CIN;
+      const int q = nbr(p0 + r, tap, L);
+      float v;
+      if constexpr (CIN == 1) v = (float)spins[(size_t)img * N + q];
+      else v = __bfloat162float(xin[((size_t)img * N + q) * kC + ci]);
+      s_x[r][k] = v;
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int r = 0; r < P; ++r) {
+      const float g = s_dz[r][co];
+#pragma unroll
+      for (int j = 0; j < KPT; ++j) {
+        const int k = k0 + 8 * j;
+        if (k < K) acc[j] += g * s_x[r][k];
+      }
+      if (k0 == 0) accb += g;
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int j = 0; j < KPT; ++j) {
+    const int k = k0 + 8 * j;
+    if (k < K) atomicAdd(&dW[co * K + k], acc[j]);
+  }
+  if (k0 == 0) atomicAdd(&db[co], accb);
+}
+
+// Head: mean pool -> linear -> sigmoid -> cross-entropy; one warp per image,
+// lane = channel.  Writes q, adds the mean loss, the head's gradients and
+// dmean[b][c] = dL/d(pooled mean).
+__global__ void k_head(int B, int N, const float *pool, const float *params, const float *labels,
+                       float *q_out, float *loss, float *grad, float *dmean) {
+  const int b = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int c = threadIdx.x & 31;
+  if (b >= B) return;
+  const float m = pool[b * kC + c] / (float)N;
+  float z = m * params[kOffWf + c];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) z += __shfl_xor_sync(0xffffffffu, z, o);
+  z += params[kOffBf];
+  const float q = 1.0f / (1.0f + expf(-z));
+  if (q_out && c == 0) q_out[b] = q;
+  if (labels) {
+    const float y = labels[b];
+    const float dz = (q - y) / (float)B;
+    if (c == 0) {
+      const float qc = fminf(fmaxf(q, 1e-7f), 1.0f - 1e-7f);
+      atomicAdd(loss, -(y * logf(qc) + (1.0f - y) * logf(1.0f - qc)) / (float)B);
+      atomicAdd(&grad[kOffBf], dz);
+    }
+    atomicAdd(&grad[kOffWf + c], dz * m);
+    dmean[b * kC + c] = dz * params[kOffWf + c];
+  }
+}
+
+// dZ4 = dmean / N on every pixel where the layer-4 activation is positive.
+__global__ void k_dz4(int B, int N, const float *dmean, const __nv_bfloat16 *a4,
+                      __nv_bfloat16 *dz4) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (long long)B * N * kC) return;
+  const int c = (int)(i % kC);
+  const long long b = i / ((long long)N * kC);
+  const float g = __bfloat162float(a4[i]) > 0.0f ? dmean[b * kC + c] / (float)N : 0.0f;
+  dz4[i] = __float2bfloat16_rn(g);
+}
+
+// BF16 copies of the weights: W1 [32][16] (taps padded), W2..4 [32][288]
+// (k = tap*32 + ci) and their transposes WT [ci][tap*32 + co].
+__global__ void k_pack_weights(const float *params, __nv_bfloat16 *w1, __nv_bfloat16 *w,
+                               __nv_bfloat16 *wt) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < kC * 16) {
+    const int co = i / 16, k = i % 16;
+    w1[i] = __float2bfloat16_rn(k < 9 ? params[kOffW1 + co * 9 + k] : 0.0f);
+  }
+  if (i < 3 * 9216) {
+    const int l = i / 9216, r = i % 9216;
+    const int co = r / 288, k = r % 288, tap = k / kC, ci = k % kC;
+    const float v = params[kOffW2 + l * (9216 + 32) + r];
+    w[i] = __float2bfloat16_rn(v);
+    wt[l * 9216 + ci * 288 + tap * kC + co] = __float2bfloat16_rn(v);
+  }
+}
+
+__global__ void k_adam(float *params, const float *grad, float *m, float *v, int n, float lr,
+                       float b1, float b2, float eps, float c1, float c2) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float g = grad[i];
+  const float mi = b1 * m[i] + (1.0f - b1) * g;
+  const float vi = b2 * v[i] + (1.0f - b2) * g * g;
+  m[i] = mi;
+  v[i] = vi;
+  params[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+}
+
+}  // namespace
+}  // namespace gasp
+
+using namespace gasp;
+
+struct gasp_cnn {
+  int device, L, N, max_batch;
+  float *d_params, *d_grad, *d_m, *d_v;
+  __nv_bfloat16 *d_w1, *d_w, *d_wt;
+  int8_t *d_spins;
+  float *d_labels, *d_q, *d_pool, *d_dmean, *d_loss;
+  __nv_bfloat16 *d_act[4];  // a1..a4
+  __nv_bfloat16 *d_dz[2];   // ping-pong data gradients
+  int *d_err;
+  int adam_t;
+};
+
+namespace {
+
+int cnn_upload(gasp_cnn *c, const int8_t *spins, const float *labels, int batch) {
+  cudaStream_t s = current_stream();
+  GASP_CUDA(cudaMemcpyAsync(c->d_spins, spins, (size_t)batch * c->N, cudaMemcpyHostToDevice, s));
+  if (labels)
+    GASP_CUDA(cudaMemcpyAsync(c->d_labels, labels, (size_t)batch * sizeof(float),
+                              cudaMemcpyHostToDevice, s));
+  return GASP_OK;
+}
+
+template <int MODE>
+int launch_conv(const ConvArgs &a, int batch, cudaStream_t s) {
+  const size_t smem = conv_smem(MODE);
+  GASP_CUDA(cudaFuncSetAttribute(k_conv_tc<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem));
+  const int grid = batch * (a.L * a.L / kTileM);
+  k_conv_tc<MODE><<<grid, 128, smem, s>>>(a);
+  GASP_CUDA(cudaGetLastError());
+  return GASP_OK;
+}
+
+int cnn_forward(gasp_cnn *c, int batch, cudaStream_t s) {
+  int rc;
+  const int B = batch;
+  k_pack_weights<<<(3 * 9216 + 255) / 256, 256, 0, s>>>(c->d_params, c->d_w1, c->d_w, c->d_wt);
+  GASP_CUDA(cudaGetLastError());
+  GASP_CUDA(cudaMemsetAsync(c->d_pool, 0, (size_t)B * kC * sizeof(float), s));
+  ConvArgs a;
+  memset(&a, 0, sizeof a);
+  a.L = c->L;
+  a.err = c->d_err;
+  a.spins = c->d_spins;
+  a.w = c->d_w1;
+  a.bias = c->d_params + kOffB1;
+  a.y = c->d_act[0];
+  if ((rc = launch_conv<kFwd1>(a, B, s))) return rc;
+  for (int l = 0; l < 3; ++l) {
+    a.x = c->d_act[l];
+    a.w = c->d_w + l * 9216;
+    a.bias = c->d_params + kOffB2 + l * (9216 + 32);
+    a.y = c->d_act[l + 1];
+    a.pool = (l == 2) ? c->d_pool : nullptr;
+    if ((rc = launch_conv<kFwd>(a, B, s))) return rc;
+  }
+  return GASP_OK;
+}
+
+int cnn_check_err(gasp_cnn *c, cudaStream_t s) {
+  int err = 0;
+  GASP_CUDA(cudaMemcpyAsync(&err, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, s));
+  GASP_CUDA(cudaStreamSynchronize(s));
+  if (err) {
+    set_error("tensor-core wait timed out");
+    return GASP_ERR_TIMEOUT;
+  }
+  return GASP_OK;
+}
+
+// Forward + loss + all gradients (into d_grad) for the uploaded batch.
+int cnn_backward(gasp_cnn *c, int batch, cudaStream_t s) {
+  int rc;
+  const int B = batch, N = c->N;
+  GASP_CUDA(cudaMemsetAsync(c->d_grad, 0, kNParam * sizeof(float), s));
+  GASP_CUDA(cudaMemsetAsync(c->d_loss, 0, sizeof(float), s));
+  if ((rc = cnn_forward(c, B, s))) return rc;
+  k_head<<<(B + 7) / 8, 256, 0, s>>>(B, N, c->d_pool, c->d_params, c->d_labels, c->d_q, c->d_loss,
+                                     c->d_grad, c->d_dmean);
+  GASP_CUDA(cudaGetLastError());
+  const long long tot = (long long)B * N * kC;
+  k_dz4<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(B, N, c->d_dmean, c->d_act[3], c->d_dz[0]);
+  GASP_CUDA(cudaGetLastError());
+  int cur = 0;
+  const int dw_grid = 148 * 4;
+  for (int l = 3; l >= 1; --l) {  // layers 4, 3, 2 (0-based l)
+    float *gW = c->d_grad + kOffW2 + (l - 1) * (9216 + 32);
+    k_conv_dw<kC><<<dw_grid, 256, 0, s>>>(c->L, B, c->d_dz[cur], c->d_act[l - 1], nullptr, gW,
+                                          gW + 9216);
+    GASP_CUDA(cudaGetLastError());
+    ConvArgs a;
+    memset(&a, 0, sizeof a);
+    a.L = c->L;
+    a.err = c->d_err;
+    a.x = c->d_dz[cur];
+    a.w = c->d_wt + (l - 1) * 9216;
+    a.y = c->d_dz[cur ^ 1];
+    a.mask_src = c->d_act[l - 1];
+    if ((rc = launch_conv<kBwd>(a, B, s))) return rc;
+    cur ^= 1;
+  }
+  k_conv_dw<1><<<dw_grid, 256, 0, s>>>(c->L, B, c->d_dz[cur], nullptr, c->d_spins,
+                                       c->d_grad + kOffW1, c->d_grad + kOffB1);
+  GASP_CUDA(cudaGetLastError());
+  return GASP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gasp_cnn_param_count(void) { return kNParam; }
+
+int gasp_cnn_create(int L, int max_batch, gasp_cnn_t **out) {
+  if (!out || max_batch <= 0 || L <= 0 || (L * L) % kTileM != 0) {
+    set_error("gasp_cnn_create: L*L must be a multiple of 128 and max_batch positive");
+    return GASP_ERR_INVALID;
+  }
+  *out = nullptr;
+  gasp_cnn *c = new (std::nothrow) gasp_cnn();
+  if (!c) return GASP_ERR_ALLOC;
+  memset(c, 0, sizeof *c);
+  cudaGetDevice(&c->device);
+  c->L = L;
+  c->N = L * L;
+  c->max_batch = max_batch;
+  const size_t act = (size_t)max_batch * c->N * kC * sizeof(__nv_bfloat16);
+  cudaError_t e = cudaSuccess;
+  auto A = [&](void **p, size_t n) {
+    if (e == cudaSuccess) e = cudaMalloc(p, n);
+  };
+  A((void **)&c->d_params, kNParam * sizeof(float));
+  A((void **)&c->d_grad, kNParam * sizeof(float));
+  A((void **)&c->d_m, kNParam * sizeof(float));
+  A((void **)&c->d_v, kNParam * sizeof(float));
+  A((void **)&c->d_w1, 32 * 16 * sizeof(__nv_bfloat16));
+  A((void **)&c->d_w, 3 * 9216 * sizeof(__nv_bfloat16));
+  A((void **)&c->d_wt, 3 * 9216 * sizeof(__nv_bfloat16));
+  A((void **)&c->d_spins, (size_t)max_batch * c->N);
+  A((void **)&c->d_labels, (size_t)max_batch * sizeof(float));
+  A((void **)&c->d_q, (size_t)max_batch * sizeof(float));
+  A((void **)&c->d_pool, (size_t)max_batch * kC * sizeof(float));
+  A((void **)&c->d_dmean, (size_t)max_batch * kC * sizeof(float));
+  A((void **)&c->d_loss, sizeof(float));
+  A((void **)&c->d_err, sizeof(int));
+  for (int i = 0; i < 4; ++i) A((void **)&c->d_act[i], act);
+  for (int i = 0; i < 2; ++i) A((void **)&c->d_dz[i], act);
+  if (e == cudaSuccess) e = cudaMemset(c->d_params, 0, kNParam * sizeof(float));
+  if (e == cudaSuccess) e = cudaMemset(c->d_m, 0, kNParam * sizeof(float));
+  if (e == cudaSuccess) e = cudaMemset(c->d_v, 0, kNParam * sizeof(float));
+  if (e == cudaSuccess) e = cudaMemset(c->d_err, 0, sizeof(int));
+  if (e != cudaSuccess) {
+    gasp_cnn_free(c);
+    return cuda_fail(e, "gasp_cnn_create", __FILE__, __LINE__);
+  }
+  *out = c;
+  return GASP_OK;
+}
+
+int gasp_cnn_free(gasp_cnn_t *c) {
+  if (!c) return GASP_OK;
+  void *ptrs[] = {c->d_params, c->d_grad, c->d_m, c->d_v, c->d_w1, c->d_w, c->d_wt, c->d_spins,
+                  c->d_labels, c->d_q, c->d_pool, c->d_dmean, c->d_loss, c->d_err,
+                  c->d_act[0], c->d_act[1], c->d_act[2], c->d_act[3], c->d_dz[0], c->d_dz[1]};
+  for (void *p : ptrs) cudaFree(p);
+  delete c;
+  return GASP_OK;
+}
+
+int gasp_cnn_set_params(gasp_cnn_t *c, const float *params) {
+  if (!c || !params) return GASP_ERR_INVALID;
+  GASP_CUDA(cudaMemcpy(c->d_params, params, kNParam * sizeof(float), cudaMemcpyHostToDevice));
+  GASP_CUDA(cudaMemset(c->d_m, 0, kNParam * sizeof(float)));
+  GASP_CUDA(cudaMemset(c->d_v, 0, kNParam * sizeof(float)));
+  c->adam_t = 0;
+  return GASP_OK;
+}
+
+int gasp_cnn_get_params(gasp_cnn_t *c, float *params) {
+  if (!c || !params) return GASP_ERR_INVALID;
+  GASP_CUDA(cudaMemcpy(params, c->d_params, kNParam * sizeof(float), cudaMemcpyDeviceToHost));
+  return GASP_OK;
+}
+
+int gasp_cnn_predict(gasp_cnn_t *c, const int8_t *spins, int batch, float *q_out) {
+  if (!c || !spins || !q_out || batch <= 0 || batch > c->max_batch) return GASP_ERR_INVALID;
+  cudaStream_t s = current_stream();
+  int rc;
+  if ((rc = cnn_upload(c, spins, nullptr, batch))) return rc;
+  if ((rc = cnn_forward(c, batch, s))) return rc;
+  k_head<<<(batch + 7) / 8, 256, 0, s>>>(batch, c->N, c->d_pool, c->d_params, nullptr, c->d_q,
+                                         nullptr, nullptr, nullptr);
+  GASP_CUDA(cudaGetLastError());
+  GASP_CUDA(cudaMemcpyAsync(q_out, c->d_q, (size_t)batch * sizeof(float), cudaMemcpyDeviceToHost, s));
+  return cnn_check_err(c, s);
+}
+
+int gasp_cnn_gradients(gasp_cnn_t *c, const int8_t *spins, const float *labels, int batch,
+                       float *loss_out, float *grad_out) {
+  if (!c || !spins || !labels || batch <= 0 || batch > c->max_batch) return GASP_ERR_INVALID;
+  cudaStream_t s = current_stream();
+  int rc;
+  if ((rc = cnn_upload(c, spins, labels, batch))) return rc;
+  if ((rc = cnn_backward(c, batch, s))) return rc;
+  if (loss_out) GASP_CUDA(cudaMemcpyAsync(loss_out, c->d_loss, sizeof(float), cudaMemcpyDeviceToHost, s));
+  if (grad_out)
+    GASP_CUDA(cudaMemcpyAsync(grad_out, c->d_grad, kNParam * sizeof(float), cudaMemcpyDeviceToHost, s));
+  return cnn_check_err(c, s);
+}
+
+int gasp_cnn_train_step(gasp_cnn_t *c, const int8_t *spins, const float *labels, int batch,
+                        float lr, float *loss_out) {
+  if (!c || !spins || !labels || batch <= 0 || batch > c->max_batch) return GASP_ERR_INVALID;
+  cudaStream_t s = current_stream();
+  int rc;
+  if ((rc = cnn_upload(c, spins, labels, batch))) return rc;
+  if ((rc = cnn_backward(c, batch, s))) return rc;
+  c->adam_t++;
+  const float b1 = 0.9f, b2 = 0.999f;
+  const float c1 = 1.0f - powf(b1, (float)c->adam_t), c2 = 1.0f - powf(b2, (float)c->adam_t);
+  k_adam<<<(kNParam + 255) / 256, 256, 0, s>>>(c->d_params, c->d_grad, c->d_m, c->d_v, kNParam,
+                                               lr, b1, b2, 1e-8f, c1, c2);
+  GASP_CUDA(cudaGetLastError());
+  if (loss_out) GASP_CUDA(cudaMemcpyAsync(loss_out, c->d_loss, sizeof(float), cudaMemcpyDeviceToHost, s));
+  return cnn_check_err(c, s);
+}
+
+}  // extern "C"

@@ -668,21 +668,21 @@ int dispatch_kind(const SweepLaunch &p, cudaStream_t s) {
     return launch_tiles(p.L == 64 ? k_sweep_exact<64, F, K> : k_sweep_exact<0, F, K>, p, s);
   }
   const size_t dyn128 = (size_t)words_per_replica(128) * kTile * sizeof(uint32_t);
-  if (p.variant == 2) {  // row kernel without pairwise speculation
+  if (p.variant == 3) {  // row kernel with pairwise speculation (measured slower)
     switch (p.L) {
-      case 32: return launch_rows(k_sweep_rows<32, true, F, K>, p, 0, s);
-      case 64: return launch_rows(k_sweep_rows<64, true, F, K>, p, 0, s);
-      case 128: return launch_rows(k_sweep_rows<128, false, F, K>, p, dyn128, s);
+      case 32: return launch_rows(k_sweep_rows_pair<32, true, F, K>, p, 0, s);
+      case 64: return launch_rows(k_sweep_rows_pair<64, true, F, K>, p, 0, s);
+      case 128: return launch_rows(k_sweep_rows_pair<128, false, F, K>, p, dyn128, s);
       default: break;
     }
   }
-  switch (p.L) {
+  switch (p.L) {  // variants 0 and 2: the software-pipelined row kernel
     case 16: return launch_tiles(k_sweep_exact<16, F, K>, p, s);
-    case 32: return launch_rows(k_sweep_rows_pair<32, true, F, K>, p, 0, s);
+    case 32: return launch_rows(k_sweep_rows<32, true, F, K>, p, 0, s);
     case 48: return launch_tiles(k_sweep_exact<48, F, K>, p, s);
-    case 64: return launch_rows(k_sweep_rows_pair<64, true, F, K>, p, 0, s);
+    case 64: return launch_rows(k_sweep_rows<64, true, F, K>, p, 0, s);
     case 96: return launch_tiles(k_sweep_exact<96, F, K>, p, s);
-    case 128: return launch_rows(k_sweep_rows_pair<128, false, F, K>, p, dyn128, s);
+    case 128: return launch_rows(k_sweep_rows<128, false, F, K>, p, dyn128, s);
     default: return launch_tiles(k_sweep_exact<0, F, K>, p, s);
   }
 }

@@ -1,0 +1,229 @@
+"""Learned committor surrogate: a small CNN trained on pB labels produced by
+this library's own shooting runs, used to screen grids before shooting.
+
+* ``CommittorCNN``: the network of include/gasp.h (gasp_cnn_*): forward,
+  gradients and Adam steps all run on the GPU (tcgen05 convolutions).
+* ``harvest_snapshots``: grids snapshotted from a nucleation swarm while
+  still between the basins.
+* ``shoot``: pB (and the reference's bootstrap error) of each grid by
+  committor shooting with compaction.
+* ``screen``: surrogate prediction for every grid, shooting fallback for
+  grids predicted near pB = 0.5.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import time
+
+import numpy as np
+
+from . import _native as nat
+from . import engine
+from ._native import check, lib
+
+NPARAM = 28097
+_SHAPES = [(32, 9, 1), (32,), (32, 9, 32), (32,), (32, 9, 32), (32,), (32, 9, 32), (32,),
+           (32,), (1,)]
+
+
+def init_params(seed=0):
+    """He-normal convolution weights, N(0, 0.1) head weights, zero biases."""
+    rs = np.random.default_rng(seed)
+    parts = []
+    for i, shp in enumerate(_SHAPES):
+        if len(shp) == 3:
+            parts.append(rs.normal(0.0, np.sqrt(2.0 / (shp[1] * shp[2])), shp).ravel())
+        elif i == 8:
+            parts.append(rs.normal(0.0, 0.1, shp))
+        else:
+            parts.append(np.zeros(shp))
+    out = np.concatenate(parts).astype(np.float32)
+    assert out.size == NPARAM
+    return out
+
+
+class CommittorCNN:
+    """Handle on a gasp_cnn_t (parameters, Adam state, activations on the GPU)."""
+
+    def __init__(self, L=64, max_batch=1024, params=None, seed=0):
+        assert lib().gasp_cnn_param_count() == NPARAM
+        self.L, self.max_batch = int(L), int(max_batch)
+        self._h = C.c_void_p()
+        check(lib().gasp_cnn_create(self.L, self.max_batch, C.byref(self._h)), "gasp_cnn_create")
+        self.set_params(init_params(seed) if params is None else params)
+
+    def set_params(self, params):
+        p = np.ascontiguousarray(params, np.float32)
+        assert p.size == NPARAM
+        check(lib().gasp_cnn_set_params(self._h, p), "gasp_cnn_set_params")
+
+    def get_params(self):
+        out = np.empty(NPARAM, np.float32)
+        check(lib().gasp_cnn_get_params(self._h, out), "gasp_cnn_get_params")
+        return out
+
+    def _spins(self, grids):
+        g = np.ascontiguousarray(grids, np.int8).reshape(-1, self.L, self.L)
+        return g
+
+    def predict(self, grids):
+        g = self._spins(grids)
+        out = np.empty(g.shape[0], np.float32)
+        for i in range(0, g.shape[0], self.max_batch):
+            chunk = np.ascontiguousarray(g[i:i + self.max_batch])
+            q = np.empty(chunk.shape[0], np.float32)
+            check(lib().gasp_cnn_predict(self._h, chunk.reshape(-1), chunk.shape[0], q),
+                  "gasp_cnn_predict")
+            out[i:i + chunk.shape[0]] = q
+        return out
+
+    def gradients(self, grids, labels):
+        g = self._spins(grids)
+        y = np.ascontiguousarray(labels, np.float32)
+        loss = C.c_float()
+        grad = np.empty(NPARAM, np.float32)
+        check(lib().gasp_cnn_gradients(self._h, g.reshape(-1), y, g.shape[0], C.byref(loss),
+                                       grad), "gasp_cnn_gradients")
+        return float(loss.value), grad
+
+    def train_step(self, grids, labels, lr):
+        g = self._spins(grids)
+        y = np.ascontiguousarray(labels, np.float32)
+        loss = C.c_float()
+        check(lib().gasp_cnn_train_step(self._h, g.reshape(-1), y, g.shape[0], float(lr),
+                                        C.byref(loss)), "gasp_cnn_train_step")
+        return float(loss.value)
+
+    def train(self, grids, labels, epochs=20, batch=256, lr=2e-3, seed=0, augment=True,
+              val=None, log=None):
+        """Mini-batch Adam.  augment: random lattice translations and the
+        8 square symmetries (the Hamiltonian's), which leave pB unchanged."""
+        g = self._spins(grids)
+        y = np.asarray(labels, np.float32)
+        rs = np.random.default_rng(seed)
+        hist = []
+        for ep in range(epochs):
+            order = rs.permutation(g.shape[0])
+            losses = []
+            for i in range(0, g.shape[0] - batch + 1, batch):
+                idx = order[i:i + batch]
+                xb = g[idx]
+                if augment:
+                    xb = _augment(xb, rs)
+                losses.append(self.train_step(xb, y[idx], lr))
+            rec = {"epoch": ep, "loss": float(np.mean(losses)) if losses else float("nan")}
+            if val is not None:
+                rec["val_mae"] = float(np.mean(np.abs(self.predict(val[0]) - val[1])))
+            hist.append(rec)
+            if log:
+                log(rec)
+        return hist
+
+    def close(self):
+        if self._h:
+            lib().gasp_cnn_free(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _augment(xb, rs):
+    out = np.empty_like(xb)
+    L = xb.shape[1]
+    for i in range(xb.shape[0]):
+        x = np.roll(xb[i], (int(rs.integers(L)), int(rs.integers(L))), axis=(0, 1))
+        k = int(rs.integers(4))
+        x = np.rot90(x, k)
+        if rs.integers(2):
+            x = x[:, ::-1]
+        out[i] = x
+    return out
+
+
+def shoot(grids, shots, beta, h, up=0.9, dn=-0.93, cap=20000, check_int=10, seed=1,
+          rng="mwc64x", max_replicas=1 << 19):
+    """pB of each grid from `shots` trajectories (compaction on).  Returns
+    (pB float64[n], attempts, seconds)."""
+    g = np.ascontiguousarray(grids, np.int32)
+    n, L = g.shape[0], g.shape[1]
+    per = max(1, max_replicas // shots)
+    pb = np.empty(n)
+    attempts, t0 = 0, time.perf_counter()
+    for i in range(0, n, per):
+        block = g[i:i + per]
+        k = block.shape[0]
+        host = np.repeat(block, shots, axis=0)
+        dg = engine.DeviceGrids(L, k * shots, host)
+        r = engine.RngStates(k * shots, seed + i, kind=rng)
+        res, fates, _, att = engine.run_driver(dg, r, beta, h, cap, check_int, cap, itask=1,
+                                               dn_thr=dn, up_thr=up, ninputs=k, compact=True)
+        pb[i:i + k] = res
+        attempts += att
+        dg.close()
+        r.close()
+    return pb, attempts, time.perf_counter() - t0
+
+
+def harvest_snapshots(n, L=64, beta=0.54, h=0.07, replicas=32768, tot=12000, every=100,
+                      lo=-0.93, hi=0.9, seed=3, rng="mwc64x", bins=16):
+    """Grids from a nucleation swarm, taken every `every` sweeps while their
+    magnetisation lies in (lo, hi), balanced over `bins` magnetisation bins so
+    that the barrier region is not drowned by metastable states."""
+    dg = engine.DeviceGrids(L, replicas, -np.ones((replicas, L, L), np.int32))
+    r = engine.RngStates(replicas, seed, kind=rng)
+    pool = [[] for _ in range(bins)]
+    cap_per_bin = 4 * n // bins + 1
+    edges = np.linspace(lo, hi, bins + 1)
+
+    def take(L_, ng_, payload, isweep, mag):
+        m = np.asarray(mag, np.float64)
+        sel = np.nonzero((m > lo) & (m < hi))[0]
+        if sel.size == 0:
+            return 0
+        which = np.clip(np.searchsorted(edges, m[sel]) - 1, 0, bins - 1)
+        nb = L_ * L_ // 8  # bytes per grid (L*L is a multiple of 8 here)
+        for b in range(bins):
+            ids = sel[which == b]
+            room = cap_per_bin - len(pool[b])
+            if room > 0 and ids.size:
+                for j in ids[:room]:
+                    bits = np.unpackbits(payload[j * nb:(j + 1) * nb], bitorder="little")
+                    pool[b].append(np.where(bits.reshape(L_, L_) == 1, 1, -1).astype(np.int8))
+        return 0
+
+    engine.run_driver(dg, r, beta, h, tot, every, every, itask=0, dn_thr=-0.95, up_thr=0.999,
+                      packed_out=take)
+    dg.close()
+    r.close()
+    rs = np.random.default_rng(seed)
+    per_bin = max(1, n // bins)
+    out = []
+    for b in range(bins):
+        items = pool[b]
+        if items:
+            idx = rs.permutation(len(items))[:per_bin]
+            out.extend(items[i] for i in idx)
+    rest = [x for b in range(bins) for x in pool[b]]
+    while len(out) < n and rest:
+        out.append(rest[int(rs.integers(len(rest)))])
+    return np.stack(out[:n]) if out else np.zeros((0, L, L), np.int8)
+
+
+def screen(cnn, grids, beta, h, fallback_shots=128, band=0.1, **shoot_kw):
+    """Surrogate pB for every grid; grids predicted within `band` of 0.5 are
+    shot instead.  Returns (pB, fallback mask, seconds)."""
+    t0 = time.perf_counter()
+    pred = cnn.predict(grids).astype(np.float64)
+    near = np.abs(pred - 0.5) < band
+    out = pred.copy()
+    if near.any():
+        pb, _, _ = shoot(np.asarray(grids)[near], fallback_shots, beta, h, **shoot_kw)
+        out[near] = pb
+    return out, near, time.perf_counter() - t0
+
+
+__all__ = ["CommittorCNN", "init_params", "shoot", "harvest_snapshots", "screen", "nat"]

@@ -88,9 +88,10 @@ int gasp_grids_download(gasp_grids_t *grids, int *host_grids);
 int gasp_grids_shape(const gasp_grids_t *grids, int *L_out, int *ngrids_out);
 
 /* Launch tuning of a set (no reference counterpart; results never depend on
- * it).  GASP_OPT_SWEEP_VARIANT: 0 the fastest exact kernel for L (default),
- * 1 the generic exact kernel.  GASP_OPT_WARPS_PER_CTA: tiles per CTA of the
- * generic kernel (1..8). */
+ * it).  GASP_OPT_SWEEP_VARIANT: 0 the fastest kernel for L (default), 1 the
+ * generic kernel, 2 the row kernel, 3 the row kernel with pairwise
+ * speculation of consecutive attempts.  GASP_OPT_WARPS_PER_CTA: tiles per
+ * CTA of the generic kernel (1..8). */
 enum { GASP_OPT_SWEEP_VARIANT = 1, GASP_OPT_WARPS_PER_CTA = 2 };
 int gasp_grids_set_option(gasp_grids_t *grids, int option, int value);
 
@@ -268,6 +269,30 @@ int gasp_batch_swarm(gasp_batch_t *batch, int tot_nsweeps, int check_int, double
  * nsweeps run and keeps the fastest.  choice_out (2*ngroups ints, may be
  * NULL): (variant, warps per CTA) chosen per group. */
 int gasp_batch_autotune(gasp_batch_t *batch, int nsweeps, int *choice_out);
+
+/* ---------------------------------------------- committor surrogate CNN */
+/* A small network predicting pB from a spin grid (no reference counterpart):
+ * 4 circular 3x3 convolutions (1->32, then 32->32 three times) each with
+ * ReLU, global average pool, 32->1 linear, sigmoid; BF16 weights and
+ * activations, FP32 accumulation (tcgen05 tensor cores for the
+ * convolutions), binomial cross-entropy loss, Adam.  Parameters are a flat
+ * FP32 vector of gasp_cnn_param_count() values:
+ *   W1[32][9] b1[32] W2[32][9][32] b2[32] W3 b3 W4 b4 Wf[32] bf[1],
+ * tap = (dy+1)*3 + (dx+1), W[co][tap][ci].  Spins are int8 +-1, [B][L][L]
+ * on the host; L*L must be a multiple of 128. */
+typedef struct gasp_cnn gasp_cnn_t;
+int gasp_cnn_param_count(void);
+int gasp_cnn_create(int L, int max_batch, gasp_cnn_t **out);
+int gasp_cnn_free(gasp_cnn_t *cnn);
+int gasp_cnn_set_params(gasp_cnn_t *cnn, const float *params);  /* also resets Adam */
+int gasp_cnn_get_params(gasp_cnn_t *cnn, float *params);
+int gasp_cnn_predict(gasp_cnn_t *cnn, const int8_t *spins, int batch, float *q_out);
+/* Loss (mean over the batch) and its gradient for labels in [0, 1]. */
+int gasp_cnn_gradients(gasp_cnn_t *cnn, const int8_t *spins, const float *labels, int batch,
+                       float *loss_out, float *grad_out);
+/* One Adam step (beta1 0.9, beta2 0.999, eps 1e-8) on the batch. */
+int gasp_cnn_train_step(gasp_cnn_t *cnn, const int8_t *spins, const float *labels, int batch,
+                        float lr, float *loss_out);
 
 /* ---------------------------------------------------- host-side helpers */
 /* Replace init_grids_uniform / init_grids_from_file / init_grids_from_array /

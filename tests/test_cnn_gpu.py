@@ -1,0 +1,71 @@
+"""The surrogate network on a B200: forward pass and gradients of the tcgen05
+convolutions against the FP64 CPU oracle (with the device's bfloat16
+rounding points), and training that learns."""
+import numpy as np
+import pytest
+
+from oracle import cnn as ocnn
+from gpu_2dising_b200 import engine, surrogate
+
+pytestmark = pytest.mark.gpu
+
+L = 64
+
+
+@pytest.fixture(scope="module", autouse=True)
+def device():
+    return engine.init_device(0)
+
+
+def _data(B, seed):
+    rs = np.random.default_rng(seed)
+    # grids with varied magnetisation: a random fraction of +1 spins per grid
+    f = rs.uniform(0.05, 0.95, size=B)
+    g = np.where(rs.random((B, L, L)) < f[:, None, None], 1, -1).astype(np.int8)
+    y = 1.0 / (1.0 + np.exp(-6.0 * g.reshape(B, -1).mean(axis=1)))
+    return g, y.astype(np.float32)
+
+
+def test_forward_matches_oracle():
+    g, _ = _data(6, 1)
+    params = surrogate.init_params(3)
+    net = surrogate.CommittorCNN(L, 8, params)
+    q = net.predict(g)
+    ref = ocnn.forward(params.astype(np.float64), g.astype(np.float64), bf16=True)["q"]
+    assert np.max(np.abs(q - ref)) < 2e-3, (q, ref)
+    # and close to the exact FP64 network
+    exact = ocnn.forward(params.astype(np.float64), g.astype(np.float64))["q"]
+    assert np.max(np.abs(q - exact)) < 2e-2
+
+
+def test_gradients_match_oracle():
+    g, y = _data(4, 2)
+    params = surrogate.init_params(5)
+    # give the head and biases non-trivial values so every gradient is exercised
+    params[-33:] = np.random.default_rng(0).normal(0, 0.5, 33).astype(np.float32)
+    net = surrogate.CommittorCNN(L, 8, params)
+    loss, grad = net.gradients(g, y)
+    rloss, rgrad, _ = ocnn.loss_and_grads(params.astype(np.float64), g.astype(np.float64),
+                                          y.astype(np.float64), bf16=True)
+    assert abs(loss - rloss) < 1e-3 * max(1.0, abs(rloss))
+    o = 0
+    for name, shp in ocnn.SHAPES:
+        n = int(np.prod(shp))
+        a, b = grad[o:o + n].astype(np.float64), rgrad[o:o + n]
+        o += n
+        rel = np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-12)
+        assert rel < 2e-2, (name, rel)
+        if np.linalg.norm(b) > 0:
+            cos = a @ b / (np.linalg.norm(a) * np.linalg.norm(b))
+            assert cos > 0.999, (name, cos)
+
+
+def test_training_learns():
+    g, y = _data(512, 3)
+    gv, yv = _data(128, 4)
+    net = surrogate.CommittorCNN(L, 256, surrogate.init_params(7))
+    mae0 = float(np.mean(np.abs(net.predict(gv) - yv)))
+    hist = net.train(g, y, epochs=12, batch=64, lr=3e-3, val=(gv, yv), augment=False)
+    mae1 = hist[-1]["val_mae"]
+    assert hist[-1]["loss"] < hist[0]["loss"]
+    assert mae1 < 0.5 * mae0 and mae1 < 0.05, (mae0, hist)

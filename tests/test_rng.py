@@ -63,3 +63,11 @@ def test_stream_statistics_are_uniform():
         chi2 = float(((hist - exp) ** 2 / exp).sum())
         assert chi2 < 45.0  # 15 dof, p ~ 1e-4
         assert abs(u.mean() - 0.5) < 4 * np.sqrt(1 / 12 / u.size)
+
+
+def test_surrogate_parameter_layout_matches_oracle():
+    from oracle import cnn as ocnn
+    from gpu_2dising_b200 import surrogate
+    assert surrogate.NPARAM == ocnn.NPARAM == 28097
+    assert np.array_equal(surrogate.init_params(11), ocnn.init_params(11))
+    assert nat.lib().gasp_cnn_param_count() == 28097
