@@ -404,6 +404,25 @@ def run_committor(args):
     print(json.dumps(line), flush=True)
 
 
+def run_surrogate(args):
+    """The learned committor surrogate: snapshots from a swarm at beta=0.54,
+    h=0.07, shooting labels, GPU training, held-out MAE against 1024-shot
+    labels, and screening throughput vs shooting alone."""
+    from gpu_2dising_b200 import engine, surrogate
+    engine.init_device(0)
+    res = surrogate.run_experiment(n_train=args.surrogate_train, n_test=args.surrogate_test,
+                                   n_screen=args.surrogate_screen, epochs=args.surrogate_epochs)
+    hist = res.pop("history")
+    line = {"metric": "committor evaluations/s, surrogate-screened vs shooting alone",
+            "value": res["screen_grids_per_s"], "unit": "grids/s", "n_gpus": 1,
+            "speedup_vs_shooting": res["speedup"], **res,
+            "val_mae_by_epoch": [round(h["val_mae"], 4) for h in hist],
+            "config": {"workload": "L=64 snapshots (beta=0.54, h=0.07) labelled by "
+                                   "256-shot pB; CNN 4x conv3x3(32)+ReLU, avg-pool, "
+                                   "32->1 sigmoid; fallback |pred-0.5|<0.1"}}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     global SWEEPS_PER_STEP
     ap = argparse.ArgumentParser()
@@ -415,12 +434,17 @@ def main():
     ap.add_argument("--sweeps-per-step", type=int, default=SWEEPS_PER_STEP,
                     help="smaller values give a short launch for ncu captures")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", default="swarm", choices=["swarm", "batched", "committor"],
+    ap.add_argument("--workload", default="swarm",
+                    choices=["swarm", "batched", "committor", "surrogate"],
                     help="swarm: the headline single-group swarm; batched: uneven groups; "
                          "committor: seeded droplet shooting")
     ap.add_argument("--committor-inputs", type=int, default=64)
     ap.add_argument("--committor-shots", type=int, default=4096)
     ap.add_argument("--committor-check", type=int, default=10)
+    ap.add_argument("--surrogate-train", type=int, default=8192)
+    ap.add_argument("--surrogate-test", type=int, default=512)
+    ap.add_argument("--surrogate-screen", type=int, default=20000)
+    ap.add_argument("--surrogate-epochs", type=int, default=30)
     ap.add_argument("--batched-sweeps", type=int, default=1000)
     ap.add_argument("--rng", default="xorwow", choices=["xorwow", "mwc64x"],
                     help="xorwow: the reference stream (bit-exact); mwc64x: production stream")
@@ -441,6 +465,9 @@ def main():
     elif args.workload == "committor":
         if rank == 0:
             run_committor(args)
+    elif args.workload == "surrogate":
+        if rank == 0:
+            run_surrogate(args)
     else:
         run_ours(args, rank, world, local_rank)
 

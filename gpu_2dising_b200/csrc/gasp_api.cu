@@ -127,9 +127,9 @@ int validate_L(int L, int device) {
     set_error("L must be >= 2 (got %d)", L);
     return GASP_ERR_INVALID;
   }
-  const int maxL = max_shared_L(device);
-  if (L > maxL) {
-    set_error("L=%d exceeds the shared-memory sweep limit %d on device %d", L, maxL, device);
+  (void)device;
+  if (L > 8192) {  // the reference's MAXL (include/mc_gpu.h:59)
+    set_error("L=%d exceeds the maximum lattice side 8192", L);
     return GASP_ERR_UNSUPPORTED;
   }
   return GASP_OK;
@@ -271,6 +271,7 @@ int gasp_init_grid(int L, int ngrids, int threads_per_block, const int *host_gri
   g.ngrids = ngrids;
   g.ntiles = tiles_for(ngrids);
   g.frame_bytes = gasp_frame_bytes(L, ngrids);
+  g.global_lattice = L > max_shared_L(dev) ? 1 : 0;
   const size_t words = (size_t)g.ntiles * g.W * kTile;
   cudaError_t e = cudaMalloc(&g.d_lat, words * sizeof(uint32_t));
   if (e == cudaSuccess) e = cudaMalloc(&g.d_mag, (size_t)g.ntiles * kTile * sizeof(float));
@@ -490,6 +491,7 @@ SweepLaunch base_launch(gasp_grids_t *g) {
   p.pacc_cpu = x.d_tab->pacc_cpu;
   p.float_compare = x.float_cmp;
   p.variant = x.variant;
+  p.lattice_in_global = g->global_lattice;
   p.warps_per_cta = x.warps_per_cta;
   return p;
 }

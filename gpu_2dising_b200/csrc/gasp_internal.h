@@ -74,6 +74,7 @@ struct SweepLaunch {
   int variant;            // 0: fastest kernel for L; 1: generic; 2: row kernel, no pairing
   int rng_kind;           // RngKind of p.rng
   const int *n_active_dev;// optional device count overriding n_active (graph replays)
+  int lattice_in_global;  // L beyond shared memory: sweep the lattice in place in HBM
 };
 
 // Sweep parameters of a replica set + RNG whose tables are ready
@@ -109,6 +110,7 @@ struct gasp_grids {
   uint8_t *d_frame;      // frame payload buffer (lazily allocated)
   size_t frame_bytes;
   int *d_scratch32;      // int32 staging (lazily allocated), ngrids*N
+  int global_lattice;    // L exceeds the shared-memory sweep: use the HBM path
 };
 
 struct gasp_rng {

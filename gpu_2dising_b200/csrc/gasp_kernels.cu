@@ -203,6 +203,51 @@ __global__ void __launch_bounds__(256) k_sweep_exact(SweepLaunch p) {
 }
 
 // ---------------------------------------------------------------------------
+// The same sweep for lattices larger than shared memory holds (the role of
+// the reference's global-memory method 0): each lane works on its replica's
+// interleaved words in place in HBM (the L2 keeps the active lines).
+// ---------------------------------------------------------------------------
+template <bool kFloatCmp, int kRng>
+__global__ void __launch_bounds__(128) k_sweep_global(SweepLaunch p) {
+  const int L = p.L;
+  const int N = L * L;
+  const int W = (N + 31) >> 5;
+  __shared__ uint32_t thr_s[16];
+  __shared__ float pacc_s[20];
+  if (threadIdx.x < 10) thr_s[threadIdx.x] = p.thr[threadIdx.x];
+  if (threadIdx.x < 20) pacc_s[threadIdx.x] = p.pacc_f[threadIdx.x];
+  __syncthreads();
+  const int n_act = p.n_active_dev ? *p.n_active_dev : p.n_active;
+  const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+  if (slot >= n_act) return;
+  const int rep = p.active ? p.active[slot] : slot;
+  uint32_t *my = p.lat + (size_t)(rep >> 5) * W * kTile + (rep & 31);
+  RngPolicy<kRng> rg;
+  rg.load(p.rng, p.rng_stride, rep);
+  const float shrink = (1.0f - FLT_EPSILON) * (float)N;
+  for (int sw = 0; sw < p.nsweeps; ++sw) {
+    for (int a = 0; a < N; ++a) {
+      const int s = (int)rg.template site<0>(shrink, N);
+      const int row = s / L;
+      const int col = s - row * L;
+      const int su = row == 0 ? s + N - L : s - L;
+      const int sd = row == L - 1 ? s - N + L : s + L;
+      const int sl = col == 0 ? s + L - 1 : s - 1;
+      const int sr = col == L - 1 ? s - L + 1 : s + 1;
+      const uint32_t wc = my[(size_t)(s >> 5) * kTile];
+      const uint32_t bs = (wc >> (s & 31)) & 1u;
+      const uint32_t k = bit_at(my, su) + bit_at(my, sd) + bit_at(my, sl) + bit_at(my, sr);
+      const uint32_t cls = 5u * bs + k;
+      const uint32_t x2 = rg.next();
+      const bool acc = kFloatCmp ? (_curand_uniform(x2) < pacc_s[2 * cls]) : (x2 <= thr_s[cls]);
+      if (acc) my[(size_t)(s >> 5) * kTile] = wc ^ (1u << (s & 31));
+    }
+  }
+  rg.store(p.rng, p.rng_stride, rep);
+  epilogue_mag(my, p, N, W, true, rep);
+}
+
+// ---------------------------------------------------------------------------
 // Exact sweep specialised for L a power of two and a multiple of 32 (32, 64,
 // 128): a row is R = L/32 whole words, so
 //   * up/down neighbours are the words R rows-words away, at the same bit,
@@ -664,6 +709,12 @@ int launch_rows(Kern kern, const SweepLaunch &p, size_t dyn_smem, cudaStream_t s
 
 template <bool F, int K>
 int dispatch_kind(const SweepLaunch &p, cudaStream_t s) {
+  if (p.lattice_in_global) {
+    if (p.n_active == 0) return GASP_OK;
+    k_sweep_global<F, K><<<(p.n_active + 127) / 128, 128, 0, s>>>(p);
+    GASP_CUDA(cudaGetLastError());
+    return GASP_OK;
+  }
   if (p.variant == 1) {  // the generic kernel, kept selectable for comparisons
     return launch_tiles(p.L == 64 ? k_sweep_exact<64, F, K> : k_sweep_exact<0, F, K>, p, s);
   }

@@ -226,4 +226,55 @@ def screen(cnn, grids, beta, h, fallback_shots=128, band=0.1, **shoot_kw):
     return out, near, time.perf_counter() - t0
 
 
-__all__ = ["CommittorCNN", "init_params", "shoot", "harvest_snapshots", "screen", "nat"]
+def run_experiment(n_train=8192, train_shots=256, n_test=512, test_shots=1024, n_screen=20000,
+                   baseline_shots=64, epochs=30, batch=256, lr=2e-3, beta=0.54, h=0.07,
+                   seed=0, log=None):
+    """Train the surrogate on shooting labels and measure what it gains.
+
+    Returns a dict with the held-out MAE (surrogate alone and screened with
+    fallback) against `test_shots`-shot labels, the MAE of `baseline_shots`
+    shooting on the same grids, and the configurations/s of screening vs
+    shooting alone with `baseline_shots` (whose binomial MAE is about 0.05
+    at pB = 0.5)."""
+    t = {}
+    t0 = time.perf_counter()
+    snaps = harvest_snapshots(n_train + n_test + n_screen, beta=beta, h=h, seed=seed + 3)
+    t["harvest_s"] = time.perf_counter() - t0
+    rs = np.random.default_rng(seed)
+    snaps = snaps[rs.permutation(snaps.shape[0])]
+    tr, te, sc = (snaps[:n_train], snaps[n_train:n_train + n_test],
+                  snaps[n_train + n_test:])
+    y_tr, a_tr, s_tr = shoot(tr, train_shots, beta, h, seed=seed + 11)
+    y_te, a_te, s_te = shoot(te, test_shots, beta, h, seed=seed + 13)
+    t["label_train_s"], t["label_test_s"] = s_tr, s_te
+    net = CommittorCNN(64, batch, init_params(seed))
+    t0 = time.perf_counter()
+    hist = net.train(tr, y_tr, epochs=epochs, batch=batch, lr=lr, seed=seed,
+                     val=(te, y_te), log=log)
+    t["train_s"] = time.perf_counter() - t0
+    pred_te = net.predict(te).astype(np.float64)
+    mae_surrogate = float(np.mean(np.abs(pred_te - y_te)))
+    scr_te, near_te, _ = screen(net, te, beta, h, fallback_shots=baseline_shots, seed=seed + 17)
+    mae_screened = float(np.mean(np.abs(scr_te - y_te)))
+    base_te, _, _ = shoot(te, baseline_shots, beta, h, seed=seed + 19)
+    mae_baseline = float(np.mean(np.abs(base_te - y_te)))
+    # throughput on the screening pool
+    _, near_sc, t_screen = screen(net, sc, beta, h, fallback_shots=baseline_shots,
+                                  seed=seed + 23)
+    _, _, t_shoot = shoot(sc, baseline_shots, beta, h, seed=seed + 29)
+    res = {
+        "n_train": int(tr.shape[0]), "train_shots": train_shots, "n_test": int(te.shape[0]),
+        "test_shots": test_shots, "n_screen": int(sc.shape[0]), "baseline_shots": baseline_shots,
+        "mae_surrogate": mae_surrogate, "mae_screened": mae_screened,
+        "mae_shooting_baseline": mae_baseline, "fallback_fraction": float(near_sc.mean()),
+        "screen_grids_per_s": sc.shape[0] / t_screen, "shoot_grids_per_s": sc.shape[0] / t_shoot,
+        "speedup": t_shoot / t_screen, "final_train_loss": hist[-1]["loss"],
+        "label_mean_train": float(y_tr.mean()), "times_s": t,
+        "history": hist,
+    }
+    net.close()
+    return res
+
+
+__all__ = ["CommittorCNN", "init_params", "shoot", "harvest_snapshots", "screen",
+           "run_experiment", "nat"]

@@ -32,7 +32,7 @@ enum {
   GASP_ERR_IO = 5,          /* file open/read/write failed                    */
   GASP_ERR_FORMAT = 6,      /* file header does not match (src/io.c:25-28)    */
   GASP_ERR_CALLBACK = 7,    /* user output callback returned non-zero         */
-  GASP_ERR_UNSUPPORTED = 8, /* e.g. L beyond the shared-memory path            */
+  GASP_ERR_UNSUPPORTED = 8, /* e.g. L above 8192 or a CV other than magnetisation */
   GASP_ERR_TIMEOUT = 9      /* a bounded device-side wait expired             */
 };
 
@@ -60,7 +60,9 @@ int gasp_select_gpu_method(int L, int ngrids, int threads_per_block, int gpu_dev
  * host expf exactly as the reference does; index 5*(s+1)+nsum+4. */
 int gasp_acceptance_table(double beta, double h, float table_out[20]);
 
-/* Largest L the shared-memory sweep supports on this device. */
+/* Largest L swept in shared memory on this device; larger lattices (up to
+ * L = 8192, the reference's MAXL) are swept in place in HBM, the role of the
+ * reference's global-memory method 0. */
 int gasp_max_shared_L(int device, int *maxL_out);
 
 /* Makes subsequent device work of this thread's handles go to `stream`

@@ -204,10 +204,23 @@ def test_full_size_swarm_step_bit_exact(ref_gpu):
     assert np.array_equal(gour.reshape(-1), gref)
 
 
+def test_large_lattice_hbm_path_matches_reference_method0(ref_gpu):
+    """L beyond the shared-memory limit runs in place in HBM, bit-exact with
+    the reference's global-memory kernel."""
+    L = engine.max_shared_L(0) + 6
+    ng, seed, beta, h = 40, 77, 0.5, 0.1
+    g0 = _grids(L, ng, "random", seed)
+    gref = g0.reshape(-1).copy()
+    mref = np.zeros(2 * ng, np.float32)
+    assert ref_gpu.refgpu_run_kernels(L, ng, 32, 0, seed, beta, h, 1, 1, gref, mref) == 0
+    gour, mour = _ours_kernels(L, ng, 0, seed, beta, h, 1, 1, g0)
+    assert np.array_equal(gour.reshape(-1), gref)
+    assert np.array_equal(mour.reshape(-1), mref)
+
+
 def test_errors_are_raised_not_hidden():
-    maxL = engine.max_shared_L(0)
     with pytest.raises(GaspError):
-        engine.DeviceGrids(maxL + 1, 32)
+        engine.DeviceGrids(8193, 32)
     dg = engine.DeviceGrids(16, 64)
     r = engine.RngStates(32, 1)
     with pytest.raises(GaspError):
