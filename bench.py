@@ -379,10 +379,10 @@ def run_committor(args):
     engine.init_device(0)
     ngrid_in, shots = args.committor_inputs, args.committor_shots
     inputs, radii = committor_inputs(ngrid_in)
-    host = np.repeat(inputs, shots, axis=0)
-    n = host.shape[0]
+    n = ngrid_in * shots
     t0 = time.perf_counter()
-    dg = engine.DeviceGrids(L, n, host)
+    dg = engine.DeviceGrids(L, n)
+    dg.upload_inputs(inputs)
     rng = engine.RngStates(n, SEED, kind=args.rng)
     res, fates, drv_s, attempts = engine.run_driver(
         dg, rng, BETA, H, 20000, args.committor_check, 20000, itask=1, dn_thr=-0.93,

@@ -322,6 +322,23 @@ int gasp_grids_upload(gasp_grids_t *g, const int *host_grids) {
   return GASP_OK;
 }
 
+int gasp_grids_upload_inputs(gasp_grids_t *g, const int *inputs, int ninputs) {
+  if (!g || !inputs || ninputs <= 0 || g->ngrids % ninputs != 0) {
+    set_error("gasp_grids_upload_inputs: ngrids must be a multiple of ninputs");
+    return GASP_ERR_INVALID;
+  }
+  int rc = check_device_of(g->device);
+  if (rc) return rc;
+  if ((rc = ensure_scratch32(g))) return rc;
+  cudaStream_t s = current_stream();
+  GASP_CUDA(cudaMemcpyAsync(g->d_scratch32, inputs, (size_t)ninputs * g->N * sizeof(int),
+                            cudaMemcpyHostToDevice, s));
+  rc = launch_pack_grids(g->d_scratch32, g->d_lat, g->L, g->ngrids, s, g->ngrids / ninputs);
+  if (rc) return rc;
+  GASP_CUDA(cudaStreamSynchronize(s));
+  return GASP_OK;
+}
+
 int gasp_grids_download(gasp_grids_t *g, int *host_grids) {
   if (!g || !host_grids) return GASP_ERR_INVALID;
   int rc = check_device_of(g->device);

@@ -93,7 +93,8 @@ int launch_build_thresholds(const float *d_pacc20, uint32_t *d_thr10, int *d_fla
 int launch_sweep_exact(const SweepLaunch &p, cudaStream_t s);
 int launch_sweep_trace_cpu(const SweepLaunch &p, cudaStream_t s);
 int launch_measure(const uint32_t *lat, int L, int ngrids, float *mag, cudaStream_t s);
-int launch_pack_grids(const int *grids32, uint32_t *lat, int L, int ngrids, cudaStream_t s);
+int launch_pack_grids(const int *grids32, uint32_t *lat, int L, int ngrids, cudaStream_t s,
+                      int per_input = 0);
 int launch_unpack_grids(const uint32_t *lat, int *grids32, int L, int ngrids, cudaStream_t s);
 int launch_pack_frame(const uint32_t *lat, uint8_t *frame, int L, int ngrids, cudaStream_t s);
 int max_shared_L(int device);

@@ -620,7 +620,10 @@ __global__ void k_measure(const uint32_t *lat, int L, int ngrids, float *mag) {
 }
 
 // int32 grids [ngrids][N] -> lattice words; one thread per (tile, w, lane).
-__global__ void k_pack_grids(const int *g, uint32_t *lat, int L, int ngrids, long long total) {
+// per_input > 0: g holds ngrids/per_input input grids and replica r takes
+// input r / per_input (the layout of init_grids_from_array, src/grid.c:59-67).
+__global__ void k_pack_grids(const int *g, uint32_t *lat, int L, int ngrids, long long total,
+                             int per_input) {
   const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= total) return;
   const int N = L * L, W = (N + 31) >> 5;
@@ -631,7 +634,7 @@ __global__ void k_pack_grids(const int *g, uint32_t *lat, int L, int ngrids, lon
   const long long rep = tile * kTile + lane;
   uint32_t word = 0u;
   if (rep < ngrids) {
-    const int *src = g + rep * N;
+    const int *src = g + (per_input > 0 ? rep / per_input : rep) * N;
     const int s0 = w * 32;
     const int nb = min(32, N - s0);
     for (int b = 0; b < nb; ++b) word |= (src[s0 + b] == 1 ? 1u : 0u) << b;
@@ -800,10 +803,12 @@ int launch_measure(const uint32_t *lat, int L, int ngrids, float *mag, cudaStrea
   return GASP_OK;
 }
 
-int launch_pack_grids(const int *g, uint32_t *lat, int L, int ngrids, cudaStream_t s) {
+int launch_pack_grids(const int *g, uint32_t *lat, int L, int ngrids, cudaStream_t s,
+                      int per_input) {
   const long long total = (long long)tiles_for(ngrids) * words_per_replica(L) * kTile;
   if (total == 0) return GASP_OK;
-  k_pack_grids<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(g, lat, L, ngrids, total);
+  k_pack_grids<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(g, lat, L, ngrids, total,
+                                                               per_input);
   GASP_CUDA(cudaGetLastError());
   return GASP_OK;
 }

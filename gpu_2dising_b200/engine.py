@@ -100,6 +100,13 @@ class DeviceGrids:
             raise ValueError("grid array has the wrong size")
         check(lib().gasp_grids_upload(self._h, g), "gasp_grids_upload")
 
+    def upload_inputs(self, inputs):
+        """Replica r starts from inputs[r // (ngrids // len(inputs))]
+        (init_grids_from_array); only the distinct inputs are copied."""
+        x = np.ascontiguousarray(inputs, dtype=np.int32).reshape(-1, self.L * self.L)
+        check(lib().gasp_grids_upload_inputs(self._h, x.reshape(-1), x.shape[0]),
+              "gasp_grids_upload_inputs")
+
     def set_option(self, option, value):
         """Launch tuning (results never depend on it): see gasp_grids_set_option."""
         check(lib().gasp_grids_set_option(self._h, int(option), int(value)), "gasp_grids_set_option")

@@ -156,8 +156,8 @@ def shoot(grids, shots, beta, h, up=0.9, dn=-0.93, cap=20000, check_int=10, seed
     for i in range(0, n, per):
         block = g[i:i + per]
         k = block.shape[0]
-        host = np.repeat(block, shots, axis=0)
-        dg = engine.DeviceGrids(L, k * shots, host)
+        dg = engine.DeviceGrids(L, k * shots)
+        dg.upload_inputs(block)
         r = engine.RngStates(k * shots, seed + i, kind=rng)
         res, fates, _, att = engine.run_driver(dg, r, beta, h, cap, check_int, cap, itask=1,
                                                dn_thr=dn, up_thr=up, ninputs=k, compact=True)

@@ -86,6 +86,10 @@ int gasp_free_grid(gasp_grids_t *grids);
 /* Host <-> device copies of all replicas in the reference's int32 layout. */
 int gasp_grids_upload(gasp_grids_t *grids, const int *host_grids);
 int gasp_grids_download(gasp_grids_t *grids, int *host_grids);
+/* Device-side form of init_grids_from_array (src/grid.c:41-71) + upload:
+ * `inputs` holds ninputs LxL grids (int32); replica r starts from input
+ * r / (ngrids/ninputs).  Only the distinct inputs cross PCIe. */
+int gasp_grids_upload_inputs(gasp_grids_t *grids, const int *inputs, int ninputs);
 /* Replica count / side length of a set. */
 int gasp_grids_shape(const gasp_grids_t *grids, int *L_out, int *ngrids_out);
 

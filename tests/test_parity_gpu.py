@@ -204,6 +204,16 @@ def test_full_size_swarm_step_bit_exact(ref_gpu):
     assert np.array_equal(gour.reshape(-1), gref)
 
 
+@pytest.mark.parametrize("L,nin,per", [(64, 3, 5), (30, 4, 16), (7, 1, 9)])
+def test_upload_inputs_replicates_like_init_grids_from_array(L, nin, per):
+    inputs = _grids(L, nin, "random", L * nin)
+    dg = engine.DeviceGrids(L, nin * per)
+    dg.upload_inputs(inputs)
+    assert np.array_equal(dg.download(), np.repeat(inputs, per, axis=0))
+    with pytest.raises(GaspError):
+        engine.DeviceGrids(L, 10).upload_inputs(np.repeat(inputs[:1], 3, axis=0))
+
+
 def test_large_lattice_hbm_path_matches_reference_method0(ref_gpu):
     """L beyond the shared-memory limit runs in place in HBM, bit-exact with
     the reference's global-memory kernel."""
