@@ -42,7 +42,8 @@ EXPORTED = (
     "gasp_status_string", "gasp_last_error", "gasp_version", "gasp_init_device",
     "gasp_select_gpu_method", "gasp_acceptance_table", "gasp_max_shared_L",
     "gasp_set_stream", "gasp_init_grid", "gasp_free_grid", "gasp_grids_upload",
-    "gasp_grids_download", "gasp_grids_upload_inputs", "gasp_grids_shape", "gasp_grids_set_option", "gasp_init_rand",
+    "gasp_grids_download", "gasp_grids_upload_inputs",
+    "gasp_grids_upload_inputs_noalloc", "gasp_grids_shape", "gasp_grids_set_option", "gasp_init_rand",
     "gasp_init_rand_mode", "gasp_mwc64x_seed_states", "gasp_free_rand",
     "gasp_sweep", "gasp_sweep_trace_cpu", "gasp_magnetisation", "gasp_pack_frame",
     "gasp_frame_bytes", "gasp_mc_driver_gpu", "gasp_mc_driver_gpu_ex",
@@ -129,6 +130,7 @@ def _bind(lib):
         "gasp_grids_upload": (I, [P, _i32p]),
         "gasp_grids_download": (I, [P, _i32p]),
         "gasp_grids_upload_inputs": (I, [P, _i32p, I]),
+        "gasp_grids_upload_inputs_noalloc": (I, [P, _i32p, I]),
         "gasp_grids_shape": (I, [P, C.POINTER(I), C.POINTER(I)]),
         "gasp_grids_set_option": (I, [P, I, I]),
         "gasp_init_rand": (I, [I, I, C.c_ulonglong, C.POINTER(P)]),

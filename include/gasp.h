@@ -90,6 +90,23 @@ int gasp_grids_download(gasp_grids_t *grids, int *host_grids);
  * `inputs` holds ninputs LxL grids (int32); replica r starts from input
  * r / (ngrids/ninputs).  Only the distinct inputs cross PCIe. */
 int gasp_grids_upload_inputs(gasp_grids_t *grids, const int *inputs, int ninputs);
+/* Same result as gasp_grids_upload_inputs, allocating no memory: the inputs
+ * are staged in one fixed device array of GASP_NOALLOC_MAX_INPUT_INTS int32
+ * (1 MiB; 64 inputs at L=64) instead of a buffer sized for the whole set.
+ * For callers that cannot allocate: a set filling most of the device, or a
+ * shooting loop that must not let cudaMalloc/cudaFree synchronise the device
+ * under work on other streams.  No counterpart in the reference.
+ * - ninputs * L * L above GASP_NOALLOC_MAX_INPUT_INTS -> GASP_ERR_INVALID
+ *   with a message naming the limit; nothing is copied.
+ * - Nothing has to start at zero: each call overwrites the staged inputs.
+ * - The first call on each device looks up the array's device address; make
+ *   that first call before any stream capture.
+ * - There is one array per device: calls that overlap in time (two host
+ *   threads, or a call while another is still running) race on it.  Calls
+ *   that follow one another are safe, as each waits for its copy and pack
+ *   on the current stream before returning. */
+#define GASP_NOALLOC_MAX_INPUT_INTS (1 << 18)
+int gasp_grids_upload_inputs_noalloc(gasp_grids_t *grids, const int *inputs, int ninputs);
 /* Replica count / side length of a set. */
 int gasp_grids_shape(const gasp_grids_t *grids, int *L_out, int *ngrids_out);
 
