@@ -195,6 +195,7 @@ def run_e2e(args, rank, world, dist, torch, engine):
     _, _, drv_s, attempts = engine.run_driver(dg2, rng2, BETA, H, SWEEPS_PER_STEP * args.steps,
                                           MAG_INT, GRID_INT, itask=0, dn_thr=-0.9, up_thr=0.9,
                                           packed_out=packed)
+    t3 = time.perf_counter()
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
     if dist is not None:
@@ -208,6 +209,7 @@ def run_e2e(args, rank, world, dist, torch, engine):
     return {"value": attempts * world / e2e_s, "unit": UNIT,
             "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
             "wall_s": e2e_s, "upload_s": t1 - t0, "rng_init_s": t2 - t1, "driver_s": drv_s,
+            "driver_call_s": t3 - t2,
             "scope": "gasp_init_grid (int32 host grids) + gasp_init_rand + "
                      "gasp_mc_driver_gpu over all steps (per-check magnetisation D2H, "
                      "packed dumps every 1000 sweeps)"}
@@ -417,9 +419,12 @@ def run_surrogate(args):
             "value": res["screen_grids_per_s"], "unit": "grids/s", "n_gpus": 1,
             "speedup_vs_shooting": res["speedup"], **res,
             "val_mae_by_epoch": [round(h["val_mae"], 4) for h in hist],
-            "config": {"workload": "L=64 snapshots (beta=0.54, h=0.07) labelled by "
-                                   "256-shot pB; CNN 4x conv3x3(32)+ReLU, avg-pool, "
-                                   "32->1 sigmoid; fallback |pred-0.5|<0.1"}}
+            "config": {"workload": f"{res['n_train']} L=64 swarm snapshots (beta=0.54, h=0.07, "
+                                   "m in (-0.93,-0.65)) labelled by 256-shot pB, "
+                                   f"{res['n_test']} held out with 1024-shot pB, "
+                                   f"{res['n_screen']} screened; CNN 4x conv3x3(32)+ReLU, "
+                                   "avg-pool, 32->1 sigmoid, batch 1024; fallback "
+                                   "|pred-0.5|<0.1 shot with 64 trajectories"}}
     print(json.dumps(line), flush=True)
 
 
@@ -441,10 +446,10 @@ def main():
     ap.add_argument("--committor-inputs", type=int, default=64)
     ap.add_argument("--committor-shots", type=int, default=4096)
     ap.add_argument("--committor-check", type=int, default=10)
-    ap.add_argument("--surrogate-train", type=int, default=8192)
-    ap.add_argument("--surrogate-test", type=int, default=512)
-    ap.add_argument("--surrogate-screen", type=int, default=20000)
-    ap.add_argument("--surrogate-epochs", type=int, default=30)
+    ap.add_argument("--surrogate-train", type=int, default=20000)
+    ap.add_argument("--surrogate-test", type=int, default=2000)
+    ap.add_argument("--surrogate-screen", type=int, default=100000)
+    ap.add_argument("--surrogate-epochs", type=int, default=40)
     ap.add_argument("--batched-sweeps", type=int, default=1000)
     ap.add_argument("--rng", default="xorwow", choices=["xorwow", "mwc64x"],
                     help="xorwow: the reference stream (bit-exact); mwc64x: production stream")

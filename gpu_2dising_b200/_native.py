@@ -45,11 +45,13 @@ EXPORTED = (
     "gasp_grids_download", "gasp_grids_upload_inputs",
     "gasp_grids_upload_inputs_noalloc", "gasp_grids_shape", "gasp_grids_set_option", "gasp_init_rand",
     "gasp_init_rand_mode", "gasp_mwc64x_seed_states", "gasp_free_rand",
-    "gasp_sweep", "gasp_sweep_trace_cpu", "gasp_magnetisation", "gasp_pack_frame",
+    "gasp_sweep", "gasp_sweep_trace_cpu", "gasp_magnetisation", "gasp_largest_cluster", "gasp_pack_frame",
     "gasp_frame_bytes", "gasp_mc_driver_gpu", "gasp_mc_driver_gpu_ex",
     "gasp_init_grids_uniform", "gasp_init_grids_from_file", "gasp_init_grids_from_array",
     "gasp_init_fates", "gasp_read_input_grid", "gasp_write_ising_grids",
     "gasp_write_packed_frame", "gasp_bootstrap_errbar", "gasp_committor_from_fates",
+    "gasp_read_frame", "gasp_write_input_grid", "gasp_checkpoint_save", "gasp_checkpoint_info",
+    "gasp_checkpoint_load",
     "gasp_batch_create", "gasp_batch_free", "gasp_batch_swarm", "gasp_batch_autotune",
     "gasp_cnn_param_count", "gasp_cnn_create", "gasp_cnn_free", "gasp_cnn_set_params",
     "gasp_cnn_get_params", "gasp_cnn_predict", "gasp_cnn_gradients", "gasp_cnn_train_step",
@@ -141,6 +143,7 @@ def _bind(lib):
         "gasp_sweep": (I, [P, P, C.c_double, C.c_double, I, I]),
         "gasp_sweep_trace_cpu": (I, [P, _f64p, C.c_double, C.c_double, I]),
         "gasp_magnetisation": (I, [P, _f32p]),
+        "gasp_largest_cluster": (I, [P, I, _f32p]),
         "gasp_pack_frame": (I, [P, _u8p]),
         "gasp_frame_bytes": (C.c_size_t, [I, I]),
         "gasp_mc_driver_gpu": (I, [GpuGridsT, C.c_double, C.c_double, P, SamplerT, FunctionT,
@@ -156,6 +159,12 @@ def _bind(lib):
         "gasp_write_ising_grids": (I, [I, I, _i32p, I, P, P, C.c_char_p, C.c_double,
                                        C.c_double, C.c_char_p]),
         "gasp_write_packed_frame": (I, [C.c_char_p, I, I, I, _u8p, C.c_size_t]),
+        "gasp_read_frame": (I, [C.c_char_p, I, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                C.POINTER(C.c_int), C.c_void_p, C.c_longlong]),
+        "gasp_write_input_grid": (I, [C.c_char_p, I, _i32p]),
+        "gasp_checkpoint_save": (I, [C.c_char_p, P, P, C.c_void_p, I]),
+        "gasp_checkpoint_info": (I, [C.c_char_p] + [C.POINTER(C.c_int)] * 5),
+        "gasp_checkpoint_load": (I, [C.c_char_p, P, P, C.c_void_p, C.POINTER(C.c_int)]),
         "gasp_bootstrap_errbar": (C.c_double, [I, I, _i32p]),
         "gasp_committor_from_fates": (I, [I, I, _i32p, _f32p]),
         "gasp_batch_create": (I, [C.POINTER(GroupT), I, C.c_ulonglong, I, C.POINTER(P)]),

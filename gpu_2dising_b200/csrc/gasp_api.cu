@@ -60,6 +60,10 @@ struct GridsExtra {
   size_t stream_cap = 0;
   float *d_mag2 = nullptr;  // second magnetisation buffer for the driver
   int *d_active = nullptr;
+  float *d_lclus = nullptr; // largest-cluster sizes [ngrids]
+  int *d_cwork = nullptr;   // largest-cluster global work area (large L only)
+  size_t cwork_bytes = 0;
+  int mask_ok = 0;          // <= 6 classes with P <= 1 (see k_sweep_rows<kMask>)
   int variant = 0;          // GASP_OPT_SWEEP_VARIANT
   int warps_per_cta = 1;    // GASP_OPT_WARPS_PER_CTA
 };
@@ -110,6 +114,11 @@ int ensure_tables(gasp_grids_t *g, double beta, double h) {
   GASP_CUDA(cudaMemcpyAsync(flags, x.d_tab->flags, sizeof flags, cudaMemcpyDeviceToHost, s));
   GASP_CUDA(cudaStreamSynchronize(s));
   x.float_cmp = flags[0] != 0;
+  // A class with P > 1 accepts every draw (u <= 1 < P); the others need a
+  // comparison.  The acceptance-mask row kernel has room for six of those.
+  int cmp_classes = 0;
+  for (int c = 0; c < 10; ++c) cmp_classes += !(hb.pacc[2 * c] > 1.0f);
+  x.mask_ok = cmp_classes <= 6;
   x.beta = beta;
   x.h = h;
   return GASP_OK;
@@ -298,6 +307,8 @@ int gasp_free_grid(gasp_grids_t *g) {
   cudaFree(im->x.d_stream);
   cudaFree(im->x.d_mag2);
   cudaFree(im->x.d_active);
+  cudaFree(im->x.d_lclus);
+  cudaFree(im->x.d_cwork);
   delete im;
   return GASP_OK;
 }
@@ -329,13 +340,23 @@ int gasp_grids_upload_inputs(gasp_grids_t *g, const int *inputs, int ninputs) {
   }
   int rc = check_device_of(g->device);
   if (rc) return rc;
-  if ((rc = ensure_scratch32(g))) return rc;
+  // Stage in the set's int32 buffer if it has one, else in a buffer sized
+  // for the inputs only (the set-sized buffer is 32x the lattice).
+  const size_t bytes = (size_t)ninputs * g->N * sizeof(int);
+  int *stage = g->d_scratch32, *owned = nullptr;
+  if (!stage) {
+    GASP_CUDA(cudaMalloc(&owned, bytes));
+    stage = owned;
+  }
   cudaStream_t s = current_stream();
-  GASP_CUDA(cudaMemcpyAsync(g->d_scratch32, inputs, (size_t)ninputs * g->N * sizeof(int),
-                            cudaMemcpyHostToDevice, s));
-  rc = launch_pack_grids(g->d_scratch32, g->d_lat, g->L, g->ngrids, s, g->ngrids / ninputs);
+  cudaError_t e = cudaMemcpyAsync(stage, inputs, bytes, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) {
+    rc = launch_pack_grids(stage, g->d_lat, g->L, g->ngrids, s, g->ngrids / ninputs);
+    e = cudaStreamSynchronize(s);
+  }
+  if (owned) cudaFree(owned);
   if (rc) return rc;
-  GASP_CUDA(cudaStreamSynchronize(s));
+  GASP_CUDA(e);
   return GASP_OK;
 }
 
@@ -356,7 +377,7 @@ int gasp_grids_download(gasp_grids_t *g, int *host_grids) {
 int gasp_grids_set_option(gasp_grids_t *g, int option, int value) {
   if (!g) return GASP_ERR_INVALID;
   GridsExtra &x = impl(g)->x;
-  if (option == GASP_OPT_SWEEP_VARIANT && value >= 0 && value <= 3) {
+  if (option == GASP_OPT_SWEEP_VARIANT && value >= 0 && value <= 4) {
     x.variant = value;
     return GASP_OK;
   }
@@ -508,6 +529,7 @@ SweepLaunch base_launch(gasp_grids_t *g) {
   p.pacc_cpu = x.d_tab->pacc_cpu;
   p.float_compare = x.float_cmp;
   p.variant = x.variant;
+  p.mask_ok = x.mask_ok;
   p.lattice_in_global = g->global_lattice;
   p.warps_per_cta = x.warps_per_cta;
   return p;
@@ -632,6 +654,180 @@ int gasp_pack_frame(gasp_grids_t *g, uint8_t *host_out) {
 
 }  // extern "C"
 
+// Largest cluster of `spin` sites of every replica into x.d_lclus (on s).
+static int measure_largest_cluster(gasp_grids_t *g, int spin, cudaStream_t s) {
+  GridsExtra &x = impl(g)->x;
+  if (!x.d_lclus) GASP_CUDA(cudaMalloc(&x.d_lclus, (size_t)g->ngrids * sizeof(float)));
+  if (spin != 1 && spin != -1) {  // no site holds such a spin
+    GASP_CUDA(cudaMemsetAsync(x.d_lclus, 0, (size_t)g->ngrids * sizeof(float), s));
+    return GASP_OK;
+  }
+  const size_t need = largest_cluster_work_bytes(g->L, g->ngrids, g->device);
+  if (need > x.cwork_bytes) {
+    cudaFree(x.d_cwork);
+    x.d_cwork = nullptr;
+    x.cwork_bytes = 0;
+    GASP_CUDA(cudaMalloc(&x.d_cwork, need));
+    x.cwork_bytes = need;
+  }
+  return launch_largest_cluster(g->d_lat, g->L, g->ngrids, spin, x.d_cwork, need, x.d_lclus, s);
+}
+
+extern "C" int gasp_largest_cluster(gasp_grids_t *g, int spin, float *host_out) {
+  if (!g || !host_out) return GASP_ERR_INVALID;
+  int rc = check_device_of(g->device);
+  if (rc) return rc;
+  cudaStream_t s = current_stream();
+  if ((rc = measure_largest_cluster(g, spin, s))) return rc;
+  GASP_CUDA(cudaMemcpyAsync(host_out, impl(g)->x.d_lclus, (size_t)g->ngrids * sizeof(float),
+                            cudaMemcpyDeviceToHost, s));
+  GASP_CUDA(cudaStreamSynchronize(s));
+  return GASP_OK;
+}
+
+// ===========================================================================
+// Checkpoint files (no reference counterpart): "GASPCKP1", int32 L, ngrids,
+// rng kind, RNG words per replica, isweep, has_fates; the grids as one
+// gridstates.bin payload (ceil(L*L*ngrids/8) bytes); the RNG words
+// component-major (uint32 [words][ngrids]); int32 fates[ngrids] if present.
+// ===========================================================================
+namespace {
+
+const char kCkptMagic[8] = {'G', 'A', 'S', 'P', 'C', 'K', 'P', '1'};
+
+// gridstates.bin payload bits -> int32 spins (bit 1 -> +1).
+void expand_frame(const uint8_t *payload, int *grids, long long nbits) {
+  for (long long i = 0; i < nbits; ++i) grids[i] = ((payload[i >> 3] >> (i & 7)) & 1) ? 1 : -1;
+}
+
+int rng_words(const gasp_rng_t *r) { return r->kind == kRngMwc ? kMwcWords : kRngWords; }
+
+struct FileCloser {
+  FILE *f;
+  ~FileCloser() {
+    if (f) fclose(f);
+  }
+};
+
+int read_ckpt_header(FILE *f, int hdr[6]) {
+  char magic[8];
+  if (fread(magic, 1, 8, f) != 8 || fread(hdr, sizeof(int), 6, f) != 6) {
+    set_error("checkpoint: truncated header");
+    return GASP_ERR_IO;
+  }
+  if (memcmp(magic, kCkptMagic, 8) != 0 || hdr[0] < 2 || hdr[1] <= 0 ||
+      (hdr[2] != kRngXorwow && hdr[2] != kRngMwc) ||
+      hdr[3] != (hdr[2] == kRngMwc ? kMwcWords : kRngWords)) {
+    set_error("checkpoint: not a gasp checkpoint or unknown version");
+    return GASP_ERR_FORMAT;
+  }
+  return GASP_OK;
+}
+
+}  // namespace
+
+extern "C" int gasp_checkpoint_save(const char *path, gasp_grids_t *g, gasp_rng_t *r,
+                                    const int *fates, int isweep) {
+  if (!path || !g || !r) return GASP_ERR_INVALID;
+  if (r->ngrids < g->ngrids) {
+    set_error("checkpoint: %d RNG states for %d replicas", r->ngrids, g->ngrids);
+    return GASP_ERR_INVALID;
+  }
+  int rc = check_device_of(g->device);
+  if (rc) return rc;
+  if ((rc = ensure_frame(g))) return rc;
+  const int ng = g->ngrids, words = rng_words(r);
+  std::vector<uint8_t> payload(g->frame_bytes);
+  std::vector<uint32_t> rs((size_t)words * ng);
+  cudaStream_t s = current_stream();
+  if ((rc = launch_pack_frame(g->d_lat, g->d_frame, g->L, ng, s))) return rc;
+  GASP_CUDA(cudaMemcpyAsync(payload.data(), g->d_frame, g->frame_bytes, cudaMemcpyDeviceToHost, s));
+  for (int k = 0; k < words; ++k)
+    GASP_CUDA(cudaMemcpyAsync(rs.data() + (size_t)k * ng, r->d_state + (size_t)k * r->stride,
+                              (size_t)ng * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  GASP_CUDA(cudaStreamSynchronize(s));
+  FileCloser fc{fopen(path, "wb")};
+  if (!fc.f) {
+    set_error("checkpoint: cannot open %s for writing", path);
+    return GASP_ERR_IO;
+  }
+  const int hdr[6] = {g->L, ng, r->kind, words, isweep, fates ? 1 : 0};
+  bool ok = fwrite(kCkptMagic, 1, 8, fc.f) == 8 && fwrite(hdr, sizeof(int), 6, fc.f) == 6 &&
+            fwrite(payload.data(), 1, payload.size(), fc.f) == payload.size() &&
+            fwrite(rs.data(), sizeof(uint32_t), rs.size(), fc.f) == rs.size();
+  if (ok && fates) ok = fwrite(fates, sizeof(int), (size_t)ng, fc.f) == (size_t)ng;
+  ok = (fclose(fc.f) == 0) && ok;
+  fc.f = nullptr;
+  if (!ok) {
+    set_error("checkpoint: write to %s failed", path);
+    return GASP_ERR_IO;
+  }
+  return GASP_OK;
+}
+
+extern "C" int gasp_checkpoint_info(const char *path, int *L_out, int *ngrids_out,
+                                    int *rng_kind_out, int *isweep_out, int *has_fates_out) {
+  if (!path) return GASP_ERR_INVALID;
+  FileCloser fc{fopen(path, "rb")};
+  if (!fc.f) {
+    set_error("checkpoint: cannot open %s", path);
+    return GASP_ERR_IO;
+  }
+  int hdr[6];
+  int rc = read_ckpt_header(fc.f, hdr);
+  if (rc) return rc;
+  if (L_out) *L_out = hdr[0];
+  if (ngrids_out) *ngrids_out = hdr[1];
+  if (rng_kind_out) *rng_kind_out = hdr[2];
+  if (isweep_out) *isweep_out = hdr[4];
+  if (has_fates_out) *has_fates_out = hdr[5];
+  return GASP_OK;
+}
+
+extern "C" int gasp_checkpoint_load(const char *path, gasp_grids_t *g, gasp_rng_t *r,
+                                    int *fates_out, int *isweep_out) {
+  if (!path || !g || !r) return GASP_ERR_INVALID;
+  FileCloser fc{fopen(path, "rb")};
+  if (!fc.f) {
+    set_error("checkpoint: cannot open %s", path);
+    return GASP_ERR_IO;
+  }
+  int hdr[6];
+  int rc = read_ckpt_header(fc.f, hdr);
+  if (rc) return rc;
+  if (hdr[0] != g->L || hdr[1] != g->ngrids || hdr[2] != r->kind || r->ngrids < hdr[1]) {
+    set_error("checkpoint: file holds L=%d ngrids=%d rng kind %d; the handles differ", hdr[0],
+              hdr[1], hdr[2]);
+    return GASP_ERR_FORMAT;
+  }
+  if ((rc = check_device_of(g->device))) return rc;
+  const int ng = hdr[1], words = hdr[3];
+  std::vector<uint8_t> payload(g->frame_bytes);
+  std::vector<uint32_t> rs((size_t)words * ng);
+  std::vector<int> fates(hdr[5] ? (size_t)ng : 0);
+  bool ok = fread(payload.data(), 1, payload.size(), fc.f) == payload.size() &&
+            fread(rs.data(), sizeof(uint32_t), rs.size(), fc.f) == rs.size();
+  if (ok && hdr[5]) ok = fread(fates.data(), sizeof(int), (size_t)ng, fc.f) == (size_t)ng;
+  if (!ok) {
+    set_error("checkpoint: %s is truncated", path);
+    return GASP_ERR_IO;
+  }
+  std::vector<int> grids((size_t)g->N * ng);
+  expand_frame(payload.data(), grids.data(), (long long)g->N * ng);
+  if ((rc = gasp_grids_upload(g, grids.data()))) return rc;
+  cudaStream_t s = current_stream();
+  for (int k = 0; k < words; ++k)
+    GASP_CUDA(cudaMemcpyAsync(r->d_state + (size_t)k * r->stride, rs.data() + (size_t)k * ng,
+                              (size_t)ng * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+  GASP_CUDA(cudaStreamSynchronize(s));
+  if (fates_out) {
+    if (hdr[5]) memcpy(fates_out, fates.data(), (size_t)ng * sizeof(int));
+    else for (int i = 0; i < ng; ++i) fates_out[i] = -1;
+  }
+  if (isweep_out) *isweep_out = hdr[4];
+  return GASP_OK;
+}
+
 // ===========================================================================
 // Driver
 // ===========================================================================
@@ -644,8 +840,120 @@ struct PinnedBuf {
   }
 };
 
-void expand_frame(const uint8_t *payload, int *grids, long long nbits) {
-  for (long long i = 0; i < nbits; ++i) grids[i] = ((payload[i >> 3] >> (i & 7)) & 1) ? 1 : -1;
+
+}  // namespace
+
+namespace {
+
+// Committor shooting with the checks on the device: the itask-1 loop of the
+// driver (check at every isweep % mag_int == 0, then spc sweeps of the
+// replicas still undecided) with fates, compaction and attempt counts kept
+// in device memory, so intervals are enqueued back to back and the host only
+// polls the number of undecided replicas now and then.  Same fates as the
+// host loop: the same thresholds are applied to the same states.
+int committor_on_device(gasp_grids_t *g, gasp_rng_t *r, int tot, int mag_int, int spc,
+                        double up, double dn, int *grid_fate, long long *attempts_out) {
+  GridsExtra &x = impl(g)->x;
+  const int ngrids = g->ngrids, N = g->N;
+  cudaStream_t s = current_stream();
+  if (!x.d_active) GASP_CUDA(cudaMalloc(&x.d_active, (size_t)ngrids * sizeof(int)));
+  struct DevBuf {
+    void *p = nullptr;
+    ~DevBuf() {
+      if (p) cudaFree(p);
+    }
+  } fates_b, small_b;
+  GASP_CUDA(cudaMalloc(&fates_b.p, (size_t)ngrids * sizeof(int)));
+  GASP_CUDA(cudaMalloc(&small_b.p, 64));
+  int *d_fates = static_cast<int *>(fates_b.p);
+  int *d_n = static_cast<int *>(small_b.p);
+  long long *d_att = reinterpret_cast<long long *>(static_cast<char *>(small_b.p) + 8);
+  PinnedBuf hact_b, hpoll_b;
+  GASP_CUDA(cudaMallocHost(&hact_b.p, (size_t)ngrids * sizeof(int)));
+  GASP_CUDA(cudaMallocHost(&hpoll_b.p, 64 * sizeof(int)));
+  int *hact = static_cast<int *>(hact_b.p);
+  volatile int *hpoll = static_cast<volatile int *>(hpoll_b.p);
+  int n0 = 0;
+  for (int i = 0; i < ngrids; ++i)
+    if (grid_fate[i] == -1) hact[n0++] = i;
+  const long long zero = 0;
+  GASP_CUDA(cudaMemcpyAsync(d_fates, grid_fate, (size_t)ngrids * sizeof(int),
+                            cudaMemcpyHostToDevice, s));
+  if (n0 > 0)
+    GASP_CUDA(cudaMemcpyAsync(x.d_active, hact, (size_t)n0 * sizeof(int), cudaMemcpyHostToDevice,
+                              s));
+  GASP_CUDA(cudaMemcpyAsync(d_n, &n0, sizeof(int), cudaMemcpyHostToDevice, s));
+  GASP_CUDA(cudaMemcpyAsync(d_att, &zero, sizeof(long long), cudaMemcpyHostToDevice, s));
+  int rc = launch_measure(g->d_lat, g->L, ngrids, g->d_mag, s);
+  if (rc) return rc;
+
+  SweepLaunch p = base_launch(g);
+  p.rng = r->d_state;
+  p.rng_stride = r->stride;
+  p.rng_kind = r->kind;
+  p.nsweeps = spc;
+  p.active = x.d_active;
+  p.n_active = ngrids;  // launch shape; the kernels read the live count from d_n
+  p.n_active_dev = d_n;
+  p.mag_out = g->d_mag;
+
+  // Poll ring: every kPollEvery checks the live count is copied to pinned
+  // memory behind an event; the host looks at completed polls without
+  // waiting and stays at most kAhead polls ahead of the device.
+  constexpr int kPollEvery = 8, kRing = 16, kAhead = 4;
+  cudaEvent_t ev[kRing];
+  int nev = 0;
+  for (; nev < kRing; ++nev)
+    if (cudaEventCreateWithFlags(&ev[nev], cudaEventDisableTiming) != cudaSuccess) break;
+  struct EvGuard {
+    cudaEvent_t *e;
+    int n;
+    ~EvGuard() {
+      for (int i = 0; i < n; ++i) cudaEventDestroy(e[i]);
+    }
+  } evg{ev, nev};
+  if (nev < kRing) GASP_CUDA(cudaGetLastError());
+  long long polls_issued = 0, polls_seen = 0;
+  bool done = n0 == 0;
+  int checks = 0;
+  for (int isweep = 0; isweep < tot && !done; isweep += spc) {
+    if (isweep % mag_int == 0) {
+      // sweeps from this check to the next one (or to the end of the run)
+      long long span = 0;
+      for (int j = isweep; j < tot && (j == isweep || j % mag_int != 0); j += spc) span += spc;
+      if ((rc = launch_fate_compact(g->d_mag, d_fates, x.d_active, d_n, up, dn, d_att,
+                                    (long long)N * span, s)))
+        return rc;
+      if (++checks % kPollEvery == 0) {
+        const int slot = (int)(polls_issued % kRing);
+        GASP_CUDA(cudaMemcpyAsync(const_cast<int *>(hpoll) + slot, d_n, sizeof(int),
+                                  cudaMemcpyDeviceToHost, s));
+        GASP_CUDA(cudaEventRecord(ev[slot], s));
+        ++polls_issued;
+      }
+    }
+    if ((rc = launch_sweep_exact(p, s))) return rc;
+    // look at finished polls; wait only when too far ahead
+    while (polls_seen < polls_issued) {
+      const int slot = (int)(polls_seen % kRing);
+      cudaError_t q = polls_issued - polls_seen > kAhead ? cudaEventSynchronize(ev[slot])
+                                                          : cudaEventQuery(ev[slot]);
+      if (q == cudaErrorNotReady) break;
+      GASP_CUDA(q);
+      ++polls_seen;
+      if (hpoll[slot] == 0) {
+        done = true;
+        break;
+      }
+    }
+  }
+  long long att = 0;
+  GASP_CUDA(cudaMemcpyAsync(grid_fate, d_fates, (size_t)ngrids * sizeof(int),
+                            cudaMemcpyDeviceToHost, s));
+  GASP_CUDA(cudaMemcpyAsync(&att, d_att, sizeof(long long), cudaMemcpyDeviceToHost, s));
+  GASP_CUDA(cudaStreamSynchronize(s));
+  if (attempts_out) *attempts_out = att;
+  return GASP_OK;
 }
 
 }  // namespace
@@ -683,8 +991,9 @@ extern "C" int gasp_mc_driver_gpu_ex(gasp_gpu_grids_t grids, double beta, double
     set_error("Error: ngrids must be divisible by ninputs!");
     return GASP_ERR_INVALID;
   }
-  if (calc.cv && strcmp(calc.cv, "magnetisation") != 0) {
-    set_error("driver: only cv='magnetisation' is provided (got '%s')", calc.cv);
+  const bool use_lclus = calc.cv && strcmp(calc.cv, "largest_cluster") == 0;
+  if (calc.cv && !use_lclus && strcmp(calc.cv, "magnetisation") != 0) {
+    set_error("driver: cv must be 'magnetisation' or 'largest_cluster' (got '%s')", calc.cv);
     return GASP_ERR_UNSUPPORTED;
   }
   if (calc.itask == 1 && !grid_fate) {
@@ -711,14 +1020,52 @@ extern "C" int gasp_mc_driver_gpu_ex(gasp_gpu_grids_t grids, double beta, double
   char *cv = const_cast<char *>(calc.cv ? calc.cv : "magnetisation");
   char *fname = const_cast<char *>(calc.filename ? calc.filename : "gridstates.bin");
 
+  if (compact && !dumps && o.verbosity == 0 && !use_lclus) {
+    // Nothing to report per check: run the shooting loop on the device.
+    long long attempts = 0;
+    const auto t0 = std::chrono::steady_clock::now();
+    int rc2 = committor_on_device(g, r, tot, mag_int, spc, up, dn, grid_fate, &attempts);
+    if (rc2) return rc2;
+    const double elapsed =
+        std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    const int sub = ngrids / ninputs;
+    for (int i = 0; i < ninputs; ++i) {  // src/mc_gpu.cu:812-826
+      int nBb = 0, nF = 0;
+      for (int j = 0; j < sub; ++j) {
+        const int f = grid_fate[i * sub + j];
+        if (f > -1) nBb += f;
+        else nF += 1;
+      }
+      result[i] = (float)nBb / (float)(sub - nF);
+    }
+    if (calc.result)
+      for (int i = 0; i < nres; ++i) calc.result[i] = result[i];
+    if (o.elapsed_s) *o.elapsed_s = elapsed;
+    if (o.attempts) *o.attempts = attempts;
+    return GASP_OK;
+  }
+
   cudaStream_t s = current_stream();
   if (!x.d_mag2) GASP_CUDA(cudaMalloc(&x.d_mag2, (size_t)g->ntiles * kTile * sizeof(float)));
   if (compact && !x.d_active) GASP_CUDA(cudaMalloc(&x.d_active, (size_t)ngrids * sizeof(int)));
   if (dumps && (rc = ensure_frame(g))) return rc;
-  PinnedBuf hmag_b, hframe_b, hact_b;
+  PinnedBuf hmag_b, hframe_b, hact_b, hlclus_b;
   GASP_CUDA(cudaMallocHost(&hmag_b.p, (size_t)ngrids * sizeof(float)));
   float *hmag = static_cast<float *>(hmag_b.p);
   std::vector<float> mag_last((size_t)ngrids, 0.0f);
+  // Collective variable compared with the thresholds: the magnetisation or
+  // the largest cluster of spins opposite to initial_spin (src/mc_gpu.cu:586-605).
+  std::vector<float> lclus_last(use_lclus ? (size_t)ngrids : 0, 0.0f);
+  float *hlclus = nullptr;
+  if (use_lclus) {
+    GASP_CUDA(cudaMallocHost(&hlclus_b.p, (size_t)ngrids * sizeof(float)));
+    hlclus = static_cast<float *>(hlclus_b.p);
+  }
+  const float *colvar = use_lclus ? lclus_last.data() : mag_last.data();
+  auto take_check = [&]() {
+    memcpy(mag_last.data(), hmag, (size_t)ngrids * sizeof(float));
+    if (use_lclus) memcpy(lclus_last.data(), hlclus, (size_t)ngrids * sizeof(float));
+  };
   if (dumps) GASP_CUDA(cudaMallocHost(&hframe_b.p, g->frame_bytes));
   if (compact) GASP_CUDA(cudaMallocHost(&hact_b.p, (size_t)ngrids * sizeof(int)));
   uint8_t *hframe = static_cast<uint8_t *>(hframe_b.p);
@@ -750,16 +1097,21 @@ extern "C" int gasp_mc_driver_gpu_ex(gasp_gpu_grids_t grids, double beta, double
     if (mag_now)
       GASP_CUDA(cudaMemcpyAsync(hmag, d_mag_cur, (size_t)ngrids * sizeof(float),
                                 cudaMemcpyDeviceToHost, s));
+    if (mag_now && use_lclus) {  // on the lattice before this interval's sweeps
+      if ((rc = measure_largest_cluster(g, -calc.initial_spin, s))) return rc;
+      GASP_CUDA(cudaMemcpyAsync(hlclus, x.d_lclus, (size_t)ngrids * sizeof(float),
+                                cudaMemcpyDeviceToHost, s));
+    }
     bool fates_done = false;
     int nA = 0, nB = 0;
     if (compact && mag_now) {
       // Fates at this check decide which replicas the next batch simulates.
       GASP_CUDA(cudaStreamSynchronize(s));
-      memcpy(mag_last.data(), hmag, (size_t)ngrids * sizeof(float));
+      take_check();
       n_active = 0;
       for (int i = 0; i < ngrids; ++i) {
         if (grid_fate[i] == -1) {
-          const double m = (double)mag_last[i];
+          const double m = (double)colvar[i];
           if (m > up) grid_fate[i] = 1;
           else if (m < dn) grid_fate[i] = 0;
         }
@@ -794,10 +1146,10 @@ extern "C" int gasp_mc_driver_gpu_ex(gasp_gpu_grids_t grids, double beta, double
         have_frame = true;
         if (outfunc) expand_frame(hframe, grids.ising_grids, (long long)N * ngrids);
       }
-      if (mag_now && !fates_done) memcpy(mag_last.data(), hmag, (size_t)ngrids * sizeof(float));
+      if (mag_now && !fates_done) take_check();
       if (have_frame) {
-        if (outfunc && outfunc(L, ngrids, grids.ising_grids, isweep, mag_last.data(), nullptr, cv,
-                               dn, up, fname) != 0) {
+        if (outfunc && outfunc(L, ngrids, grids.ising_grids, isweep, mag_last.data(),
+                               use_lclus ? lclus_last.data() : nullptr, cv, dn, up, fname) != 0) {
           cudaStreamSynchronize(s);
           set_error("output callback returned non-zero at isweep %d", isweep);
           return GASP_ERR_CALLBACK;
@@ -814,14 +1166,14 @@ extern "C" int gasp_mc_driver_gpu_ex(gasp_gpu_grids_t grids, double beta, double
     if (mag_now || isweep == tot - 1) {
       if (mag_now && !fates_done) {
         GASP_CUDA(cudaStreamSynchronize(s));
-        memcpy(mag_last.data(), hmag, (size_t)ngrids * sizeof(float));
+        take_check();
       }
       if (itask == 0) {
         int nnuc = 0;
-        for (int i = 0; i < ngrids; ++i) nnuc += ((double)mag_last[i] > up) ? 1 : 0;
+        for (int i = 0; i < ngrids; ++i) nnuc += ((double)colvar[i] > up) ? 1 : 0;
         if (o.first_up)
           for (int i = 0; i < ngrids; ++i)
-            if (o.first_up[i] < 0 && (double)mag_last[i] > up) o.first_up[i] = isweep;
+            if (o.first_up[i] < 0 && (double)colvar[i] > up) o.first_up[i] = isweep;
         const int idx = isweep / mag_int;
         if (idx < nres) result[idx] = (float)((double)nnuc / (double)ngrids);
         if (o.verbosity == 1) {  // CLI (src/mc_gpu.cu:726)
@@ -842,7 +1194,7 @@ extern "C" int gasp_mc_driver_gpu_ex(gasp_gpu_grids_t grids, double beta, double
             } else if (grid_fate[i] == 1) {
               nB++;
             } else {
-              const double m = (double)mag_last[i];
+              const double m = (double)colvar[i];
               if (m > up) { grid_fate[i] = 1; nB++; }
               else if (m < dn) { grid_fate[i] = 0; nA++; }
             }

@@ -94,12 +94,74 @@ __global__ void __launch_bounds__(kCheckThreads)
   }
 }
 
+// Committor check on the device (the driver's itask-1 check, src/mc_gpu.cu:
+// 744-750): every active replica whose colvar is above up_thr (B) or below
+// dn_thr (A) gets its fate and leaves the active list (stable, in place, as
+// k_check_compact).  *attempts grows by the attempts of the sweep that
+// follows (survivors x attempts_per_replica).
+__global__ void __launch_bounds__(kCheckThreads)
+    k_fate_compact(const float *colvar, int *fates, int *active, int *n_active, double up_thr,
+                   double dn_thr, long long *attempts, long long attempts_per_replica) {
+  __shared__ int warp_sums[32];
+  __shared__ int round_total;
+  __shared__ int out_base;
+  const int n = *n_active;
+  if (threadIdx.x == 0) out_base = 0;
+  __syncthreads();
+  for (int start = 0; start < n; start += kCheckThreads * kCheckPerThread) {
+    int ids[kCheckPerThread];
+    int keep = 0;
+    const int first = start + threadIdx.x * kCheckPerThread;
+#pragma unroll
+    for (int j = 0; j < kCheckPerThread; ++j) {
+      const int i = first + j;
+      int id = -1;
+      if (i < n) {
+        id = active[i];
+        const double m = (double)colvar[id];
+        if (m > up_thr) {
+          fates[id] = 1;
+          id = -1;
+        } else if (m < dn_thr) {
+          fates[id] = 0;
+          id = -1;
+        } else {
+          keep++;
+        }
+      }
+      ids[j] = id;
+    }
+    const int off = block_exclusive_scan(keep, warp_sums, &round_total);
+    const int base = out_base;
+    int o = base + off;
+#pragma unroll
+    for (int j = 0; j < kCheckPerThread; ++j)
+      if (ids[j] >= 0) active[o++] = ids[j];
+    __syncthreads();
+    if (threadIdx.x == 0) out_base = base + round_total;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    *n_active = out_base;
+    *attempts += (long long)out_base * attempts_per_replica;
+  }
+}
+
 __global__ void k_iota(int *a, int n) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) a[i] = i;
 }
 
 }  // namespace
+
+int launch_fate_compact(const float *colvar, int *fates, int *active, int *n_active,
+                        double up_thr, double dn_thr, long long *attempts,
+                        long long attempts_per_replica, cudaStream_t s) {
+  k_fate_compact<<<1, kCheckThreads, 0, s>>>(colvar, fates, active, n_active, up_thr, dn_thr,
+                                             attempts, attempts_per_replica);
+  GASP_CUDA(cudaGetLastError());
+  return GASP_OK;
+}
 
 int launch_check_compact(const float *mag, int *active, int *n_active, int ngrids, double up_thr,
                          int *counts, int *interval, int max_intervals, cudaStream_t s) {

@@ -91,6 +91,16 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
   return false;
 }
 
+// 16-byte global -> shared copy that does not pass through registers, so a
+// thread keeps all of its im2col gathers in flight at once.
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void *src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
   uint32_t r[32];
   asm volatile(
@@ -132,8 +142,11 @@ struct ConvArgs {
   const __nv_bfloat16 *mask_src; // kBwd: activations of the previous layer (ReLU mask)
   float *pool;                   // layer 4 forward: per-image channel sums [B][32]
   int *err;                      // set on a timed-out wait
+  int ntiles;                    // images * (L*L / 128)
 };
 
+// Persistent: each CTA allocates its TMEM columns and stages the weights once,
+// then loops over 128-pixel tiles (tile = image * tiles_per_image + index).
 template <int MODE>
 __global__ void __launch_bounds__(128) k_conv_tc(ConvArgs a) {
   constexpr int K = (MODE == kFwd1) ? 16 : 9 * kC;
@@ -148,8 +161,6 @@ __global__ void __launch_bounds__(128) k_conv_tc(ConvArgs a) {
   const int L = a.L, N = L * L;
   const int tid = threadIdx.x, warp = tid >> 5;
   const int tiles_per_img = N / kTileM;
-  const int img = blockIdx.x / tiles_per_img;
-  const int p = (blockIdx.x % tiles_per_img) * kTileM + tid;
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
@@ -162,91 +173,119 @@ __global__ void __launch_bounds__(128) k_conv_tc(ConvArgs a) {
     mbar_init(smem_u32(mbar), 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-
-  // ---- stage A (im2col row of this thread's pixel) ----
-  if constexpr (MODE == kFwd1) {
-    const int8_t *s = a.spins + (size_t)img * N;
-    __align__(16) __nv_bfloat16 v[16];
-#pragma unroll
-    for (int k = 0; k < 16; ++k)
-      v[k] = __float2bfloat16_rn(k < 9 ? (float)s[nbr(p, k, L)] : 0.0f);
-    *reinterpret_cast<uint4 *>(sA + il_off(tid, 0, SBO)) = *reinterpret_cast<uint4 *>(&v[0]);
-    *reinterpret_cast<uint4 *>(sA + il_off(tid, 8, SBO)) = *reinterpret_cast<uint4 *>(&v[8]);
-  } else {
-    const __nv_bfloat16 *x = a.x + (size_t)img * N * kC;
-#pragma unroll 1
-    for (int tap = 0; tap < 9; ++tap) {
-      // forward reads the tap's neighbour; the data gradient the opposite one
-      const int q = nbr(p, MODE == kBwd ? 8 - tap : tap, L);
-      const uint4 *src = reinterpret_cast<const uint4 *>(x + (size_t)q * kC);
-#pragma unroll
-      for (int c = 0; c < 4; ++c)
-        *reinterpret_cast<uint4 *>(sA + il_off(tid, tap * kC + 8 * c, SBO)) = src[c];
-    }
-  }
-  // ---- stage B (32 x K weights) ----
+  // ---- stage B (32 x K weights), once ----
   for (int i = tid; i < kC * (K / 8); i += blockDim.x) {
     const int n = i / (K / 8), kc = i % (K / 8);
-    *reinterpret_cast<uint4 *>(sB + il_off(n, kc * 8, SBO)) =
-        *reinterpret_cast<const uint4 *>(a.w + (size_t)n * K + kc * 8);
+    cp_async16(smem_u32(sB + il_off(n, kc * 8, SBO)), a.w + (size_t)n * K + kc * 8);
   }
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  cp_async_wait_all();
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t taddr = *tslot;
 
-  if (tid == 0) {
-    const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
-#pragma unroll
-    for (int j = 0; j < K / 16; ++j)
-      umma_bf16(taddr, umma_desc(a0 + j * 256, 128, SBO), umma_desc(b0 + j * 256, 128, SBO),
-                j > 0 ? 1u : 0u);
-    umma_commit(smem_u32(mbar));
-  }
-  const bool ok = mbar_wait(smem_u32(mbar), 0);
-  if (!ok && a.err) atomicExch(a.err, 1);
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  float acc[32];
-  tmem_ld32(taddr + ((uint32_t)(warp * 32) << 16), acc);
+  uint32_t phase = 0;
+  for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
+    const int img = tile / tiles_per_img;
+    const int p0 = (tile % tiles_per_img) * kTileM;
+    const int p = p0 + tid;  // this thread's pixel in the epilogue
 
-  // ---- epilogue: this thread owns pixel p's 32 channels ----
-  if (ok) {
-    __align__(16) __nv_bfloat16 o[32];
-    if constexpr (MODE == kBwd) {
-      const __nv_bfloat16 *m = a.mask_src + ((size_t)img * N + p) * kC;
+    // ---- stage A (im2col rows of the tile) ----
+    if constexpr (MODE == kFwd1) {
+      const int8_t *sp = a.spins + (size_t)img * N;
+      __align__(16) __nv_bfloat16 v[16];
 #pragma unroll
-      for (int c = 0; c < 32; ++c)
-        o[c] = __float2bfloat16_rn(__bfloat162float(m[c]) > 0.0f ? acc[c] : 0.0f);
+      for (int k = 0; k < 16; ++k)
+        v[k] = __float2bfloat16_rn(k < 9 ? (float)sp[nbr(p, k, L)] : 0.0f);
+      *reinterpret_cast<uint4 *>(sA + il_off(tid, 0, SBO)) = *reinterpret_cast<uint4 *>(&v[0]);
+      *reinterpret_cast<uint4 *>(sA + il_off(tid, 8, SBO)) = *reinterpret_cast<uint4 *>(&v[8]);
     } else {
+      // Four consecutive threads copy the four 16-byte channel chunks of one
+      // neighbour pixel, so a warp reads 8 whole pixels (512 contiguous bytes
+      // within an image row) per instruction.
+      const __nv_bfloat16 *x = a.x + (size_t)img * N * kC;
+      const int c = tid & 3;
 #pragma unroll
-      for (int c = 0; c < 32; ++c) {
-        const float z = acc[c] + a.bias[c];
-        acc[c] = z > 0.0f ? z : 0.0f;
-        o[c] = __float2bfloat16_rn(acc[c]);
+      for (int tap = 0; tap < 9; ++tap) {
+        // forward reads the tap's neighbour; the data gradient the opposite one
+        const int t = MODE == kBwd ? 8 - tap : tap;
+#pragma unroll
+        for (int it = 0; it < kTileM / 32; ++it) {
+          const int r = it * 32 + (tid >> 2);  // tile row (pixel) handled by this thread
+          const int pp = p0 + r;
+          const int y = pp / L, xc = pp - y * L;
+          const int yy = y + t / 3 - 1, xx = xc + t % 3 - 1;
+          const int q = (yy < 0 ? yy + L : (yy >= L ? yy - L : yy)) * L +
+                        (xx < 0 ? xx + L : (xx >= L ? xx - L : xx));
+          const char *src = reinterpret_cast<const char *>(x + (size_t)q * kC) + 16 * c;
+          cp_async16(smem_u32(sA + il_off(r, tap * kC + 8 * c, SBO)), src);
+        }
+      }
+      cp_async_wait_all();
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+
+    if (tid == 0) {
+      const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
+#pragma unroll
+      for (int j = 0; j < K / 16; ++j)
+        umma_bf16(taddr, umma_desc(a0 + j * 256, 128, SBO), umma_desc(b0 + j * 256, 128, SBO),
+                  j > 0 ? 1u : 0u);
+      umma_commit(smem_u32(mbar));
+    }
+    const bool ok = mbar_wait(smem_u32(mbar), phase);
+    phase ^= 1u;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    float acc[32];
+    tmem_ld32(taddr + ((uint32_t)(warp * 32) << 16), acc);
+
+    // ---- epilogue: this thread owns pixel p's 32 channels ----
+    if (ok) {
+      __align__(16) __nv_bfloat16 o[32];
+      if constexpr (MODE == kBwd) {
+        const __nv_bfloat16 *m = a.mask_src + ((size_t)img * N + p) * kC;
+#pragma unroll
+        for (int c = 0; c < 32; ++c)
+          o[c] = __float2bfloat16_rn(__bfloat162float(m[c]) > 0.0f ? acc[c] : 0.0f);
+      } else {
+#pragma unroll
+        for (int c = 0; c < 32; ++c) {
+          const float z = acc[c] + a.bias[c];
+          acc[c] = z > 0.0f ? z : 0.0f;
+          o[c] = __float2bfloat16_rn(acc[c]);
+        }
+      }
+      uint4 *dst = reinterpret_cast<uint4 *>(a.y + ((size_t)img * N + p) * kC);
+#pragma unroll
+      for (int c = 0; c < 4; ++c) dst[c] = reinterpret_cast<uint4 *>(o)[c];
+      if (MODE == kFwd && a.pool != nullptr) {
+        // channel sums of the rounded activations over the tile
+#pragma unroll
+        for (int c = 0; c < 32; ++c) red[tid * 33 + c] = __bfloat162float(o[c]);
       }
     }
-    uint4 *dst = reinterpret_cast<uint4 *>(a.y + ((size_t)img * N + p) * kC);
-#pragma unroll
-    for (int c = 0; c < 4; ++c) dst[c] = reinterpret_cast<uint4 *>(o)[c];
     if (MODE == kFwd && a.pool != nullptr) {
-      // channel sums of the rounded activations over the tile
-#pragma unroll
-      for (int c = 0; c < 32; ++c) red[tid * 33 + c] = __bfloat162float(o[c]);
+      __syncthreads();
+      if (ok && tid < 32) {
+        float sum = 0.f;
+        for (int r = 0; r < kTileM; ++r) sum += red[r * 33 + tid];
+        atomicAdd(&a.pool[img * kC + tid], sum);
+      }
     }
-  }
-  if (MODE == kFwd && a.pool != nullptr) {
-    __syncthreads();
-    if (ok && tid < 32) {
-      float sum = 0.f;
-      for (int r = 0; r < kTileM; ++r) sum += red[r * 33 + tid];
-      atomicAdd(&a.pool[img * kC + tid], sum);
-    }
-  }
-  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-  __syncthreads();
-  if (warp == 0) {
+    // every TMEM read and shared-memory use of this tile is done before the
+    // next tile's staging and MMA
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    const int bad = __syncthreads_or(ok ? 0 : 1);
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (bad) {
+      if (tid == 0 && a.err) atomicExch(a.err, 1);
+      break;
+    }
+  }
+  if (warp == 0) {
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(32)
                  : "memory");
   }
@@ -415,11 +454,29 @@ int cnn_upload(gasp_cnn *c, const int8_t *spins, const float *labels, int batch)
 
 template <int MODE>
 int launch_conv(const ConvArgs &a, int batch, cudaStream_t s) {
-  const size_t smem = conv_smem(MODE);
+  const size_t smem_max = conv_smem(MODE);
   GASP_CUDA(cudaFuncSetAttribute(k_conv_tc<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem));
-  const int grid = batch * (a.L * a.L / kTileM);
-  k_conv_tc<MODE><<<grid, 128, smem, s>>>(a);
+                                 (int)smem_max));
+  // the pooling scratch at the end is only touched by the layer that pools
+  const size_t smem = a.pool ? smem_max : smem_max - (size_t)kTileM * 33 * 4;
+  ConvArgs b = a;
+  b.ntiles = batch * (a.L * a.L / kTileM);
+  int dev = 0, nsm = 0, smem_sm = 0;
+  GASP_CUDA(cudaGetDevice(&dev));
+  GASP_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  GASP_CUDA(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+  // CTAs per SM: shared memory (1 KiB reserved per CTA), registers, and
+  // TMEM (512 columns, 32 per CTA) bound it; the grid is sized so that all
+  // of its persistent CTAs are resident at once and share the tiles evenly.
+  int per_sm = smem_sm / (int)(smem + 1024);
+  cudaFuncAttributes fa;
+  GASP_CUDA(cudaFuncGetAttributes(&fa, k_conv_tc<MODE>));
+  const int by_regs = fa.numRegs > 0 ? 65536 / (fa.numRegs * 128) : 16;
+  if (per_sm > by_regs) per_sm = by_regs;
+  if (per_sm > 16) per_sm = 16;  // 2048 threads per SM; also all TMEM (16 x 32 columns)
+  if (per_sm < 1) per_sm = 1;
+  const int grid = b.ntiles < nsm * per_sm ? b.ntiles : nsm * per_sm;
+  k_conv_tc<MODE><<<grid, 128, smem, s>>>(b);
   GASP_CUDA(cudaGetLastError());
   return GASP_OK;
 }

@@ -83,6 +83,66 @@ int gasp_write_packed_frame(const char *path, int L, int ngrids, int isweep,
   return ok ? GASP_OK : GASP_ERR_IO;
 }
 
+int gasp_read_frame(const char *path, int iframe, int *L_out, int *ngrids_out, int *isweep_out,
+                    int *grids_out, long long grids_cap) {
+  if (!path || iframe < 0) return GASP_ERR_INVALID;
+  FILE *f = fopen(path, "rb");
+  if (!f) return GASP_ERR_IO;
+  int hdr[3] = {0, 0, 0};
+  long long payload = 0;
+  for (int k = 0;; ++k) {
+    if (fread(hdr, sizeof(int), 3, f) != 3 || hdr[0] <= 0 || hdr[1] <= 0) {
+      fclose(f);
+      return GASP_ERR_IO; /* fewer than iframe+1 frames, or a damaged header */
+    }
+    payload = ((long long)hdr[0] * hdr[0] * hdr[1] + 7) / 8;
+    if (k == iframe) break;
+    if (fseek(f, (long)payload, SEEK_CUR) != 0) {
+      fclose(f);
+      return GASP_ERR_IO;
+    }
+  }
+  if (L_out) *L_out = hdr[0];
+  if (ngrids_out) *ngrids_out = hdr[1];
+  if (isweep_out) *isweep_out = hdr[2];
+  int rc = GASP_OK;
+  if (grids_out) {
+    const long long nbits = (long long)hdr[0] * hdr[0] * hdr[1];
+    uint8_t *buf = NULL;
+    if (grids_cap < nbits) {
+      rc = GASP_ERR_INVALID;
+    } else if (!(buf = (uint8_t *)malloc((size_t)payload))) {
+      rc = GASP_ERR_ALLOC;
+    } else if (fread(buf, 1, (size_t)payload, f) != (size_t)payload) {
+      rc = GASP_ERR_IO;
+    } else {
+      for (long long i = 0; i < nbits; ++i) grids_out[i] = ((buf[i >> 3] >> (i & 7)) & 1) ? 1 : -1;
+    }
+    free(buf);
+  }
+  fclose(f);
+  return rc;
+}
+
+int gasp_write_input_grid(const char *path, int L, const int *grid) {
+  if (L <= 0 || !grid) return GASP_ERR_INVALID;
+  const int N = L * L;
+  const size_t nbytes = (size_t)(N + 7) / 8;
+  uint8_t *buf = (uint8_t *)calloc(nbytes, 1);
+  if (!buf) return GASP_ERR_ALLOC;
+  for (int s = 0; s < N; ++s)
+    if (grid[s] == 1) buf[s >> 3] |= (uint8_t)(1u << (s & 7));
+  FILE *f = fopen(path ? path : "gridinput.bin", "wb");
+  if (!f) {
+    free(buf);
+    return GASP_ERR_IO;
+  }
+  int ok = fwrite(&L, sizeof(int), 1, f) == 1 && fwrite(buf, 1, nbytes, f) == nbytes;
+  ok = (fclose(f) == 0) && ok;
+  free(buf);
+  return ok ? GASP_OK : GASP_ERR_IO;
+}
+
 int gasp_write_ising_grids(int L, int ngrids, int *ising_grids, int isweep,
                            float *magnetisation, float *lclus_size, char *cv,
                            double dn_thr, double up_thr, char *filename) {

@@ -75,12 +75,19 @@ struct SweepLaunch {
   int rng_kind;           // RngKind of p.rng
   const int *n_active_dev;// optional device count overriding n_active (graph replays)
   int lattice_in_global;  // L beyond shared memory: sweep the lattice in place in HBM
+  int mask_ok;            // at most 6 classes can reject (the acceptance-mask row kernel applies)
 };
 
 // Sweep parameters of a replica set + RNG whose tables are ready
 // (prepare_tables called for the set's beta, h); gasp_api.cu.
 SweepLaunch launch_for(gasp_grids_t *g, gasp_rng_t *r);
 int prepare_tables(gasp_grids_t *g, double beta, double h);
+
+// Device-side committor check + compaction (gasp_batch.cu): fates of active
+// replicas past a threshold, survivors compacted, attempts accumulated.
+int launch_fate_compact(const float *colvar, int *fates, int *active, int *n_active,
+                        double up_thr, double dn_thr, long long *attempts,
+                        long long attempts_per_replica, cudaStream_t s);
 
 // Device-side check + compaction of one replica group (gasp_batch.cu).
 int launch_check_compact(const float *mag, int *active, int *n_active, int ngrids,
@@ -98,6 +105,13 @@ int launch_pack_grids(const int *grids32, uint32_t *lat, int L, int ngrids, cuda
 int launch_unpack_grids(const uint32_t *lat, int *grids32, int L, int ngrids, cudaStream_t s);
 int launch_pack_frame(const uint32_t *lat, uint8_t *frame, int L, int ngrids, cudaStream_t s);
 int max_shared_L(int device);
+
+// Largest cluster of `spin` sites per replica (gasp_cluster.cu).  work_bytes
+// from largest_cluster_work_bytes: 0 when the labels fit shared memory,
+// otherwise the size of the global work area the launcher needs.
+size_t largest_cluster_work_bytes(int L, int ngrids, int device);
+int launch_largest_cluster(const uint32_t *lat, int L, int ngrids, int spin, int *work,
+                           size_t work_bytes, float *out, cudaStream_t s);
 
 }  // namespace gasp
 

@@ -326,6 +326,60 @@ __device__ __forceinline__ void row_attempt(uint32_t &s, Rng &rg, const char *la
   if (acc) *reinterpret_cast<uint32_t *>(const_cast<char *>(latb) + offc) = wc ^ (1u << (sc & 31u));
 }
 
+// row_attempt with the threshold lookup taken off the dependency chain.  For
+// the raw acceptance draw x2, the accepted classes are those whose threshold
+// is >= x2; with the classes sorted by threshold that is a suffix of the
+// order, so one count r = #{i < 6 : x2 <= S_i} over the six smallest
+// thresholds S (every other class has P > 1 and accepts everything) selects
+// a 32-bit mask pm[r] of accepted 5-spin patterns.  r and pm[r] depend only
+// on the draw, so they are computed while the lattice loads are in flight;
+// the attempt's own chain ends in a shift of that mask by the pattern.
+// Bit-identical to the table lookup: the same "x2 <= thr[class]" decisions.
+template <int L, bool kLookahead, typename Rng>
+__device__ __forceinline__ void row_attempt_mask(uint32_t &s, Rng &rg, const char *latb,
+                                                 const uint32_t (&S)[6], const uint32_t *pm,
+                                                 uint32_t lane4, float shrink) {
+  constexpr int N = L * L;
+  constexpr int R = L / 32;
+  constexpr uint32_t kMask = (uint32_t)(4 * N - 1) & ~127u;
+  const uint32_t b = s & 31u;
+  const uint32_t offc = ((s << 2) & kMask) | lane4;
+  const uint32_t offu = ((offc - 128u * R) & kMask) | lane4;
+  const uint32_t offd = ((offc + 128u * R) & kMask) | lane4;
+  const uint32_t wu = *reinterpret_cast<const uint32_t *>(latb + offu);
+  const uint32_t wd = *reinterpret_cast<const uint32_t *>(latb + offd);
+  uint32_t wc, lo, hi;
+  if constexpr (R == 1) {
+    wc = *reinterpret_cast<const uint32_t *>(latb + offc);
+    lo = hi = wc;
+  } else if constexpr (R == 2) {
+    wc = *reinterpret_cast<const uint32_t *>(latb + offc);
+    const uint32_t wx = *reinterpret_cast<const uint32_t *>(latb + (offc ^ 128u));
+    lo = (b == 0u) ? wx : wc;
+    hi = (b == 31u) ? wx : wc;
+  } else {
+    const uint32_t wi = (offc >> 7) & (uint32_t)(R - 1);
+    const uint32_t offl = (b == 0u) ? (wi == 0u ? offc + 128u * (R - 1) : offc - 128u) : offc;
+    const uint32_t offr =
+        (b == 31u) ? (wi == (uint32_t)(R - 1) ? offc - 128u * (R - 1) : offc + 128u) : offc;
+    lo = *reinterpret_cast<const uint32_t *>(latb + offl);
+    hi = *reinterpret_cast<const uint32_t *>(latb + offr);
+    wc = (b == 0u) ? hi : lo;
+  }
+  const uint32_t x2 = rg.next();
+  const uint32_t r = (uint32_t)(x2 <= S[0]) + (uint32_t)(x2 <= S[1]) + (uint32_t)(x2 <= S[2]) +
+                     (uint32_t)(x2 <= S[3]) + (uint32_t)(x2 <= S[4]) + (uint32_t)(x2 <= S[5]);
+  const uint32_t m = pm[r];
+  const uint32_t sc = s;
+  if constexpr (kLookahead) s = rg.template site<N>(shrink, N);
+  const uint32_t t = __funnelshift_r(lo, hi, b + 31u);  // bits 0,1,2: left, centre, right
+  const uint32_t u = __funnelshift_r(wu, wu, b + 29u);  // bit 3: up
+  const uint32_t d = __funnelshift_r(wd, wd, b + 28u);  // bit 4: down
+  const uint32_t pat = (t & 7u) | (u & 8u) | (d & 16u);
+  if ((m >> pat) & 1u)
+    *reinterpret_cast<uint32_t *>(const_cast<char *>(latb) + offc) = wc ^ (1u << (sc & 31u));
+}
+
 // The shared-memory words one attempt reads, and its 5-spin pattern.
 struct Probe {
   uint32_t offc;  // byte offset of the centre word
@@ -481,13 +535,17 @@ __global__ void __launch_bounds__(32) k_sweep_rows_pair(SweepLaunch p) {
   stage_out(lat, p, W, tile, lane, live, rep);
 }
 
-template <int L, bool kStatic, bool kFloatCmp, int kRng>
+template <int L, bool kStatic, bool kFloatCmp, int kRng, bool kMask = false>
 __global__ void __launch_bounds__(32) k_sweep_rows(SweepLaunch p) {
   static_assert(L % 32 == 0 && (L & (L - 1)) == 0, "L must be a power of two >= 32");
+  static_assert(!(kMask && kFloatCmp), "the acceptance mask needs integer thresholds");
   constexpr int N = L * L;
   constexpr int W = N / 32;
   __shared__ __align__(16) uint32_t thrP[32];   // threshold by 5-spin pattern
   __shared__ __align__(16) float paccP[32];     // float table by pattern
+  __shared__ uint32_t sortS[16];                // kMask: thresholds in ascending order
+  __shared__ int sortC[16];                     // kMask: their classes
+  __shared__ uint32_t pmS[8];                   // kMask: accepted-pattern masks by count
   extern __shared__ __align__(16) uint32_t dyn[];
   uint32_t *lat = LatticeStore<W * kTile, kStatic>::get(dyn);
 
@@ -498,6 +556,32 @@ __global__ void __launch_bounds__(32) k_sweep_rows(SweepLaunch p) {
     const int cls = 5 * c + __popc(lane & 0x1D);
     thrP[lane] = p.thr[cls];
     paccP[lane] = p.pacc_f[2 * cls];
+  }
+  uint32_t S[6];
+  if constexpr (kMask) {
+    if (lane < 10) {  // rank of class `lane` by (threshold, class)
+      const uint32_t v = p.thr[lane];
+      int rank = 0;
+      for (int j = 0; j < 10; ++j) {
+        const uint32_t w = p.thr[j];
+        rank += (w < v || (w == v && j < lane)) ? 1 : 0;
+      }
+      sortS[rank] = v;
+      sortC[rank] = lane;
+    }
+    __syncwarp();
+    if (lane < 7) {  // count r accepts the classes of ranks 6-r .. 9
+      uint32_t m = 0;
+      for (int q = 0; q < 32; ++q) {
+        const int cls = 5 * ((q >> 1) & 1) + __popc(q & 0x1D);
+        for (int j = 6 - lane; j < 10; ++j)
+          if (sortC[j] == cls) m |= 1u << q;
+      }
+      pmS[lane] = m;
+    }
+    __syncwarp();
+#pragma unroll
+    for (int i = 0; i < 6; ++i) S[i] = sortS[i];
   }
   const int n_act = p.n_active_dev ? *p.n_active_dev : p.n_active;
   const int tile = blockIdx.x;
@@ -520,10 +604,17 @@ __global__ void __launch_bounds__(32) k_sweep_rows(SweepLaunch p) {
     // x1(a+1), ... as in the reference.  The host keeps N*nsweeps < 2^31.
     uint32_t s = rg.template site<N>(shrink, N);
     const int total = N * p.nsweeps;
+    if constexpr (kMask) {
 #pragma unroll 5
-    for (int a = 0; a < total - 1; ++a)
-      row_attempt<L, kFloatCmp, true>(s, rg, latb, thrb, paccb, lane4, shrink);
-    row_attempt<L, kFloatCmp, false>(s, rg, latb, thrb, paccb, lane4, shrink);
+      for (int a = 0; a < total - 1; ++a)
+        row_attempt_mask<L, true>(s, rg, latb, S, pmS, lane4, shrink);
+      row_attempt_mask<L, false>(s, rg, latb, S, pmS, lane4, shrink);
+    } else {
+#pragma unroll 5
+      for (int a = 0; a < total - 1; ++a)
+        row_attempt<L, kFloatCmp, true>(s, rg, latb, thrb, paccb, lane4, shrink);
+      row_attempt<L, kFloatCmp, false>(s, rg, latb, thrb, paccb, lane4, shrink);
+    }
     rg.store(p.rng, p.rng_stride, rep);
   }
   __syncwarp();
@@ -727,6 +818,14 @@ int dispatch_kind(const SweepLaunch &p, cudaStream_t s) {
       case 32: return launch_rows(k_sweep_rows_pair<32, true, F, K>, p, 0, s);
       case 64: return launch_rows(k_sweep_rows_pair<64, true, F, K>, p, 0, s);
       case 128: return launch_rows(k_sweep_rows_pair<128, false, F, K>, p, dyn128, s);
+      default: break;
+    }
+  }
+  if (p.variant == 4 && p.mask_ok && !F) {  // row kernel with the acceptance mask
+    switch (p.L) {
+      case 32: return launch_rows(k_sweep_rows<32, true, false, K, true>, p, 0, s);
+      case 64: return launch_rows(k_sweep_rows<64, true, false, K, true>, p, 0, s);
+      case 128: return launch_rows(k_sweep_rows<128, false, false, K, true>, p, dyn128, s);
       default: break;
     }
   }

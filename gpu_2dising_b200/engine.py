@@ -121,6 +121,12 @@ class DeviceGrids:
         check(lib().gasp_magnetisation(self._h, out), "gasp_magnetisation")
         return out
 
+    def largest_cluster(self, spin):
+        """Largest periodic 4-connected cluster of `spin` per replica (float32)."""
+        out = np.empty(self.ngrids, np.float32)
+        check(lib().gasp_largest_cluster(self._h, int(spin), out), "gasp_largest_cluster")
+        return out
+
     def pack_frame(self):
         n = lib().gasp_frame_bytes(self.L, self.ngrids)
         out = np.empty(n, np.uint8)
@@ -154,13 +160,17 @@ class DeviceGrids:
 def run_driver(dgrids, rng, beta, h, tot_nsweeps, mag_output_int, grid_output_int, itask=0,
                dn_thr=-0.9, up_thr=0.9, ninputs=1, host_grids=None, fates=None,
                outfunc=None, packed_out=None, verbosity=0, compact=False,
-               threads_per_block=32, gpu_method=2, filename="gridstates.bin", first_up=None):
+               threads_per_block=32, gpu_method=2, filename="gridstates.bin", first_up=None,
+               cv="magnetisation", initial_spin=-1):
     """Runs gasp_mc_driver_gpu_ex; returns (result, fates, elapsed_s, attempts).
 
+    ``cv``: "magnetisation" or "largest_cluster" (largest cluster of spins
+    -initial_spin, compared with the thresholds as a number of sites).
     ``first_up`` (int32[ngrids], optional) receives each replica's first check
-    isweep with magnetisation above up_thr (-1: never).
+    isweep with the cv above up_thr (-1: never).
     ``outfunc(L, ngrids, grids_int32[ngrids,L,L], isweep, mag)`` mirrors the
-    reference's GridOutputFunc; ``packed_out(L, ngrids, payload_u8, isweep,
+    reference's GridOutputFunc (with cv "largest_cluster" it gets the cluster
+    sizes as a sixth argument); ``packed_out(L, ngrids, payload_u8, isweep,
     mag)`` receives gridstates.bin payloads.  Either returns 0 on success.
     """
     L, ngrids = dgrids.L, dgrids.ngrids
@@ -180,6 +190,9 @@ def run_driver(dgrids, rng, beta, h, tot_nsweeps, mag_output_int, grid_output_in
         try:
             g = np.ctypeslib.as_array(gptr, shape=(ng_ * L_ * L_,)).reshape(ng_, L_, L_)
             m = np.ctypeslib.as_array(magp, shape=(ng_,))
+            if lcp:
+                lc = np.ctypeslib.as_array(lcp, shape=(ng_,))
+                return int(outfunc(L_, ng_, g, isweep, m, lc) or 0)
             return int(outfunc(L_, ng_, g, isweep, m) or 0)
         except Exception:  # a Python error stops the driver
             return 1
@@ -204,9 +217,70 @@ def run_driver(dgrids, rng, beta, h, tot_nsweeps, mag_output_int, grid_output_in
                            C.pointer(elapsed), C.pointer(attempts), fu_ptr)
     grids_t = nat.GpuGridsT(L, ngrids, hg_ptr, dgrids.handle)
     samp = nat.SamplerT(tot_nsweeps, mag_output_int, grid_output_int)
-    calc = nat.FunctionT(itask, dn_thr, up_thr, ninputs, -1, b"magnetisation",
+    calc = nat.FunctionT(itask, dn_thr, up_thr, ninputs, int(initial_spin), cv.encode(),
                          result.ctypes.data_as(C.POINTER(C.c_float)), filename.encode())
     run = nat.GpuRunT(rng.handle, threads_per_block, gpu_method)
     check(lib().gasp_mc_driver_gpu_ex(grids_t, float(beta), float(h), fate_ptr, samp, calc, run,
                                       cb, C.byref(opts)), "gasp_mc_driver_gpu")
     return result[:nres], fates, elapsed.value, attempts.value
+
+
+# ---- checkpoints and gridstates.bin frames ---------------------------------
+_RNG_NAMES = {nat.RNG_XORWOW: "xorwow", nat.RNG_MWC64X: "mwc64x"}
+
+
+def checkpoint_info(path):
+    """Header of a checkpoint: dict(L, ngrids, rng, isweep, has_fates)."""
+    v = [C.c_int() for _ in range(5)]
+    check(lib().gasp_checkpoint_info(str(path).encode(), *[C.byref(x) for x in v]),
+          "gasp_checkpoint_info")
+    return {"L": v[0].value, "ngrids": v[1].value, "rng": _RNG_NAMES[v[2].value],
+            "isweep": v[3].value, "has_fates": bool(v[4].value)}
+
+
+def save_checkpoint(path, dgrids, rng, fates=None, isweep=0):
+    """Grids, RNG states and (optionally) fates of a run, to one file."""
+    fp = None
+    if fates is not None:
+        fates = np.ascontiguousarray(fates, np.int32)
+        assert fates.size == dgrids.ngrids
+        fp = fates.ctypes.data_as(C.c_void_p)
+    check(lib().gasp_checkpoint_save(str(path).encode(), dgrids.handle, rng.handle, fp,
+                                     int(isweep)), "gasp_checkpoint_save")
+
+
+def load_checkpoint(path, seed=0):
+    """New (DeviceGrids, RngStates, fates or None, isweep) from a checkpoint;
+    every replica continues its trajectory exactly."""
+    info = checkpoint_info(path)
+    dg = DeviceGrids(info["L"], info["ngrids"])
+    rng = RngStates(info["ngrids"], seed, kind=info["rng"])
+    fates = np.empty(info["ngrids"], np.int32)
+    isweep = C.c_int()
+    check(lib().gasp_checkpoint_load(str(path).encode(), dg.handle, rng.handle,
+                                     fates.ctypes.data_as(C.c_void_p), C.byref(isweep)),
+          "gasp_checkpoint_load")
+    return dg, rng, (fates if info["has_fates"] else None), isweep.value
+
+
+def read_frame(path, iframe, grids=True):
+    """Frame `iframe` of a gridstates.bin file: (L, ngrids, isweep, int32
+    grids [ngrids, L, L] or None).  Host only."""
+    L, ng, isw = C.c_int(), C.c_int(), C.c_int()
+    check(lib().gasp_read_frame(str(path).encode(), int(iframe), C.byref(L), C.byref(ng),
+                                C.byref(isw), None, 0), "gasp_read_frame")
+    if not grids:
+        return L.value, ng.value, isw.value, None
+    out = np.empty((ng.value, L.value, L.value), np.int32)
+    check(lib().gasp_read_frame(str(path).encode(), int(iframe), C.byref(L), C.byref(ng),
+                                C.byref(isw), out.ctypes.data_as(C.c_void_p), out.size),
+          "gasp_read_frame")
+    return L.value, ng.value, isw.value, out
+
+
+def write_input_grid(path, grid):
+    """One LxL grid (+1/-1) as gridinput.bin.  Host only."""
+    g = np.ascontiguousarray(grid, np.int32)
+    assert g.ndim == 2 and g.shape[0] == g.shape[1]
+    check(lib().gasp_write_input_grid(str(path).encode(), g.shape[0], g.reshape(-1)),
+          "gasp_write_input_grid")

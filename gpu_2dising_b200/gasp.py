@@ -14,7 +14,9 @@ deliberate:
 * there is no CPU fallback: without a CUDA device the calls raise;
 * the HDF5 side files (gridstates.hdf5 / pBgrids.hdf5) are not written
   (HDF5 is not a dependency of this library);
-* ``cv='largest_cluster'`` is rejected with NotImplementedError;
+* with ``cv='largest_cluster'`` and thresholds below 2 in magnitude a
+  UserWarning is issued through ``warnings`` (the reference sets the warning
+  as a pending exception, src/ising_ext.cu:572-577);
 * ``seed`` (default: the clock, as the reference) and ``compact`` (committor
   runs stop simulating replicas whose fate is decided; pB and fates are
   unchanged) are extra keywords;
@@ -28,6 +30,7 @@ import copy
 import os
 import sys
 import time
+import warnings
 
 import numpy as np
 
@@ -102,16 +105,20 @@ class _History:
         self.keep, self.maxhist, self.L = keep, maxhist, L
         self.ihist = 0
 
-    def __call__(self, L, ngrids, g, isweep, mag, dn, up):
+    def __call__(self, L, ngrids, g, isweep, mag, dn, up, lclus=None):
         magnetisation.append([float(x) for x in mag])
+        if lclus is not None:  # recorded only when it is the cv (src/ising_ext.cu:331-357)
+            largest_cluster.append([float(x) for x in lclus])
         if not self.keep or self.ihist >= self.maxhist:
             return 0
         snaps = []
-        cvv = mag.astype(np.float64)
+        cvv = (mag if lclus is None else lclus).astype(np.float64)
         sel = np.nonzero((cvv > dn) & (cvv < up))[0]
         for i in sel:
             snap = GridSnapObject(isweep, int(i), g[i].astype(np.int8))
             snap.magnetisation = float(mag[i])
+            if lclus is not None:
+                snap.lclus_size = float(lclus[i])
             snap.committor = -1.0
             snaps.append(snap)
             self.ihist += 1
@@ -133,8 +140,9 @@ def _require_device():
 def _check_cv(cv, up, dn):
     if cv not in ("magnetisation", "largest_cluster"):
         raise ValueError("cv must be either 'magnetisation' or 'largest_cluster'")
-    if cv == "largest_cluster":
-        raise NotImplementedError("cv='largest_cluster' is not provided by gasp-b200")
+    if cv == "largest_cluster" and (abs(up) < 2.0 or abs(dn) < 2.0):
+        warnings.warn("For cv='largest_cluster', up_threshold and dn_threshold should have "
+                      "magnitudes >= 2", UserWarning, stacklevel=3)
 
 
 def run_nucleation_swarm(L, ngrid, tot_nsweeps, beta, h, initial_spin=-1, cv="magnetisation",
@@ -165,9 +173,10 @@ def run_nucleation_swarm(L, ngrid, tot_nsweeps, beta, h, initial_spin=-1, cv="ma
         res, _, _, _ = engine.run_driver(
             dg, rng, beta, h, tot_nsweeps, mag_output_int, grid_output_int, itask=0,
             dn_thr=dn_threshold, up_thr=up_threshold, host_grids=host,
-            outfunc=lambda L_, ng_, g, isweep, m: hist(L_, ng_, g, isweep, m, dn_threshold,
-                                                        up_threshold),
-            verbosity=2 if verbose else 0, threads_per_block=threadsPerBlock)
+            outfunc=lambda L_, ng_, g, isweep, m, *lc: hist(L_, ng_, g, isweep, m, dn_threshold,
+                                                             up_threshold, *lc),
+            verbosity=2 if verbose else 0, threads_per_block=threadsPerBlock, cv=cv,
+            initial_spin=initial_spin)
     finally:
         dg.close()
         rng.close()
@@ -243,9 +252,10 @@ def run_committor_calc(L, ngrid, tot_nsweeps, beta, h, initial_spin=-1, cv="magn
             dg, rng, beta, h, tot_nsweeps, mag_output_int, grid_output_int, itask=1,
             dn_thr=dn_threshold, up_thr=up_threshold, ninputs=count, host_grids=host,
             fates=fates, compact=compact,
-            outfunc=lambda L_, ng_, g, isweep, m: hist(L_, ng_, g, isweep, m, dn_threshold,
-                                                        up_threshold),
-            verbosity=2 if verbose else 0, threads_per_block=threadsPerBlock)
+            outfunc=lambda L_, ng_, g, isweep, m, *lc: hist(L_, ng_, g, isweep, m, dn_threshold,
+                                                             up_threshold, *lc),
+            verbosity=2 if verbose else 0, threads_per_block=threadsPerBlock, cv=cv,
+            initial_spin=initial_spin)
     finally:
         dg.close()
         rng.close()

@@ -145,9 +145,12 @@ def _augment(xb, rs):
 
 
 def shoot(grids, shots, beta, h, up=0.9, dn=-0.93, cap=20000, check_int=10, seed=1,
-          rng="mwc64x", max_replicas=1 << 19):
-    """pB of each grid from `shots` trajectories (compaction on).  Returns
-    (pB float64[n], attempts, seconds)."""
+          rng="mwc64x", max_replicas=1 << 19, stats=None):
+    """pB of each grid from `shots` trajectories (compaction on), each run
+    until it reaches a basin or `cap` sweeps; unresolved trajectories are
+    left out of pB as in the reference (src/mc_gpu.cu:812-826).  Returns
+    (pB float64[n], attempts, seconds); `stats` (a dict) receives the number
+    of trajectories and of unresolved ones."""
     g = np.ascontiguousarray(grids, np.int32)
     n, L = g.shape[0], g.shape[1]
     per = max(1, max_replicas // shots)
@@ -163,16 +166,21 @@ def shoot(grids, shots, beta, h, up=0.9, dn=-0.93, cap=20000, check_int=10, seed
                                                dn_thr=dn, up_thr=up, ninputs=k, compact=True)
         pb[i:i + k] = res
         attempts += att
+        if stats is not None:
+            stats["trajectories"] = stats.get("trajectories", 0) + k * shots
+            stats["unresolved"] = stats.get("unresolved", 0) + int(np.count_nonzero(fates == -1))
         dg.close()
         r.close()
     return pb, attempts, time.perf_counter() - t0
 
 
-def harvest_snapshots(n, L=64, beta=0.54, h=0.07, replicas=32768, tot=12000, every=100,
-                      lo=-0.93, hi=0.9, seed=3, rng="mwc64x", bins=16):
+def harvest_snapshots(n, L=64, beta=0.54, h=0.07, replicas=32768, tot=12000, every=10,
+                      lo=-0.93, hi=-0.65, seed=3, rng="mwc64x", bins=14):
     """Grids from a nucleation swarm, taken every `every` sweeps while their
     magnetisation lies in (lo, hi), balanced over `bins` magnetisation bins so
-    that the barrier region is not drowned by metastable states."""
+    that the barrier region is not drowned by metastable states.  The default
+    window spans the metastable edge (m just above the A threshold -0.93)
+    to grids whose droplet is well past the critical size."""
     dg = engine.DeviceGrids(L, replicas, -np.ones((replicas, L, L), np.int32))
     r = engine.RngStates(replicas, seed, kind=rng)
     pool = [[] for _ in range(bins)]
@@ -226,9 +234,9 @@ def screen(cnn, grids, beta, h, fallback_shots=128, band=0.1, **shoot_kw):
     return out, near, time.perf_counter() - t0
 
 
-def run_experiment(n_train=8192, train_shots=256, n_test=512, test_shots=1024, n_screen=20000,
-                   baseline_shots=64, epochs=30, batch=256, lr=2e-3, beta=0.54, h=0.07,
-                   seed=0, log=None):
+def run_experiment(n_train=20000, train_shots=256, n_test=2000, test_shots=1024,
+                   n_screen=100000, baseline_shots=64, epochs=40, batch=1024, lr=2e-3, beta=0.54,
+                   h=0.07, seed=0, log=None, short_cap=4000):
     """Train the surrogate on shooting labels and measure what it gains.
 
     Returns a dict with the held-out MAE (surrogate alone and screened with
@@ -256,19 +264,60 @@ def run_experiment(n_train=8192, train_shots=256, n_test=512, test_shots=1024, n
     mae_surrogate = float(np.mean(np.abs(pred_te - y_te)))
     scr_te, near_te, _ = screen(net, te, beta, h, fallback_shots=baseline_shots, seed=seed + 17)
     mae_screened = float(np.mean(np.abs(scr_te - y_te)))
+    # the screening question: is pB in [0.3, 0.7]?
+    want, got = (y_te >= 0.3) & (y_te <= 0.7), (scr_te >= 0.3) & (scr_te <= 0.7)
+    tp = int(np.count_nonzero(want & got))
     base_te, _, _ = shoot(te, baseline_shots, beta, h, seed=seed + 19)
     mae_baseline = float(np.mean(np.abs(base_te - y_te)))
-    # throughput on the screening pool
-    _, near_sc, t_screen = screen(net, sc, beta, h, fallback_shots=baseline_shots,
-                                  seed=seed + 23)
-    _, _, t_shoot = shoot(sc, baseline_shots, beta, h, seed=seed + 29)
+    # MAE of shooting alone with fewer shots on the same held-out grids
+    mae_by_shots = {baseline_shots: mae_baseline}
+    for k, ns in enumerate((8, 16, 32)):
+        est, _, _ = shoot(te, ns, beta, h, seed=seed + 41 + k)
+        mae_by_shots[ns] = float(np.mean(np.abs(est - y_te)))
+    mid = (y_te >= 0.1) & (y_te <= 0.9)
+    # throughput on the screening pool, at the reference committor cap (20000
+    # sweeps) and at a short cap that bounds the slowest trajectories
+    t0 = time.perf_counter()
+    net.predict(sc)
+    t_cnn = time.perf_counter() - t0
+    arms = {}
+    for cap in (20000, short_cap):
+        st_fb, st_sh = {}, {}
+        _, near_sc, t_scr = screen(net, sc, beta, h, fallback_shots=baseline_shots,
+                                   seed=seed + 23, cap=cap, stats=st_fb)
+        _, a_sh, t_sh = shoot(sc, baseline_shots, beta, h, seed=seed + 29, cap=cap, stats=st_sh)
+        arms[cap] = {"screen_s": t_scr, "shoot_s": t_sh, "speedup": t_sh / t_scr,
+                     "screen_grids_per_s": sc.shape[0] / t_scr,
+                     "shoot_grids_per_s": sc.shape[0] / t_sh,
+                     "fallback_unresolved": st_fb.get("unresolved", 0),
+                     "shoot_unresolved": st_sh.get("unresolved", 0),
+                     "shoot_attempts_per_s": a_sh / t_sh}
+    t_screen, t_shoot = arms[20000]["screen_s"], arms[20000]["shoot_s"]
+    # shooting alone with the fewest shots whose held-out MAE is <= 0.05
+    few = min((k for k, v in mae_by_shots.items() if v <= 0.05), default=baseline_shots)
+    _, _, t_few = shoot(sc, few, beta, h, seed=seed + 31)
+    arms["equal_mae"] = {"shots": few, "mae": mae_by_shots[few], "shoot_s": t_few,
+                         "shoot_grids_per_s": sc.shape[0] / t_few,
+                         "speedup": t_few / t_screen}
     res = {
         "n_train": int(tr.shape[0]), "train_shots": train_shots, "n_test": int(te.shape[0]),
         "test_shots": test_shots, "n_screen": int(sc.shape[0]), "baseline_shots": baseline_shots,
         "mae_surrogate": mae_surrogate, "mae_screened": mae_screened,
         "mae_shooting_baseline": mae_baseline, "fallback_fraction": float(near_sc.mean()),
+        "mae_shooting_by_shots": {str(k): v for k, v in sorted(mae_by_shots.items())},
+        "test_mid_0.1_0.9": {"n": int(mid.sum()),
+                             "mae_surrogate": float(np.mean(np.abs(pred_te[mid] - y_te[mid]))),
+                             "mae_screened": float(np.mean(np.abs(scr_te[mid] - y_te[mid]))),
+                             "mae_shooting_baseline": float(np.mean(np.abs(base_te[mid] -
+                                                                          y_te[mid])))},
         "screen_grids_per_s": sc.shape[0] / t_screen, "shoot_grids_per_s": sc.shape[0] / t_shoot,
         "speedup": t_shoot / t_screen, "final_train_loss": hist[-1]["loss"],
+        "by_cap": {str(k): v for k, v in arms.items()},
+        "cnn_only_grids_per_s": sc.shape[0] / t_cnn,
+        "label_hist_train": np.histogram(y_tr, bins=10, range=(0.0, 1.0))[0].tolist(),
+        "label_hist_test": np.histogram(y_te, bins=10, range=(0.0, 1.0))[0].tolist(),
+        "band_0.3_0.7": {"test_in_band": int(want.sum()), "flagged": int(got.sum()),
+                         "true_positives": tp},
         "label_mean_train": float(y_tr.mean()), "times_s": t,
         "history": hist,
     }

@@ -32,7 +32,7 @@ enum {
   GASP_ERR_IO = 5,          /* file open/read/write failed                    */
   GASP_ERR_FORMAT = 6,      /* file header does not match (src/io.c:25-28)    */
   GASP_ERR_CALLBACK = 7,    /* user output callback returned non-zero         */
-  GASP_ERR_UNSUPPORTED = 8, /* e.g. L above 8192 or a CV other than magnetisation */
+  GASP_ERR_UNSUPPORTED = 8, /* e.g. L above 8192 or an unknown cv name          */
   GASP_ERR_TIMEOUT = 9      /* a bounded device-side wait expired             */
 };
 
@@ -113,7 +113,9 @@ int gasp_grids_shape(const gasp_grids_t *grids, int *L_out, int *ngrids_out);
 /* Launch tuning of a set (no reference counterpart; results never depend on
  * it).  GASP_OPT_SWEEP_VARIANT: 0 the fastest kernel for L (default), 1 the
  * generic kernel, 2 the row kernel, 3 the row kernel with pairwise
- * speculation of consecutive attempts.  GASP_OPT_WARPS_PER_CTA: tiles per
+ * speculation of consecutive attempts, 4 the row kernel with the acceptance
+ * decided by a per-draw mask of accepted neighbourhoods (falls back to 2 when
+ * more than six classes can reject).  GASP_OPT_WARPS_PER_CTA: tiles per
  * CTA of the generic kernel (1..8). */
 enum { GASP_OPT_SWEEP_VARIANT = 1, GASP_OPT_WARPS_PER_CTA = 2 };
 int gasp_grids_set_option(gasp_grids_t *grids, int option, int value);
@@ -175,6 +177,14 @@ int gasp_sweep_trace_cpu(gasp_grids_t *grids, const double *stream, double beta,
  * host_mag receives ngrids floats (synchronous). */
 int gasp_magnetisation(gasp_grids_t *grids, float *host_mag);
 
+/* Replaces compute_largest_cluster_gpu (src/mc_gpu.cu:457-526; CPU twin
+ * compute_largest_cluster_cpu, src/mc_cpu.c:310-364): size of the largest
+ * 4-connected periodic cluster of sites with spin `spin` (+1 or -1; any other
+ * value gives 0) per replica, as float.  No user work area: labels live in
+ * shared memory up to L=170 and in a library-owned area beyond.
+ * host_out receives ngrids floats (synchronous). */
+int gasp_largest_cluster(gasp_grids_t *grids, int spin, float *host_out);
+
 /* gridstates.bin frame payload (src/io.c:89-117): ceil(L*L*ngrids/8) bytes,
  * grid-major, row-major, LSB-first, bit 1 iff spin +1.  Packed on the device;
  * host_out receives the bytes (synchronous). */
@@ -189,8 +199,11 @@ typedef struct {
   int grid_output_int;
 } gasp_sampler_t;
 
-/* Mirrors mc_function_t (include/mc_cpu.h:19-28). cv must be "magnetisation"
- * (the largest_cluster CV is not provided by this library). */
+/* Mirrors mc_function_t (include/mc_cpu.h:19-28).  cv: "magnetisation" (also
+ * for NULL) or "largest_cluster", the size of the largest cluster of spins
+ * -initial_spin, computed at each check (src/mc_gpu.cu:586-605,669-672) and
+ * compared with dn_thr/up_thr as a number of sites; other names are rejected
+ * with GASP_ERR_UNSUPPORTED (the reference treats them as magnetisation). */
 typedef struct {
   int itask;           /* 0 nucleation swarm, 1 committor                  */
   double dn_thr;       /* below: basin A (strict <)                        */
@@ -339,6 +352,34 @@ int gasp_write_ising_grids(int L, int ngrids, int *ising_grids, int isweep,
 /* Appends a frame from an already packed payload. */
 int gasp_write_packed_frame(const char *path, int L, int ngrids, int isweep,
                             const uint8_t *payload, size_t nbytes);
+/* Reads frame `iframe` (0-based) of a gridstates.bin file: its header
+ * (L, ngrids, isweep) and, when grids_out is not NULL, its spins as int32
+ * [ngrids][L][L] (grids_cap ints available).  The frame layout is that of
+ * write_ising_grids (src/io.c:89-117): 12-byte header, ceil(L*L*ngrids/8)
+ * payload bytes.  GASP_ERR_IO if the file has fewer frames. */
+int gasp_read_frame(const char *path, int iframe, int *L_out, int *ngrids_out, int *isweep_out,
+                    int *grids_out, long long grids_cap);
+/* Writes one grid as gridinput.bin (int32 L, then ceil(L*L/8) bytes
+ * LSB-first, bit 1 iff +1): what the viewer's `w` key writes
+ * (tools/vis_gridstates.py:109-114) and read_input_grid (src/io.c:4-65)
+ * reads.  path NULL: "gridinput.bin". */
+int gasp_write_input_grid(const char *path, int L, const int *grid);
+
+/* ----------------------------------------------------------- checkpoints */
+/* Checkpoint / resume of a run's state (no reference counterpart; the
+ * reference can only restart from gridinput.bin, src/io.c:4-65): the grids,
+ * every replica's RNG state and optionally the committor fates, with the
+ * caller's sweep counter.  Loading into handles of the same L, ngrids and RNG
+ * kind continues every replica's trajectory bit for bit.  A driver run
+ * resumed from a checkpoint taken at a check boundary reproduces the rest of
+ * an uninterrupted run, with its isweep counted from 0 again.
+ * gasp_checkpoint_info reads the header so the caller can create the handles. */
+int gasp_checkpoint_save(const char *path, gasp_grids_t *grids, gasp_rng_t *rng,
+                         const int *fates, int isweep);
+int gasp_checkpoint_info(const char *path, int *L_out, int *ngrids_out, int *rng_kind_out,
+                         int *isweep_out, int *has_fates_out);
+int gasp_checkpoint_load(const char *path, gasp_grids_t *grids, gasp_rng_t *rng,
+                         int *fates_out, int *isweep_out);
 
 /* Replaces bootstrap_errbar (include/bootstrap.h:5, src/bootstrap.c:6-65):
  * m resamples with libc rand()%ngrids, population standard deviation.

@@ -57,6 +57,8 @@ def lib():
         L.orc_magnetisation_gpu.restype = C.c_float
         L.orc_magnetisation_cpu.argtypes = [C.c_int, _i32p]
         L.orc_magnetisation_cpu.restype = C.c_float
+        L.orc_largest_cluster.argtypes = [C.c_int, _i32p, C.c_int]
+        L.orc_largest_cluster.restype = C.c_int
         L.orc_pack_frame.argtypes = [C.c_int, C.c_int, _i32p, _u8p]
         L.orc_pack_frame.restype = C.c_longlong
         L.orc_unpack_frame.argtypes = [C.c_int, C.c_int, _u8p, _i32p]
@@ -109,6 +111,13 @@ def magnetisation_gpu(L, grids):
 def magnetisation_cpu(L, grids):
     g = np.ascontiguousarray(grids, np.int32).reshape(-1, L * L)
     return np.array([lib().orc_magnetisation_cpu(L, np.ascontiguousarray(x)) for x in g], np.float32)
+
+
+def largest_cluster(L, grids, spin):
+    """Largest cluster size of `spin` per grid (float32, as the reference)."""
+    g = np.ascontiguousarray(grids, np.int32).reshape(-1, L * L)
+    return np.array([lib().orc_largest_cluster(L, np.ascontiguousarray(x), int(spin)) for x in g],
+                    np.float32)
 
 
 def pack_frame(L, grids):

@@ -109,6 +109,44 @@ float orc_magnetisation_cpu(int L, const int *grid) {
   return (float)(m / (double)(L * L));
 }
 
+/* src/mc_cpu.c:310-364 (and its GPU twin src/mc_gpu.cu:457-526): size of the
+ * largest 4-connected cluster of sites equal to `spin`, periodic in both
+ * directions, found by flood fill from every unvisited matching site.
+ * Returns -1 if the work arrays cannot be allocated. */
+int orc_largest_cluster(int L, const int *grid, int spin) {
+  const int N = L * L;
+  unsigned char *seen = (unsigned char *)calloc((size_t)N, 1);
+  int *todo = (int *)malloc((size_t)N * sizeof(int));
+  if (!seen || !todo) {
+    free(seen);
+    free(todo);
+    return -1;
+  }
+  int best = 0;
+  for (int start = 0; start < N; ++start) {
+    if (grid[start] != spin || seen[start]) continue;
+    int head = 0, tail = 0, size = 0;
+    seen[start] = 1;
+    todo[tail++] = start;
+    while (head < tail) {
+      const int s = todo[head++];
+      ++size;
+      const int r = s / L, c = s % L;
+      const int nb[4] = {r * L + (c + L - 1) % L, r * L + (c + 1) % L,
+                         ((r + L - 1) % L) * L + c, ((r + 1) % L) * L + c};
+      for (int k = 0; k < 4; ++k)
+        if (grid[nb[k]] == spin && !seen[nb[k]]) {
+          seen[nb[k]] = 1;
+          todo[tail++] = nb[k];
+        }
+    }
+    if (size > best) best = size;
+  }
+  free(seen);
+  free(todo);
+  return best;
+}
+
 /* src/io.c:89-117: one running bit cursor over all L*L*ngrids spins. */
 long long orc_pack_frame(int L, int ngrids, const int *grids, uint8_t *out) {
   long long nbits = (long long)L * L * ngrids;

@@ -36,6 +36,8 @@ long long orc_sweep_gpu_stream(int L, int *grid, long long nattempts,
 float orc_magnetisation_gpu(int L, const int *grid);
 /* CPU flavour: double sum, (float)(m/(double)N) (src/mc_cpu.c:91-104). */
 float orc_magnetisation_cpu(int L, const int *grid);
+/* src/mc_cpu.c:310-364: largest periodic 4-connected cluster of `spin`. */
+int orc_largest_cluster(int L, const int *grid, int spin);
 
 /* gridstates.bin payload: all grids contiguous, row-major, LSB-first,
  * bit=1 iff spin==+1 (src/io.c:89-117).  Returns bytes written to `out`

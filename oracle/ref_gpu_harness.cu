@@ -14,6 +14,11 @@
 #include "mc_gpu.h"
 #include "gpu_tools.h"
 
+// The reference's cluster kernel as defined in src/mc_gpu.cu:457 (its header
+// declaration, include/mc_gpu.h:44, differs in the type of the last argument).
+__global__ void compute_largest_cluster_gpu(const int L, const int ngrids, int *d_ising_grids,
+                                            const int spin, int *d_work, float *lclus_size);
+
 namespace {
 
 int padded_ngrids(int ngrids) { return ((ngrids + 63) / 64) * 64; }
@@ -117,16 +122,38 @@ int refgpu_uniform_stream(unsigned long long seed, int ngrids, int n, float *out
   return 0;
 }
 
+// The reference cluster kernel (src/mc_gpu.cu:457-526) on caller grids,
+// tpb 32.  Every thread of the last block zeroes its own 2*L*L work slice
+// even past ngrids, so the work area here covers all launched threads.
+int refgpu_largest_cluster(int L, int ngrids, int spin, const int *grids, float *out) {
+  const int tpb = 32, blocks = (ngrids + tpb - 1) / tpb;
+  const size_t n = (size_t)L * L, nthreads = (size_t)blocks * tpb;
+  int *d_grids = nullptr, *d_work = nullptr;
+  float *d_out = nullptr;
+  HCHECK(cudaMalloc(&d_grids, n * nthreads * sizeof(int)));
+  HCHECK(cudaMemset(d_grids, 0, n * nthreads * sizeof(int)));
+  HCHECK(cudaMemcpy(d_grids, grids, n * ngrids * sizeof(int), cudaMemcpyHostToDevice));
+  HCHECK(cudaMalloc(&d_work, 2 * n * nthreads * sizeof(int)));
+  HCHECK(cudaMalloc(&d_out, nthreads * sizeof(float)));
+  compute_largest_cluster_gpu<<<blocks, tpb>>>(L, ngrids, d_grids, spin, d_work, d_out);
+  HCHECK(cudaGetLastError());
+  HCHECK(cudaMemcpy(out, d_out, ngrids * sizeof(float), cudaMemcpyDeviceToHost));
+  cudaFree(d_grids); cudaFree(d_work); cudaFree(d_out);
+  return 0;
+}
+
 static int *g_cap_grids = nullptr, *g_cap_isweep = nullptr;
-static float *g_cap_mag = nullptr;
+static float *g_cap_mag = nullptr, *g_cap_lclus = nullptr;
 static int g_cap_max = 0, g_cap_n = 0;
 
 static int capture_outfunc(int L, int ngrids, int *grid_data, int isweep, float *magnetisation,
-                           float *, char *, double, double, char *) {
+                           float *lclus, char *, double, double, char *) {
   if (g_cap_n < g_cap_max) {
     size_t n = (size_t)L * L * ngrids;
     if (g_cap_grids) memcpy(g_cap_grids + (size_t)g_cap_n * n, grid_data, n * sizeof(int));
     if (g_cap_mag) memcpy(g_cap_mag + (size_t)g_cap_n * ngrids, magnetisation, ngrids * sizeof(float));
+    if (g_cap_lclus && lclus)
+      memcpy(g_cap_lclus + (size_t)g_cap_n * ngrids, lclus, ngrids * sizeof(float));
     if (g_cap_isweep) g_cap_isweep[g_cap_n] = isweep;
   }
   g_cap_n++;
@@ -135,11 +162,16 @@ static int capture_outfunc(int L, int ngrids, int *grid_data, int isweep, float 
 
 // Runs the reference driver mc_driver_gpu (src/mc_gpu.cu:530-831) end to end
 // with a capturing output callback.  Returns the number of callback calls.
-int refgpu_run_driver(int L, int ngrids, int tpb, int method, unsigned long long seed,
-                      double beta, double h, int tot_nsweeps, int mag_output_int,
-                      int grid_output_int, int itask, double dn_thr, double up_thr,
-                      int ninputs, int *grids_inout, int *fates_inout, float *result,
-                      int max_frames, int *frame_grids, int *frame_isweep, float *frame_mag) {
+// With cv "largest_cluster" the reference's work area is sized for ngrids
+// threads (src/mc_gpu.cu:597-598) while the cluster kernel runs
+// ceil(ngrids/tpb)*tpb: callers keep ngrids a multiple of tpb.
+int refgpu_run_driver_cv(int L, int ngrids, int tpb, int method, unsigned long long seed,
+                         double beta, double h, int tot_nsweeps, int mag_output_int,
+                         int grid_output_int, int itask, double dn_thr, double up_thr,
+                         int ninputs, int *grids_inout, int *fates_inout, float *result,
+                         int max_frames, int *frame_grids, int *frame_isweep, float *frame_mag,
+                         const char *cv, int initial_spin, float *frame_lclus) {
+  if (strcmp(cv, "largest_cluster") == 0 && ngrids % tpb != 0) return -3;
   int npad = padded_ngrids(ngrids);
   size_t n = (size_t)L * L;
   int *d_grids = nullptr, *d_nbr = nullptr;
@@ -152,6 +184,7 @@ int refgpu_run_driver(int L, int ngrids, int tpb, int method, unsigned long long
   gpuInitRand(ngrids, tpb, (unsigned long)seed, &d_state);
   preComputeProbs_gpu(beta, h);
   g_cap_grids = frame_grids; g_cap_isweep = frame_isweep; g_cap_mag = frame_mag;
+  g_cap_lclus = frame_lclus;
   g_cap_max = max_frames; g_cap_n = 0;
   mc_gpu_grids_t grids; grids.L = L; grids.ngrids = ngrids; grids.ising_grids = grids_inout;
   grids.d_ising_grids = d_grids; grids.d_neighbour_list = d_nbr;
@@ -159,7 +192,7 @@ int refgpu_run_driver(int L, int ngrids, int tpb, int method, unsigned long long
   samples.mag_output_int = mag_output_int; samples.grid_output_int = grid_output_int;
   mc_function_t calc; memset(&calc, 0, sizeof calc);
   calc.itask = itask; calc.dn_thr = dn_thr; calc.up_thr = up_thr; calc.ninputs = ninputs;
-  calc.initial_spin = -1; calc.cv = (char *)"magnetisation"; calc.result = result;
+  calc.initial_spin = initial_spin; calc.cv = const_cast<char *>(cv); calc.result = result;
   calc.filename = (char *)"gridstates.bin";
   gpu_run_t gs; gs.d_state = d_state; gs.threadsPerBlock = tpb; gs.gpu_method = method;
   mc_driver_gpu(grids, beta, h, fates_inout, samples, calc, gs, capture_outfunc);
@@ -167,6 +200,17 @@ int refgpu_run_driver(int L, int ngrids, int tpb, int method, unsigned long long
   HCHECK(cudaMemcpy(grids_inout, d_grids, n * ngrids * sizeof(int), cudaMemcpyDeviceToHost));
   cudaFree(d_grids); cudaFree(d_nbr); cudaFree(d_state);
   return g_cap_n;
+}
+
+int refgpu_run_driver(int L, int ngrids, int tpb, int method, unsigned long long seed,
+                      double beta, double h, int tot_nsweeps, int mag_output_int,
+                      int grid_output_int, int itask, double dn_thr, double up_thr,
+                      int ninputs, int *grids_inout, int *fates_inout, float *result,
+                      int max_frames, int *frame_grids, int *frame_isweep, float *frame_mag) {
+  return refgpu_run_driver_cv(L, ngrids, tpb, method, seed, beta, h, tot_nsweeps, mag_output_int,
+                              grid_output_int, itask, dn_thr, up_thr, ninputs, grids_inout,
+                              fates_inout, result, max_frames, frame_grids, frame_isweep,
+                              frame_mag, "magnetisation", -1, nullptr);
 }
 
 }  // extern "C"

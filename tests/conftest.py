@@ -48,6 +48,7 @@ def ref_cpu():
     lib.ref_sweep_cpu.argtypes = [C.c_int, i32, C.c_int, C.c_double, C.c_double, C.c_int]
     lib.ref_magnetisation_cpu.argtypes = [C.c_int, i32, C.c_int]
     lib.ref_magnetisation_cpu.restype = C.c_float
+    lib.compute_largest_cluster_cpu.argtypes = [C.c_int, i32, C.c_int, C.c_int, f32]
     lib.ref_bootstrap_errbar.argtypes = [C.c_int, C.c_int, i32]
     lib.ref_bootstrap_errbar.restype = C.c_double
     lib.ref_init_grids_from_array.argtypes = [C.c_int, C.c_int, C.c_int, i32, i32]
@@ -75,6 +76,9 @@ def ref_gpu():
                                       C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int,
                                       C.c_double, C.c_double, C.c_int, i32, C.c_void_p, f32,
                                       C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.refgpu_run_driver_cv.argtypes = lib.refgpu_run_driver.argtypes + [C.c_char_p, C.c_int,
+                                                                          C.c_void_p]
+    lib.refgpu_largest_cluster.argtypes = [C.c_int, C.c_int, C.c_int, i32, f32]
     return lib
 
 

@@ -8,9 +8,14 @@ Fixtures (numpy .npz, small):
   ref_cpu_driver.npz   mc_driver_cpu runs (src/mc_cpu.c:106-308) seeded with
                        init_genrand: result, fates, callback frames, final grids
   ref_bootstrap.npz    bootstrap_errbar (src/bootstrap.c:6-65) after srand(1)
+  ref_cluster.npz      compute_largest_cluster_cpu (src/mc_cpu.c:310-364) of
+                       seeded grids (random densities around the percolation
+                       threshold, wrapping stripes, checkerboards), both spins
 
-The GPU fixtures (ref_gpu_*.npz) come from tests/golden/make_golden_gpu.py,
-which runs the reference kernels on a CUDA device.
+    python tests/golden/make_golden.py cluster   # only ref_cluster.npz
+
+The GPU parity tests compare with the reference's GPU kernels directly
+(oracle/_ref/libref_gpu.so) instead of GPU fixtures.
 """
 import ctypes as C
 import os
@@ -94,8 +99,44 @@ def run_driver(lib, case):
                 frame_mag=fm[:n * ng].reshape(n, ng))
 
 
+CLUSTER_LS = [2, 3, 5, 8, 16, 31, 64]
+
+
+def cluster_grids(L, seed):
+    """Seeded grids whose clusters wrap, percolate, or are all singletons."""
+    rng = np.random.default_rng(seed)
+    out = [np.where(rng.random((L, L)) < p, 1, -1) for p in (0.3, 0.5, 0.593, 0.7)]
+    out.append(np.ones((L, L)))
+    out.append(-np.ones((L, L)))
+    stripe = -np.ones((L, L))
+    stripe[L // 2, :] = 1  # one row: wraps around in x
+    out.append(stripe)
+    y, x = np.indices((L, L))
+    out.append(np.where((x + y) % 2 == 0, 1, -1))  # checkerboard (odd L: seam)
+    return np.stack(out).astype(np.int32)
+
+
+def make_cluster(lib):
+    lib.compute_largest_cluster_cpu.argtypes = [C.c_int, i32, C.c_int, C.c_int, f32]
+    out = {"Ls": np.array(CLUSTER_LS)}
+    for L in CLUSTER_LS:
+        g = cluster_grids(L, 1000 + L)
+        res = np.zeros((2, g.shape[0]), np.float32)
+        flat = np.ascontiguousarray(g.reshape(-1))
+        for k, spin in enumerate((1, -1)):
+            for i in range(g.shape[0]):
+                lib.compute_largest_cluster_cpu(L, flat, i, spin, res[k])
+        out[f"L{L}_grids"] = g.astype(np.int8)
+        out[f"L{L}_sizes"] = res  # [spin +1, spin -1][grid]
+    np.savez_compressed(os.path.join(HERE, "ref_cluster.npz"), **out)
+
+
 def main():
     lib = load_ref()
+    make_cluster(lib)
+    if sys.argv[1:] == ["cluster"]:
+        print("ref_cluster.npz written to", HERE)
+        return
     tabs = []
     for beta, h in TABLE_CASES:
         P = np.zeros(20, np.float64)

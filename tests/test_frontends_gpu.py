@@ -156,18 +156,22 @@ def test_cli_committor_reads_gridinput(ref_gpu, tmp_path):
 
 @pytest.mark.parametrize("L", [32, 64, 128])
 @pytest.mark.parametrize("kind", ["xorwow", "mwc64x"])
-def test_kernel_variants_agree(L, kind):
-    """The pairwise-speculative, plain row and generic kernels give identical
-    results for both RNG kinds (the speculation never changes a trajectory)."""
+@pytest.mark.parametrize("beta,h", [(0.45, 0.1), (0.5, 0.0), (1e-9, 0.1)])
+def test_kernel_variants_agree(L, kind, beta, h):
+    """The generic, row, pairwise-speculative and acceptance-mask kernels give
+    identical results for both RNG kinds.  h = 0 leaves six classes that can
+    reject (the most the mask kernel takes); at beta = 1e-9 every P rounds to
+    1.0, ten classes can reject and the mask variant falls back to the row
+    kernel."""
     ng, seed = 96, 31 + L
     g0 = np.where(np.random.default_rng(seed).random((ng, L, L)) < 0.3, 1, -1).astype(np.int32)
     outs = []
-    for variant in (0, 1, 2):
+    for variant in (0, 1, 2, 3, 4):
         dg = engine.DeviceGrids(L, ng, g0)
         dg.set_option(1, variant)
         r = engine.RngStates(ng, seed, kind=kind)
-        dg.sweep(r, 0.45, 0.1, 3)
-        dg.sweep(r, 0.45, 0.1, 2)
+        dg.sweep(r, beta, h, 3)
+        dg.sweep(r, beta, h, 2)
         outs.append((dg.download(), dg.magnetisation()))
     for o in outs[1:]:
         assert np.array_equal(outs[0][0], o[0])

@@ -164,3 +164,38 @@ def test_read_input_grid(tmp_path):
     assert rc == -2
     rc, _ = oracle.read_input_grid(str(tmp_path / "missing.bin"), L, 1)
     assert rc == -1
+
+
+def _cluster_golden():
+    d = np.load(os.path.join(GOLDEN, "ref_cluster.npz"))
+    for L in d["Ls"]:
+        yield int(L), d[f"L{L}_grids"].astype(np.int32), d[f"L{L}_sizes"]
+
+
+def test_largest_cluster_restatement_matches_golden():
+    for L, g, sizes in _cluster_golden():
+        for k, spin in enumerate((1, -1)):
+            assert np.array_equal(oracle.largest_cluster(L, g, spin), sizes[k]), (L, spin)
+
+
+def test_largest_cluster_restatement_matches_reference(ref_cpu):
+    rng = np.random.default_rng(8)
+    for L in (4, 7, 20, 45):
+        g = np.where(rng.random((6, L, L)) < 0.59, 1, -1).astype(np.int32)
+        flat = np.ascontiguousarray(g.reshape(-1))
+        for spin in (1, -1):
+            ref = np.zeros(6, np.float32)
+            for i in range(6):
+                ref_cpu.compute_largest_cluster_cpu(L, flat, i, spin, ref)
+            assert np.array_equal(oracle.largest_cluster(L, g, spin), ref)
+
+
+def test_largest_cluster_known_answers():
+    L = 6
+    g = -np.ones((1, L, L), np.int32)
+    assert oracle.largest_cluster(L, g, 1)[0] == 0
+    assert oracle.largest_cluster(L, g, -1)[0] == L * L
+    g[0, :, 0] = 1  # a column: connected through the periodic wrap in y
+    g[0, 2, L - 1] = 1  # joins the column through the wrap in x
+    assert oracle.largest_cluster(L, g, 1)[0] == L + 1
+    assert oracle.largest_cluster(L, g, 0)[0] == 0

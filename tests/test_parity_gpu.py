@@ -182,6 +182,34 @@ def test_driver_matches_reference_driver(ref_gpu, case, compact):
         assert np.array_equal(dg.download(), r_final)
 
 
+@pytest.mark.parametrize("case", [c for c in DRIVER_CASES if c[8] == 1])
+@pytest.mark.parametrize("mag_grid", [None, (10, 7)])
+def test_committor_on_device_matches_reference_driver(ref_gpu, case, mag_grid):
+    """Compaction without callbacks runs the checks on the device; fates and
+    pB must equal the reference driver's (and so the host loop's)."""
+    (L, ng, seed, beta, h, tot, mag, grid, itask, dn, up, ninputs, init) = case
+    if mag_grid is not None:  # checks every 10 sweeps, launches of 7 sweeps
+        mag, grid = mag_grid
+    g0 = _grids(L, ng, init, seed)
+    r_res, r_fates, _, _, _ = _ref_driver(ref_gpu, L, ng, seed, beta, h, tot, mag, grid, itask,
+                                          dn, up, ninputs, g0)
+    dg = engine.DeviceGrids(L, ng, g0)
+    rng = engine.RngStates(ng, seed)
+    res, fates, _, att = engine.run_driver(dg, rng, beta, h, tot, mag, grid, itask=1, dn_thr=dn,
+                                           up_thr=up, ninputs=ninputs, compact=True)
+    assert np.array_equal(fates, r_fates)
+    assert np.array_equal(res, r_res)
+    # the host loop (a no-op packed callback keeps the driver on the host)
+    dg2 = engine.DeviceGrids(L, ng, g0)
+    rng2 = engine.RngStates(ng, seed)
+    res2, fates2, _, att2 = engine.run_driver(dg2, rng2, beta, h, tot, mag, grid, itask=1,
+                                              dn_thr=dn, up_thr=up, ninputs=ninputs,
+                                              compact=True, packed_out=lambda *a: 0)
+    assert np.array_equal(fates2, fates) and np.array_equal(res2, res)
+    assert att == att2
+    assert np.array_equal(dg.download(), dg2.download())
+
+
 @pytest.mark.parametrize("L,ng", [(5, 7), (16, 33), (64, 64), (30, 65)])
 def test_pack_unpack_frame_and_magnetisation(L, ng):
     g = _grids(L, ng, "random", L + ng)
