@@ -27,6 +27,8 @@ import numpy as np
 REPO = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, REPO)
 
+from gpu_2dising_b200 import shards  # noqa: E402  (replica shards over ranks)
+
 L, R, BETA, H = 64, 32768, 0.54, 0.07
 SWEEPS_PER_STEP, MAG_INT, GRID_INT = 100, 100, 1000
 SEED = 20240501
@@ -177,7 +179,8 @@ def read_profile_traffic():
 
 def run_e2e(args, rank, world, dist, torch, engine):
     engine.set_stream(0)
-    host = -np.ones((R, L, L), np.int32)
+    # the user's initial grids, in pinned host memory
+    host = torch.full((R, L, L), -1, dtype=torch.int32).pin_memory().numpy()
     dumped = [0]
 
     def packed(L_, ng_, payload, isweep, m):
@@ -190,7 +193,7 @@ def run_e2e(args, rank, world, dist, torch, engine):
     t0 = time.perf_counter()
     dg2 = engine.DeviceGrids(L, R, host)
     t1 = time.perf_counter()
-    rng2 = engine.RngStates(R, SEED + 7919 * rank + 1, kind=args.rng)
+    rng2 = engine.RngStates(R, shards.rank_seed(SEED, rank) + 1, kind=args.rng)
     t2 = time.perf_counter()
     _, _, drv_s, attempts = engine.run_driver(dg2, rng2, BETA, H, SWEEPS_PER_STEP * args.steps,
                                           MAG_INT, GRID_INT, itask=0, dn_thr=-0.9, up_thr=0.9,
@@ -198,10 +201,7 @@ def run_e2e(args, rank, world, dist, torch, engine):
     t3 = time.perf_counter()
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
-    if dist is not None:
-        t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = shards.max_over_ranks(e2e_s, dist, device="cuda")
     h2d = R * L * L * 4 + 20 * 4 + 20 * 8
     d2h = R * 4 * (SWEEPS_PER_STEP * args.steps // MAG_INT) + dumped[0]
     dg2.close()
@@ -233,7 +233,7 @@ def run_ours(args, rank, world, local_rank):
 
     dg = engine.DeviceGrids(L, R, -np.ones((R, L, L), np.int32))
     dg.set_option(1, args.variant)  # GASP_OPT_SWEEP_VARIANT
-    rng = engine.RngStates(R, SEED + 7919 * rank, kind=args.rng)
+    rng = engine.RngStates(R, shards.rank_seed(SEED, rank), kind=args.rng)
 
     def barrier():
         torch.cuda.synchronize()
@@ -255,11 +255,7 @@ def run_ours(args, rank, world, local_rank):
                 e1.record(stream)
             barrier()
         t_ms = sum(e0.elapsed_time(e1) for e0, e1 in evs)
-    t_max = t_ms
-    if dist is not None:
-        t = torch.tensor([t_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_max = float(t.item())
+    t_max = shards.max_over_ranks(t_ms, dist, device="cuda")
     attempts_step = float(R) * L * L * SWEEPS_PER_STEP
     value = attempts_step * args.steps * world / (t_max / 1e3)
     mag = dg.magnetisation()
@@ -406,6 +402,81 @@ def run_committor(args):
     print(json.dumps(line), flush=True)
 
 
+def run_cnn(args):
+    """Surrogate CNN inference throughput: predict() on int8 L=64 grids from
+    host memory (batches of 1024), timed on the host around synchronised
+    calls, plus one timed Adam step on a 1024-grid batch."""
+    from gpu_2dising_b200 import engine, surrogate
+    engine.init_device(0)
+    n = args.cnn_grids
+    rs = np.random.default_rng(SEED)
+    grids = np.where(rs.random((n, L, L)) < 0.1, 1, -1).astype(np.int8)
+    labels = rs.random(1024).astype(np.float32)
+    net = surrogate.CommittorCNN(L, 1024, surrogate.init_params(0))
+    for _ in range(args.warmup):
+        net.predict(grids[:2048])
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        net.predict(grids)
+    pred_s = (time.perf_counter() - t0) / args.steps
+    for _ in range(args.warmup):
+        net.train_step(grids[:1024], labels, 1e-3)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        net.train_step(grids[:1024], labels, 1e-3)
+    step_s = (time.perf_counter() - t0) / args.steps
+    flop = 2.0 * L * L * (32 * 9 + 3 * 32 * 288) + 2.0 * 32  # convolutions + head, per grid
+    line = {"metric": "committor CNN inference (grids/s)", "value": n / pred_s, "unit": "grids/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * pred_s, "higher_is_better": True, "dtype": "bf16",
+            "effective_tflops": flop * n / pred_s / 1e12,
+            "train_step_ms_batch1024": 1e3 * step_s,
+            "config": {"workload": f"predict on {n} int8 L=64 grids (host memory, batches of "
+                                   "1024); 4x conv3x3(32) tcgen05, pool, 32->1"}}
+    net.close()
+    print(json.dumps(line), flush=True)
+
+
+def run_rate(args):
+    """The full production swarm of the headline workload (L=64, 32768
+    replicas, beta=0.54, h=0.07, 50 000 sweeps, checks every 100, dumps every
+    1000 not written): nucleated-fraction curve fitted to 1 - exp(-k (t - t0))
+    as the reference's notebook does, bootstrap errors over replicas, for the
+    reference stream and the production stream."""
+    from gpu_2dising_b200 import analysis, engine
+    engine.init_device(0)
+    tot = args.rate_sweeps
+    out = {}
+    for kind in ("xorwow", "mwc64x"):
+        dg = engine.DeviceGrids(L, R)
+        rng = engine.RngStates(R, SEED, kind=kind)
+        fu = np.full(R, -1, np.int32)
+        t0 = time.perf_counter()
+        res, _, drv_s, att = engine.run_driver(dg, rng, BETA, H, tot, MAG_INT, GRID_INT, itask=0,
+                                               dn_thr=-0.9, up_thr=0.9, first_up=fu)
+        wall = time.perf_counter() - t0
+        k, t_ind, k_site = analysis.fit_nucleation_rate(res, MAG_INT, L=L)
+        bs = analysis.bootstrap_rate(fu, tot, MAG_INT, nboot=100, L=L)
+        out[kind] = {"k": k, "t0": t_ind, "k_per_site": k_site, "k_se": bs["k_se"],
+                     "t0_se": bs["t0_se"], "final_fraction": float(res[-1]),
+                     "never_crossed": int(np.count_nonzero(fu < 0)), "wall_s": wall,
+                     "attempts_per_s": att / drv_s}
+        dg.close()
+        rng.close()
+    a, b = out["xorwow"], out["mwc64x"]
+    line = {"metric": "nucleation rate k (1/sweep), full production swarm", "value": a["k"],
+            "unit": "1/sweep", "n_gpus": 1, "higher_is_better": None,
+            "exact_stream": a, "production_stream": b,
+            "k_diff_sigma": abs(a["k"] - b["k"]) / float(np.hypot(a["k_se"], b["k_se"])),
+            "t0_diff_sigma": abs(a["t0"] - b["t0"]) / float(np.hypot(a["t0_se"], b["t0_se"])),
+            "published_anchor": {"k": 1.5032e-4, "replicas": 1024,
+                                 "source": "Jupyter/GASP_rates.ipynb:178 (single run, Quadro "
+                                           "P2000)"},
+            "config": {"workload": f"L=64, {R} replicas, beta=0.54, h=0.07, all-down, {tot} "
+                                   "sweeps, magnetisation checked every 100 sweeps, up 0.9"}}
+    print(json.dumps(line), flush=True)
+
+
 def run_surrogate(args):
     """The learned committor surrogate: snapshots from a swarm at beta=0.54,
     h=0.07, shooting labels, GPU training, held-out MAE against 1024-shot
@@ -440,9 +511,11 @@ def main():
                     help="smaller values give a short launch for ncu captures")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--workload", default="swarm",
-                    choices=["swarm", "batched", "committor", "surrogate"],
+                    choices=["swarm", "batched", "committor", "surrogate", "cnn", "rate"],
                     help="swarm: the headline single-group swarm; batched: uneven groups; "
                          "committor: seeded droplet shooting")
+    ap.add_argument("--cnn-grids", type=int, default=100000)
+    ap.add_argument("--rate-sweeps", type=int, default=50000)
     ap.add_argument("--committor-inputs", type=int, default=64)
     ap.add_argument("--committor-shots", type=int, default=4096)
     ap.add_argument("--committor-check", type=int, default=10)
@@ -473,6 +546,12 @@ def main():
     elif args.workload == "surrogate":
         if rank == 0:
             run_surrogate(args)
+    elif args.workload == "cnn":
+        if rank == 0:
+            run_cnn(args)
+    elif args.workload == "rate":
+        if rank == 0:
+            run_rate(args)
     else:
         run_ours(args, rank, world, local_rank)
 

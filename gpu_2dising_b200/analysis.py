@@ -41,8 +41,8 @@ def fraction_from_first_passage(first_passage, tot_nsweeps, mag_output_int):
     (-1: never crossed)."""
     fp = np.asarray(first_passage)
     t = np.arange(tot_nsweeps // mag_output_int) * mag_output_int
-    done = fp >= 0
-    return ((fp[None, :] <= t[:, None]) & done[None, :]).mean(axis=1)
+    crossed = np.sort(fp[fp >= 0])
+    return np.searchsorted(crossed, t, side="right") / max(fp.size, 1)
 
 
 def bootstrap_rate(first_passage, tot_nsweeps, mag_output_int, nboot=200, block=1, seed=0,

@@ -291,6 +291,190 @@ __global__ void __launch_bounds__(128) k_conv_tc(ConvArgs a) {
   }
 }
 
+// The 32-channel layers without an im2col buffer.  A tile's 128 output
+// pixels p0..p0+127 need input pixels p0-L .. p0+127+L (a window of
+// W = 128 + 2L consecutive pixels, row-major, rows wrapping); the window is
+// staged three times, rotated by dx = -1, 0, +1 within each image row, so
+// the A operand of tap (dy, dx) is the rotated copy dx starting (dy+1)*L
+// pixels into the window: 128 consecutive pixels at a 16-byte stride, which a
+// UMMA descriptor addresses directly (8-pixel groups 128 B apart, 8-channel
+// chunks W*16 B apart).  Shared memory per tile: 3 * W * 64 B (48 KB at L=64)
+// instead of the 72 KB im2col, and every input pixel is read from L2 once per
+// tile instead of nine times.  Same arithmetic as k_conv_tc (same K order:
+// tap-major, 32 channels per tap; same FP32 accumulation order per MMA).
+//
+// LT > 0 (L = 32, 64, 128, dividing the 128-pixel tile): the window is whole
+// image rows, so each thread loads its 16-byte chunks once from global memory
+// into registers and stores them to the three rotated copies itself (one L2
+// read per input chunk); LT == 0: any L, three cp.async per chunk.
+template <int MODE, int LT>
+__global__ void __launch_bounds__(128) k_conv_win(ConvArgs a) {
+  static_assert(MODE == kFwd || MODE == kBwd, "32-channel layers only");
+  static_assert(LT == 0 || (kTileM % (LT > 0 ? LT : 1) == 0 && (LT & (LT - 1)) == 0),
+                "LT divides the tile");
+  constexpr int K = 9 * kC;
+  constexpr int SBO_B = K * 16;  // weights: bytes between 8-row groups
+  extern __shared__ __align__(1024) unsigned char smem[];
+  const int L = a.L, N = L * L;
+  const int W = kTileM + 2 * L;          // window pixels
+  const uint32_t lbo = (uint32_t)W * 16; // bytes between 8-channel chunks
+  const uint32_t vstride = 4u * lbo;     // bytes between the three rotated copies
+  unsigned char *sA = smem;                             // [3][4][W][16 B]
+  unsigned char *sB = smem + 3 * vstride;               // 32 x K bf16 (interleaved)
+  uint64_t *mbar = reinterpret_cast<uint64_t *>(sB + kC * K * 2);
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(mbar + 1);
+  float *red = reinterpret_cast<float *>(tslot + 4);   // [128][33] (pool)
+
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int tiles_per_img = N / kTileM;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(tslot)),
+                 "r"(32)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    mbar_init(smem_u32(mbar), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  for (int i = tid; i < kC * (K / 8); i += blockDim.x) {
+    const int n = i / (K / 8), kc = i % (K / 8);
+    cp_async16(smem_u32(sB + il_off(n, kc * 8, SBO_B)), a.w + (size_t)n * K + kc * 8);
+  }
+  cp_async_wait_all();
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t taddr = *tslot;
+
+  uint32_t phase = 0;
+  for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
+    const int img = tile / tiles_per_img;
+    const int p0 = (tile % tiles_per_img) * kTileM;
+    const int p = p0 + tid;
+    const __nv_bfloat16 *x = a.x + (size_t)img * N * kC;
+
+    // ---- stage the three rotated windows (16-byte chunks, channel chunk fastest) ----
+    if constexpr (LT > 0) {
+      constexpr int LR = LT > 0 ? LT : 1;         // LT (never 0 on this branch)
+      constexpr int kWin = kTileM + 2 * LR;       // window pixels: kTileM / LT + 2 whole rows
+      constexpr int kPer = kWin * 4 / 128;        // chunks per thread
+      const int y0 = p0 / LR;                     // first output row of the tile
+      uint4 v4[kPer];
+#pragma unroll
+      for (int j = 0; j < kPer; ++j) {
+        const int idx = j * 128 + tid;
+        const int c = idx & 3, w = idx >> 2;
+        int row = y0 - 1 + w / LR;
+        row = row < 0 ? row + LR : (row >= LR ? row - LR : row);
+        v4[j] = *reinterpret_cast<const uint4 *>(x + ((size_t)row * LR + (w % LR)) * kC + 8 * c);
+      }
+#pragma unroll
+      for (int j = 0; j < kPer; ++j) {
+        const int idx = j * 128 + tid;
+        const int c = idx & 3, w = idx >> 2;
+        const int col = w % LR, rbase = w - col;
+#pragma unroll
+        for (int v = 0; v < 3; ++v) {  // copy v holds, at column col', input column col' + v - 1
+          const int cd = (col - (v - 1) + LR) % LR;
+          *reinterpret_cast<uint4 *>(sA + v * vstride + c * lbo + (uint32_t)(rbase + cd) * 16) =
+              v4[j];
+        }
+      }
+    } else {
+      for (int i = tid; i < 3 * W * 4; i += blockDim.x) {
+        const int c = i & 3;
+        const int w = (i >> 2) % W;
+        const int v = (i >> 2) / W;                // rotation dx = v - 1
+        int q = p0 - L + w;
+        q = q < 0 ? q + N : (q >= N ? q - N : q);  // window pixel (rows wrap)
+        const int r = q / L, col = q - r * L;
+        int cs = col + v - 1;
+        cs = cs < 0 ? cs + L : (cs >= L ? cs - L : cs);
+        const char *src = reinterpret_cast<const char *>(x + ((size_t)r * L + cs) * kC) + 16 * c;
+        cp_async16(smem_u32(sA + v * vstride + c * lbo + (uint32_t)w * 16), src);
+      }
+      cp_async_wait_all();
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+
+    if (tid == 0) {
+      const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
+#pragma unroll
+      for (int tap = 0; tap < 9; ++tap) {
+        // forward reads the tap's neighbour; the data gradient the opposite one
+        const int t = MODE == kBwd ? 8 - tap : tap;
+        const int dy = t / 3 - 1, dx = t % 3 - 1;
+        const uint32_t abase = a0 + (uint32_t)(dx + 1) * vstride + (uint32_t)((dy + 1) * L) * 16;
+#pragma unroll
+        for (int j = 0; j < 2; ++j)
+          umma_bf16(taddr, umma_desc(abase + 2u * j * lbo, lbo, 128),
+                    umma_desc(b0 + (uint32_t)(tap * 2 + j) * 256, 128, SBO_B),
+                    (tap | j) ? 1u : 0u);
+      }
+      umma_commit(smem_u32(mbar));
+    }
+    const bool ok = mbar_wait(smem_u32(mbar), phase);
+    phase ^= 1u;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    float acc[32];
+    tmem_ld32(taddr + ((uint32_t)(warp * 32) << 16), acc);
+
+    if (ok) {
+      __align__(16) __nv_bfloat16 o[32];
+      if constexpr (MODE == kBwd) {
+        const __nv_bfloat16 *m = a.mask_src + ((size_t)img * N + p) * kC;
+#pragma unroll
+        for (int c = 0; c < 32; ++c)
+          o[c] = __float2bfloat16_rn(__bfloat162float(m[c]) > 0.0f ? acc[c] : 0.0f);
+      } else {
+#pragma unroll
+        for (int c = 0; c < 32; ++c) {
+          const float z = acc[c] + a.bias[c];
+          acc[c] = z > 0.0f ? z : 0.0f;
+          o[c] = __float2bfloat16_rn(acc[c]);
+        }
+      }
+      uint4 *dst = reinterpret_cast<uint4 *>(a.y + ((size_t)img * N + p) * kC);
+#pragma unroll
+      for (int c = 0; c < 4; ++c) dst[c] = reinterpret_cast<uint4 *>(o)[c];
+      if (MODE == kFwd && a.pool != nullptr) {
+#pragma unroll
+        for (int c = 0; c < 32; ++c) red[tid * 33 + c] = __bfloat162float(o[c]);
+      }
+    }
+    if (MODE == kFwd && a.pool != nullptr) {
+      __syncthreads();
+      if (ok && tid < 32) {
+        float sum = 0.f;
+        for (int r = 0; r < kTileM; ++r) sum += red[r * 33 + tid];
+        atomicAdd(&a.pool[img * kC + tid], sum);
+      }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    const int bad = __syncthreads_or(ok ? 0 : 1);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (bad) {
+      if (tid == 0 && a.err) atomicExch(a.err, 1);
+      break;
+    }
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(32)
+                 : "memory");
+  }
+}
+
+size_t conv_win_smem(int L, bool pool) {
+  const size_t W = (size_t)kTileM + 2 * (size_t)L;
+  return 3 * 4 * W * 16 + (size_t)kC * 9 * kC * 2 + 64 + (pool ? (size_t)kTileM * 33 * 4 : 0);
+}
+
 size_t conv_smem(int mode) {
   const int K = mode == kFwd1 ? 16 : 9 * kC;
   return (size_t)kTileM * K * 2 + (size_t)kC * K * 2 + 64 + (size_t)kTileM * 33 * 4;
@@ -452,33 +636,53 @@ int cnn_upload(gasp_cnn *c, const int8_t *spins, const float *labels, int batch)
   return GASP_OK;
 }
 
-template <int MODE>
-int launch_conv(const ConvArgs &a, int batch, cudaStream_t s) {
-  const size_t smem_max = conv_smem(MODE);
-  GASP_CUDA(cudaFuncSetAttribute(k_conv_tc<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem_max));
-  // the pooling scratch at the end is only touched by the layer that pools
-  const size_t smem = a.pool ? smem_max : smem_max - (size_t)kTileM * 33 * 4;
-  ConvArgs b = a;
-  b.ntiles = batch * (a.L * a.L / kTileM);
+// Persistent launch of a convolution kernel: the grid is sized so that all
+// of its CTAs are resident at once and share the tiles evenly.  CTAs per SM
+// are bounded by shared memory (1 KiB reserved per CTA), registers, and TMEM
+// (512 columns, 32 per CTA).
+template <typename Kern>
+int launch_persistent(Kern kern, size_t smem_max, size_t smem, const ConvArgs &b, cudaStream_t s) {
+  GASP_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max));
   int dev = 0, nsm = 0, smem_sm = 0;
   GASP_CUDA(cudaGetDevice(&dev));
   GASP_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
   GASP_CUDA(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
-  // CTAs per SM: shared memory (1 KiB reserved per CTA), registers, and
-  // TMEM (512 columns, 32 per CTA) bound it; the grid is sized so that all
-  // of its persistent CTAs are resident at once and share the tiles evenly.
   int per_sm = smem_sm / (int)(smem + 1024);
   cudaFuncAttributes fa;
-  GASP_CUDA(cudaFuncGetAttributes(&fa, k_conv_tc<MODE>));
+  GASP_CUDA(cudaFuncGetAttributes(&fa, kern));
   const int by_regs = fa.numRegs > 0 ? 65536 / (fa.numRegs * 128) : 16;
   if (per_sm > by_regs) per_sm = by_regs;
   if (per_sm > 16) per_sm = 16;  // 2048 threads per SM; also all TMEM (16 x 32 columns)
   if (per_sm < 1) per_sm = 1;
   const int grid = b.ntiles < nsm * per_sm ? b.ntiles : nsm * per_sm;
-  k_conv_tc<MODE><<<grid, 128, smem, s>>>(b);
+  kern<<<grid, 128, smem, s>>>(b);
   GASP_CUDA(cudaGetLastError());
   return GASP_OK;
+}
+
+// Largest shared-memory footprint the window kernel is used with.
+constexpr size_t kWinSmemLimit = 110 * 1024;
+
+template <int MODE>
+int launch_conv(const ConvArgs &a, int batch, cudaStream_t s) {
+  ConvArgs b = a;
+  b.ntiles = batch * (a.L * a.L / kTileM);
+  if constexpr (MODE != kFwd1) {
+    const size_t win_max = conv_win_smem(a.L, MODE == kFwd);
+    if (win_max <= kWinSmemLimit) {
+      const size_t sm = conv_win_smem(a.L, a.pool != nullptr);
+      switch (a.L) {
+        case 32: return launch_persistent(k_conv_win<MODE, 32>, win_max, sm, b, s);
+        case 64: return launch_persistent(k_conv_win<MODE, 64>, win_max, sm, b, s);
+        case 128: return launch_persistent(k_conv_win<MODE, 128>, win_max, sm, b, s);
+        default: return launch_persistent(k_conv_win<MODE, 0>, win_max, sm, b, s);
+      }
+    }
+  }
+  const size_t smem_max = conv_smem(MODE);
+  // the pooling scratch at the end is only touched by the layer that pools
+  const size_t smem = a.pool ? smem_max : smem_max - (size_t)kTileM * 33 * 4;
+  return launch_persistent(k_conv_tc<MODE>, smem_max, smem, b, s);
 }
 
 int cnn_forward(gasp_cnn *c, int batch, cudaStream_t s) {

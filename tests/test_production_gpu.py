@@ -89,3 +89,25 @@ def test_committor_agrees_within_binomial_error():
     assert informative.any(), out
     se = np.sqrt(pa * (1 - pa) / n + pb * (1 - pb) / n)
     assert np.all(np.abs(pa - pb)[informative] < 4 * se[informative]), out
+
+
+def test_committor_of_13x13_square_matches_published_value():
+    """The reference's own published committor check (Jupyter/GASP_Tests.ipynb,
+    cells 21-23): a 13x13 square of +1 spins centred in an all-down L=64
+    lattice, beta=0.54, h=0.07, up 0.9, dn -0.93, checks every 100 sweeps;
+    ten repeats of 1024 shots gave pB = 0.7818 +- 0.0060 (mean +- standard
+    error).  Both streams must agree with it within 4 combined standard
+    errors."""
+    Lq, n, beta, h = 64, 8192, 0.54, 0.07
+    yy, xx = np.mgrid[0:Lq, 0:Lq]
+    square = np.where((np.abs(yy - Lq / 2) <= 6) & (np.abs(xx - Lq / 2) <= 6), 1, -1)
+    for kind, seed in (("xorwow", 101), ("mwc64x", 202)):
+        dg = engine.DeviceGrids(Lq, n)
+        dg.upload_inputs(square[None].astype(np.int32))
+        rng = engine.RngStates(n, seed, kind=kind)
+        res, fates, _, _ = engine.run_driver(dg, rng, beta, h, 50000, 100, 100, itask=1,
+                                             dn_thr=-0.93, up_thr=0.9, ninputs=1, compact=True)
+        assert np.count_nonzero(fates == -1) == 0
+        pb = float(res[0])
+        se = np.sqrt(pb * (1 - pb) / n + 0.0060 ** 2)
+        assert abs(pb - 0.7818) < 4 * se, (kind, pb)
