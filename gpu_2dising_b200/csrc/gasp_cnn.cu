@@ -236,7 +236,11 @@ __global__ void __launch_bounds__(128) k_conv_tc(ConvArgs a) {
                   j > 0 ? 1u : 0u);
       umma_commit(smem_u32(mbar));
     }
-    const bool ok = mbar_wait(smem_u32(mbar), phase);
+    // One thread polls the MMA barrier; the CTA barrier passes the result on
+    // (127 spinning threads would keep the shared-memory pipe busy).
+    bool waited = true;
+    if (tid == 0) waited = mbar_wait(smem_u32(mbar), phase);
+    const bool ok = __syncthreads_and(waited ? 1 : 0) != 0;
     phase ^= 1u;
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     float acc[32];
@@ -419,7 +423,11 @@ __global__ void __launch_bounds__(128) k_conv_win(ConvArgs a) {
       }
       umma_commit(smem_u32(mbar));
     }
-    const bool ok = mbar_wait(smem_u32(mbar), phase);
+    // One thread polls the MMA barrier; the CTA barrier passes the result on
+    // (127 spinning threads would keep the shared-memory pipe busy).
+    bool waited = true;
+    if (tid == 0) waited = mbar_wait(smem_u32(mbar), phase);
+    const bool ok = __syncthreads_and(waited ? 1 : 0) != 0;
     phase ^= 1u;
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     float acc[32];
@@ -537,6 +545,85 @@ __global__ void __launch_bounds__(256) k_conv_dw(int L, int B, const __nv_bfloat
     if (k < K) atomicAdd(&dW[co * K + k], acc[j]);
   }
   if (k0 == 0) atomicAdd(&db[co], accb);
+}
+
+// FP32 weight gradient of a 32->32 layer, register-tiled: dW[co][k] +=
+// sum_p dZ[p][co] * X[p, k] (k = tap*32 + ci, X the layer input at the tap's
+// neighbour).  A block takes chunks of 32 pixels; thread t accumulates the 4
+// output channels 4*(t/32).. and the 9 k values (t%32) + 32*j, so each pixel
+// costs it 13 shared-memory loads for 36 FMAs (broadcast dZ, conflict-free X).
+// The neighbour rows are gathered with 16-byte loads.  Partial sums go to dW
+// with one atomicAdd per value and block.
+__global__ void __launch_bounds__(256) k_conv_dw32(int L, int B, const __nv_bfloat16 *dz,
+                                                   const __nv_bfloat16 *xin, float *dW,
+                                                   float *db) {
+  constexpr int K = 9 * kC;  // 288
+  constexpr int P = 32;      // pixels per chunk
+  __shared__ __align__(16) float s_x[P][K];
+  __shared__ __align__(16) float s_dz[P][kC];
+  const int N = L * L;
+  const int tid = threadIdx.x;
+  const int cog = (tid >> 5) * 4;  // first of this thread's 4 output channels
+  const int kg = tid & 31;         // this thread's k values: kg + 32 j
+  float acc[4][9];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 9; ++j) acc[i][j] = 0.f;
+  float accb[4] = {0.f, 0.f, 0.f, 0.f};
+  const long long nchunks = (long long)B * N / P;
+  for (long long ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
+    const long long pix0 = ch * P;
+    const int img = (int)(pix0 / N);
+    const int p0 = (int)(pix0 % N);
+    // dZ rows: 32 pixels x 32 channels = 128 chunks of 8 bf16
+    if (tid < P * 4) {
+      const int r = tid >> 2, c8 = (tid & 3) * 8;
+      const uint4 v = *reinterpret_cast<const uint4 *>(dz + ((size_t)img * N + p0 + r) * kC + c8);
+      const __nv_bfloat16 *h = reinterpret_cast<const __nv_bfloat16 *>(&v);
+#pragma unroll
+      for (int e = 0; e < 8; ++e) s_dz[r][c8 + e] = __bfloat162float(h[e]);
+    }
+    // X at the 9 neighbours: 32 pixels x 9 taps x 4 chunks of 8 bf16
+    for (int i = tid; i < P * 9 * 4; i += blockDim.x) {
+      const int r = i / 36, rem = i - r * 36, tap = rem >> 2, c8 = (rem & 3) * 8;
+      const int q = nbr(p0 + r, tap, L);
+      const uint4 v = *reinterpret_cast<const uint4 *>(xin + ((size_t)img * N + q) * kC + c8);
+      const __nv_bfloat16 *h = reinterpret_cast<const __nv_bfloat16 *>(&v);
+      float4 lo, hi;
+      lo.x = __bfloat162float(h[0]); lo.y = __bfloat162float(h[1]);
+      lo.z = __bfloat162float(h[2]); lo.w = __bfloat162float(h[3]);
+      hi.x = __bfloat162float(h[4]); hi.y = __bfloat162float(h[5]);
+      hi.z = __bfloat162float(h[6]); hi.w = __bfloat162float(h[7]);
+      *reinterpret_cast<float4 *>(&s_x[r][tap * kC + c8]) = lo;
+      *reinterpret_cast<float4 *>(&s_x[r][tap * kC + c8 + 4]) = hi;
+    }
+    __syncthreads();
+#pragma unroll 2
+    for (int r = 0; r < P; ++r) {
+      const float4 g = *reinterpret_cast<const float4 *>(&s_dz[r][cog]);
+      float xv[9];
+#pragma unroll
+      for (int j = 0; j < 9; ++j) xv[j] = s_x[r][kg + 32 * j];
+#pragma unroll
+      for (int j = 0; j < 9; ++j) {
+        acc[0][j] = fmaf(g.x, xv[j], acc[0][j]);
+        acc[1][j] = fmaf(g.y, xv[j], acc[1][j]);
+        acc[2][j] = fmaf(g.z, xv[j], acc[2][j]);
+        acc[3][j] = fmaf(g.w, xv[j], acc[3][j]);
+      }
+      if (kg == 0) {
+        accb[0] += g.x; accb[1] += g.y; accb[2] += g.z; accb[3] += g.w;
+      }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+#pragma unroll
+    for (int j = 0; j < 9; ++j) atomicAdd(&dW[(cog + i) * K + kg + 32 * j], acc[i][j]);
+    if (kg == 0) atomicAdd(&db[cog + i], accb[i]);
+  }
 }
 
 // Head: mean pool -> linear -> sigmoid -> cross-entropy; one warp per image,
@@ -736,11 +823,13 @@ int cnn_backward(gasp_cnn *c, int batch, cudaStream_t s) {
   k_dz4<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(B, N, c->d_dmean, c->d_act[3], c->d_dz[0]);
   GASP_CUDA(cudaGetLastError());
   int cur = 0;
-  const int dw_grid = 148 * 4;
+  int dev = 0, nsm = 148;
+  GASP_CUDA(cudaGetDevice(&dev));
+  GASP_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  const int dw_grid = nsm * 3;  // k_conv_dw32: 3 resident blocks per SM (registers)
   for (int l = 3; l >= 1; --l) {  // layers 4, 3, 2 (0-based l)
     float *gW = c->d_grad + kOffW2 + (l - 1) * (9216 + 32);
-    k_conv_dw<kC><<<dw_grid, 256, 0, s>>>(c->L, B, c->d_dz[cur], c->d_act[l - 1], nullptr, gW,
-                                          gW + 9216);
+    k_conv_dw32<<<dw_grid, 256, 0, s>>>(c->L, B, c->d_dz[cur], c->d_act[l - 1], gW, gW + 9216);
     GASP_CUDA(cudaGetLastError());
     ConvArgs a;
     memset(&a, 0, sizeof a);

@@ -279,7 +279,7 @@ struct LatticeStore<Words, false> {
 // attempt's site (after this attempt's acceptance draw, as the reference's
 // stream order requires) so its conversion overlaps this attempt's
 // shared-memory round trips.
-template <int L, bool kFloatCmp, bool kLookahead, typename Rng>
+template <int L, bool kFloatCmp, bool kLookahead, bool kStoreAlways, typename Rng>
 __device__ __forceinline__ void row_attempt(uint32_t &s, Rng &rg, const char *latb,
                                             const char *thrb, const char *paccb, uint32_t lane4,
                                             float shrink) {
@@ -323,7 +323,12 @@ __device__ __forceinline__ void row_attempt(uint32_t &s, Rng &rg, const char *la
   } else {
     acc = x2 <= *reinterpret_cast<const uint32_t *>(thrb + p4);
   }
-  if (acc) *reinterpret_cast<uint32_t *>(const_cast<char *>(latb) + offc) = wc ^ (1u << (sc & 31u));
+  uint32_t *dst = reinterpret_cast<uint32_t *>(const_cast<char *>(latb) + offc);
+  if constexpr (kStoreAlways) {
+    *dst = acc ? wc ^ (1u << (sc & 31u)) : wc;  // rejected: the word written back unchanged
+  } else {
+    if (acc) *dst = wc ^ (1u << (sc & 31u));
+  }
 }
 
 // row_attempt with the threshold lookup taken off the dependency chain.  For
@@ -535,7 +540,8 @@ __global__ void __launch_bounds__(32) k_sweep_rows_pair(SweepLaunch p) {
   stage_out(lat, p, W, tile, lane, live, rep);
 }
 
-template <int L, bool kStatic, bool kFloatCmp, int kRng, bool kMask = false>
+template <int L, bool kStatic, bool kFloatCmp, int kRng, bool kMask = false,
+          bool kStoreAlways = false>
 __global__ void __launch_bounds__(32) k_sweep_rows(SweepLaunch p) {
   static_assert(L % 32 == 0 && (L & (L - 1)) == 0, "L must be a power of two >= 32");
   static_assert(!(kMask && kFloatCmp), "the acceptance mask needs integer thresholds");
@@ -612,8 +618,8 @@ __global__ void __launch_bounds__(32) k_sweep_rows(SweepLaunch p) {
     } else {
 #pragma unroll 5
       for (int a = 0; a < total - 1; ++a)
-        row_attempt<L, kFloatCmp, true>(s, rg, latb, thrb, paccb, lane4, shrink);
-      row_attempt<L, kFloatCmp, false>(s, rg, latb, thrb, paccb, lane4, shrink);
+        row_attempt<L, kFloatCmp, true, kStoreAlways>(s, rg, latb, thrb, paccb, lane4, shrink);
+      row_attempt<L, kFloatCmp, false, kStoreAlways>(s, rg, latb, thrb, paccb, lane4, shrink);
     }
     rg.store(p.rng, p.rng_stride, rep);
   }
@@ -829,7 +835,15 @@ int dispatch_kind(const SweepLaunch &p, cudaStream_t s) {
       default: break;
     }
   }
-  switch (p.L) {  // variants 0 and 2: the software-pipelined row kernel
+  if (p.variant == 0) {  // the row kernel writing the centre word back on every attempt
+    switch (p.L) {
+      case 32: return launch_rows(k_sweep_rows<32, true, F, K, false, true>, p, 0, s);
+      case 64: return launch_rows(k_sweep_rows<64, true, F, K, false, true>, p, 0, s);
+      case 128: return launch_rows(k_sweep_rows<128, false, F, K, false, true>, p, dyn128, s);
+      default: break;
+    }
+  }
+  switch (p.L) {  // variant 2 (and other L): the software-pipelined row kernel
     case 16: return launch_tiles(k_sweep_exact<16, F, K>, p, s);
     case 32: return launch_rows(k_sweep_rows<32, true, F, K>, p, 0, s);
     case 48: return launch_tiles(k_sweep_exact<48, F, K>, p, s);

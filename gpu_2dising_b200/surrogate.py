@@ -236,7 +236,7 @@ def screen(cnn, grids, beta, h, fallback_shots=128, band=0.1, **shoot_kw):
 
 def run_experiment(n_train=20000, train_shots=256, n_test=2000, test_shots=1024,
                    n_screen=100000, baseline_shots=64, epochs=40, batch=1024, lr=2e-3, beta=0.54,
-                   h=0.07, seed=0, log=None, short_cap=4000):
+                   h=0.07, seed=0, log=None):
     """Train the surrogate on shooting labels and measure what it gains.
 
     Returns a dict with the held-out MAE (surrogate alone and screened with
@@ -281,13 +281,20 @@ def run_experiment(n_train=20000, train_shots=256, n_test=2000, test_shots=1024,
     net.predict(sc)
     t_cnn = time.perf_counter() - t0
     arms = {}
-    for cap in (20000, short_cap):
-        st_fb, st_sh = {}, {}
-        _, near_sc, t_scr = screen(net, sc, beta, h, fallback_shots=baseline_shots,
-                                   seed=seed + 23, cap=cap, stats=st_fb)
+    for cap in (20000,):
+        # The screened arm's time is set by its slowest fallback trajectories,
+        # so it is taken three times (fresh shooting seeds) and the median kept.
+        st_fb, st_sh, t_scr = {}, {}, []
+        for rep in range(3):
+            _, near_sc, ts = screen(net, sc, beta, h, fallback_shots=baseline_shots,
+                                    seed=seed + 23 + 101 * rep, cap=cap, stats=st_fb)
+            t_scr.append(ts)
+        t_scr_med = float(np.median(t_scr))
         _, a_sh, t_sh = shoot(sc, baseline_shots, beta, h, seed=seed + 29, cap=cap, stats=st_sh)
-        arms[cap] = {"screen_s": t_scr, "shoot_s": t_sh, "speedup": t_sh / t_scr,
-                     "screen_grids_per_s": sc.shape[0] / t_scr,
+        arms[cap] = {"screen_s": t_scr_med, "screen_s_runs": t_scr, "shoot_s": t_sh,
+                     "speedup": t_sh / t_scr_med,
+                     "speedup_range": [t_sh / max(t_scr), t_sh / min(t_scr)],
+                     "screen_grids_per_s": sc.shape[0] / t_scr_med,
                      "shoot_grids_per_s": sc.shape[0] / t_sh,
                      "fallback_unresolved": st_fb.get("unresolved", 0),
                      "shoot_unresolved": st_sh.get("unresolved", 0),
