@@ -192,7 +192,8 @@ __global__ void __launch_bounds__(256) k_sweep_exact(SweepLaunch p) {
         } else {
           acc = x2 <= thr_s[cls];
         }
-        if (acc) my[(s >> 5) * kTile] = wc ^ (1u << (s & 31));
+        // written back on every attempt (unchanged when rejected): no divergent branch
+        my[(s >> 5) * kTile] = acc ? wc ^ (1u << (s & 31)) : wc;
       }
     }
     rg.store(p.rng, p.rng_stride, rep);

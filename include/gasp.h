@@ -111,8 +111,10 @@ int gasp_grids_upload_inputs_noalloc(gasp_grids_t *grids, const int *inputs, int
 int gasp_grids_shape(const gasp_grids_t *grids, int *L_out, int *ngrids_out);
 
 /* Launch tuning of a set (no reference counterpart; results never depend on
- * it).  GASP_OPT_SWEEP_VARIANT: 0 the fastest kernel for L (default), 1 the
- * generic kernel, 2 the row kernel, 3 the row kernel with pairwise
+ * it).  GASP_OPT_SWEEP_VARIANT: 0 the fastest kernel for L (default: for
+ * L = 32, 64, 128 the row kernel writing the centre word back on every
+ * attempt, no divergent branch), 1 the generic kernel, 2 the row kernel with a
+ * store only on acceptance, 3 the row kernel with pairwise
  * speculation of consecutive attempts, 4 the row kernel with the acceptance
  * decided by a per-draw mask of accepted neighbourhoods (falls back to 2 when
  * more than six classes can reject).  GASP_OPT_WARPS_PER_CTA: tiles per
