@@ -377,7 +377,7 @@ int gasp_grids_download(gasp_grids_t *g, int *host_grids) {
 int gasp_grids_set_option(gasp_grids_t *g, int option, int value) {
   if (!g) return GASP_ERR_INVALID;
   GridsExtra &x = impl(g)->x;
-  if (option == GASP_OPT_SWEEP_VARIANT && value >= 0 && value <= 4) {
+  if (option == GASP_OPT_SWEEP_VARIANT && value >= 0 && value <= 5) {
     x.variant = value;
     return GASP_OK;
   }
@@ -868,10 +868,10 @@ int committor_on_device(gasp_grids_t *g, gasp_rng_t *r, int tot, int mag_int, in
   int *d_fates = static_cast<int *>(fates_b.p);
   int *d_n = static_cast<int *>(small_b.p);
   long long *d_att = reinterpret_cast<long long *>(static_cast<char *>(small_b.p) + 8);
-  PinnedBuf hact_b, hpoll_b;
-  GASP_CUDA(cudaMallocHost(&hact_b.p, (size_t)ngrids * sizeof(int)));
+  PinnedBuf hpoll_b;  // read behind events while the host runs ahead: pinned
   GASP_CUDA(cudaMallocHost(&hpoll_b.p, 64 * sizeof(int)));
-  int *hact = static_cast<int *>(hact_b.p);
+  std::vector<int> hact_v((size_t)ngrids);
+  int *hact = hact_v.data();
   volatile int *hpoll = static_cast<volatile int *>(hpoll_b.p);
   int n0 = 0;
   for (int i = 0; i < ngrids; ++i)
@@ -1049,27 +1049,26 @@ extern "C" int gasp_mc_driver_gpu_ex(gasp_gpu_grids_t grids, double beta, double
   if (!x.d_mag2) GASP_CUDA(cudaMalloc(&x.d_mag2, (size_t)g->ntiles * kTile * sizeof(float)));
   if (compact && !x.d_active) GASP_CUDA(cudaMalloc(&x.d_active, (size_t)ngrids * sizeof(int)));
   if (dumps && (rc = ensure_frame(g))) return rc;
-  PinnedBuf hmag_b, hframe_b, hact_b, hlclus_b;
-  GASP_CUDA(cudaMallocHost(&hmag_b.p, (size_t)ngrids * sizeof(float)));
-  float *hmag = static_cast<float *>(hmag_b.p);
+  // Host staging is pageable: the loop waits on every read-back anyway, and
+  // page-locking (16 MiB for a frame at L=64 x 32768) can cost more than the
+  // copies it would speed up.
+  std::vector<float> hmag_v((size_t)ngrids);
+  float *hmag = hmag_v.data();
   std::vector<float> mag_last((size_t)ngrids, 0.0f);
   // Collective variable compared with the thresholds: the magnetisation or
   // the largest cluster of spins opposite to initial_spin (src/mc_gpu.cu:586-605).
   std::vector<float> lclus_last(use_lclus ? (size_t)ngrids : 0, 0.0f);
-  float *hlclus = nullptr;
-  if (use_lclus) {
-    GASP_CUDA(cudaMallocHost(&hlclus_b.p, (size_t)ngrids * sizeof(float)));
-    hlclus = static_cast<float *>(hlclus_b.p);
-  }
+  std::vector<float> hlclus_v(use_lclus ? (size_t)ngrids : 0);
+  float *hlclus = use_lclus ? hlclus_v.data() : nullptr;
   const float *colvar = use_lclus ? lclus_last.data() : mag_last.data();
   auto take_check = [&]() {
     memcpy(mag_last.data(), hmag, (size_t)ngrids * sizeof(float));
     if (use_lclus) memcpy(lclus_last.data(), hlclus, (size_t)ngrids * sizeof(float));
   };
-  if (dumps) GASP_CUDA(cudaMallocHost(&hframe_b.p, g->frame_bytes));
-  if (compact) GASP_CUDA(cudaMallocHost(&hact_b.p, (size_t)ngrids * sizeof(int)));
-  uint8_t *hframe = static_cast<uint8_t *>(hframe_b.p);
-  int *hact = static_cast<int *>(hact_b.p);
+  std::vector<uint8_t> hframe_v(dumps ? g->frame_bytes : 0);
+  std::vector<int> hact_v(compact ? (size_t)ngrids : 0);
+  uint8_t *hframe = dumps ? hframe_v.data() : nullptr;
+  int *hact = compact ? hact_v.data() : nullptr;
 
   float *d_mag_cur = g->d_mag, *d_mag_next = x.d_mag2;
   SweepLaunch p = base_launch(g);

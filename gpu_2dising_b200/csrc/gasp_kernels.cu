@@ -141,7 +141,7 @@ __device__ __forceinline__ void epilogue_mag(const uint32_t *my, const SweepLaun
 // ---------------------------------------------------------------------------
 // Exact sweep.  L_ > 0: compile-time side length; L_ == 0: runtime p.L.
 // ---------------------------------------------------------------------------
-template <int L_, bool kFloatCmp, int kRng>
+template <int L_, bool kFloatCmp, int kRng, bool kStoreAlways = false>
 __global__ void __launch_bounds__(256) k_sweep_exact(SweepLaunch p) {
   const int L = L_ > 0 ? L_ : p.L;
   const int N = L * L;
@@ -192,8 +192,11 @@ __global__ void __launch_bounds__(256) k_sweep_exact(SweepLaunch p) {
         } else {
           acc = x2 <= thr_s[cls];
         }
-        // written back on every attempt (unchanged when rejected): no divergent branch
-        my[(s >> 5) * kTile] = acc ? wc ^ (1u << (s & 31)) : wc;
+        if constexpr (kStoreAlways) {  // written back unchanged when rejected: no branch
+          my[(s >> 5) * kTile] = acc ? wc ^ (1u << (s & 31)) : wc;
+        } else {
+          if (acc) my[(s >> 5) * kTile] = wc ^ (1u << (s & 31));
+        }
       }
     }
     rg.store(p.rng, p.rng_stride, rep);
@@ -847,9 +850,11 @@ int dispatch_kind(const SweepLaunch &p, cudaStream_t s) {
   switch (p.L) {  // variant 2 (and other L): the software-pipelined row kernel
     case 16: return launch_tiles(k_sweep_exact<16, F, K>, p, s);
     case 32: return launch_rows(k_sweep_rows<32, true, F, K>, p, 0, s);
-    case 48: return launch_tiles(k_sweep_exact<48, F, K>, p, s);
+    case 48: return p.variant == 5 ? launch_tiles(k_sweep_exact<48, F, K, true>, p, s)
+                                   : launch_tiles(k_sweep_exact<48, F, K>, p, s);
     case 64: return launch_rows(k_sweep_rows<64, true, F, K>, p, 0, s);
-    case 96: return launch_tiles(k_sweep_exact<96, F, K>, p, s);
+    case 96: return p.variant == 5 ? launch_tiles(k_sweep_exact<96, F, K, true>, p, s)
+                                   : launch_tiles(k_sweep_exact<96, F, K>, p, s);
     case 128: return launch_rows(k_sweep_rows<128, false, F, K>, p, dyn128, s);
     default: return launch_tiles(k_sweep_exact<0, F, K>, p, s);
   }

@@ -117,7 +117,8 @@ int gasp_grids_shape(const gasp_grids_t *grids, int *L_out, int *ngrids_out);
  * store only on acceptance, 3 the row kernel with pairwise
  * speculation of consecutive attempts, 4 the row kernel with the acceptance
  * decided by a per-draw mask of accepted neighbourhoods (falls back to 2 when
- * more than six classes can reject).  GASP_OPT_WARPS_PER_CTA: tiles per
+ * more than six classes can reject), 5 the generic kernel (L other than 32,
+ * 64, 128) writing the centre word back on every attempt.  GASP_OPT_WARPS_PER_CTA: tiles per
  * CTA of the generic kernel (1..8). */
 enum { GASP_OPT_SWEEP_VARIANT = 1, GASP_OPT_WARPS_PER_CTA = 2 };
 int gasp_grids_set_option(gasp_grids_t *grids, int option, int value);
