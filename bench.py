@@ -437,6 +437,35 @@ def run_cnn(args):
     print(json.dumps(line), flush=True)
 
 
+def run_cluster(args):
+    """Largest-cluster collective variable on the device: gasp_largest_cluster
+    over 32768 L=64 grids, near the site-percolation threshold (p = 0.593,
+    the largest and most tangled clusters) and sparse (2 % of sites up, like a
+    metastable swarm)."""
+    from gpu_2dising_b200 import engine
+    engine.init_device(0)
+    rs = np.random.default_rng(SEED)
+    out = {}
+    for name, grids in (("percolating p=0.593", np.where(rs.random((R, L, L)) < 0.593, 1, -1)),
+                        ("all -1 with 2% flips", np.where(rs.random((R, L, L)) < 0.02, 1, -1))):
+        dg = engine.DeviceGrids(L, R, grids.astype(np.int32))
+        for _ in range(args.warmup):
+            dg.largest_cluster(1)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            dg.largest_cluster(1)
+        dt = (time.perf_counter() - t0) / args.steps
+        out[name] = {"grids_per_s": R / dt, "ms_per_call": 1e3 * dt}
+        dg.close()
+    line = {"metric": "largest-cluster evaluations (grids/s)",
+            "value": out["percolating p=0.593"]["grids_per_s"], "unit": "grids/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "cases": out,
+            "config": {"workload": f"gasp_largest_cluster(spin=+1) on {R} L=64 grids, "
+                                   "including the device->host copy of the sizes"}}
+    print(json.dumps(line), flush=True)
+
+
 def run_rate(args):
     """The full production swarm of the headline workload (L=64, 32768
     replicas, beta=0.54, h=0.07, 50 000 sweeps, checks every 100, dumps every
@@ -511,7 +540,8 @@ def main():
                     help="smaller values give a short launch for ncu captures")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--workload", default="swarm",
-                    choices=["swarm", "batched", "committor", "surrogate", "cnn", "rate"],
+                    choices=["swarm", "batched", "committor", "surrogate", "cnn", "rate",
+                             "cluster"],
                     help="swarm: the headline single-group swarm; batched: uneven groups; "
                          "committor: seeded droplet shooting")
     ap.add_argument("--cnn-grids", type=int, default=100000)
@@ -552,6 +582,9 @@ def main():
     elif args.workload == "rate":
         if rank == 0:
             run_rate(args)
+    elif args.workload == "cluster":
+        if rank == 0:
+            run_cluster(args)
     else:
         run_ours(args, rank, world, local_rank)
 
