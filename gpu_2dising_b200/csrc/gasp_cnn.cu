@@ -4,14 +4,15 @@
 //
 // Convolutions (forward, and the data gradient of the backward pass) are
 // implicit GEMMs on the 5th-generation tensor cores: per CTA a 128-pixel tile,
-// D[128 x 32] (FP32, in TMEM) = A[128 x K] (im2col, BF16) * B[32 x K]^T
-// (weights, BF16), K = 9 taps * 32 channels = 288 (16 for the first layer).
-// Both operands are staged K-major in shared memory in the no-swizzle
-// interleaved layout (8x8 core matrices, leading-byte offset 128 B between
-// k-chunks, stride-byte offset K*16 B between 8-row groups); one thread
-// issues K/16 tcgen05.mma (kind::f16, M=128, N=32), a tcgen05.commit arrives
-// on an mbarrier, and every warp reads its 32 rows of D with tcgen05.ld.
-// Weight gradients are FP32 reductions over pixels on the CUDA cores.
+// D[128 x 32] (FP32, in TMEM) = A[128 x K] (BF16) * B[32 x K]^T (weights,
+// BF16), K = 9 taps * 32 channels = 288 (16 for the first layer).  A is an
+// im2col buffer (k_conv_tc) or, for the 32-channel layers, shifted windows
+// over the tile's staged input rows (k_conv_win).  Operands are K-major in
+// shared memory in the no-swizzle interleaved layout (8-row x 16-byte core
+// matrices); one thread issues K/16 tcgen05.mma (kind::f16, M=128, N=32), a
+// tcgen05.commit arrives on an mbarrier, and every warp reads its 32 rows of D
+// with tcgen05.ld.  Weight gradients are FP32 reductions over pixels on the
+// CUDA cores.
 //
 // Activations: BF16, [image][pixel][32 channels] (pixel = row*L + col).
 #include <cuda_bf16.h>
@@ -369,16 +370,20 @@ __global__ void __launch_bounds__(128) k_conv_win(ConvArgs a) {
       uint4 v4[kPer];
 #pragma unroll
       for (int j = 0; j < kPer; ++j) {
-        const int idx = j * 128 + tid;
-        const int c = idx & 3, w = idx >> 2;
+        // a quarter-warp (8 lanes) takes one 16-byte channel chunk of 8
+        // consecutive pixels: each rotated-copy store is one 128-byte row per
+        // quarter-warp (no bank conflict); the warp still reads 512 contiguous bytes
+        const int c = (tid & 31) >> 3, w = j * 32 + (tid >> 5) * 8 + (tid & 7);
         int row = y0 - 1 + w / LR;
         row = row < 0 ? row + LR : (row >= LR ? row - LR : row);
         v4[j] = *reinterpret_cast<const uint4 *>(x + ((size_t)row * LR + (w % LR)) * kC + 8 * c);
       }
 #pragma unroll
       for (int j = 0; j < kPer; ++j) {
-        const int idx = j * 128 + tid;
-        const int c = idx & 3, w = idx >> 2;
+        // a quarter-warp (8 lanes) takes one 16-byte channel chunk of 8
+        // consecutive pixels: each rotated-copy store is one 128-byte row per
+        // quarter-warp (no bank conflict); the warp still reads 512 contiguous bytes
+        const int c = (tid & 31) >> 3, w = j * 32 + (tid >> 5) * 8 + (tid & 7);
         const int col = w % LR, rbase = w - col;
 #pragma unroll
         for (int v = 0; v < 3; ++v) {  // copy v holds, at column col', input column col' + v - 1
