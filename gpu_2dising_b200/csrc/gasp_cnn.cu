@@ -354,6 +354,30 @@ __global__ void __launch_bounds__(128) k_conv_win(ConvArgs a) {
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t taddr = *tslot;
 
+  // LT > 0: a tile's window is loaded into registers one tile ahead, so the
+  // global loads of tile i+1 are in flight during the MMA and epilogue of i.
+  constexpr int LR0 = LT > 0 ? LT : 1;
+  constexpr int kPerW = (kTileM + 2 * LR0) * 4 / 128;  // 16-byte chunks per thread
+  uint4 v4[kPerW];
+  auto load_window = [&](int t) {
+    const int timg = t / tiles_per_img;
+    const int y0 = ((t % tiles_per_img) * kTileM) / LR0;  // first output row of the tile
+    const __nv_bfloat16 *xs = a.x + (size_t)timg * N * kC;
+#pragma unroll
+    for (int j = 0; j < kPerW; ++j) {
+      // a quarter-warp (8 lanes) takes one 16-byte channel chunk of 8
+      // consecutive pixels: each rotated-copy store is one 128-byte row per
+      // quarter-warp (no bank conflict); the warp still reads 512 contiguous bytes
+      const int c = (tid & 31) >> 3, w = j * 32 + (tid >> 5) * 8 + (tid & 7);
+      int row = y0 - 1 + w / LR0;
+      row = row < 0 ? row + LR0 : (row >= LR0 ? row - LR0 : row);
+      v4[j] = *reinterpret_cast<const uint4 *>(xs + ((size_t)row * LR0 + (w % LR0)) * kC + 8 * c);
+    }
+  };
+  if constexpr (LT > 0) {
+    if ((int)blockIdx.x < a.ntiles) load_window(blockIdx.x);
+  }
+
   uint32_t phase = 0;
   for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
     const int img = tile / tiles_per_img;
@@ -363,31 +387,13 @@ __global__ void __launch_bounds__(128) k_conv_win(ConvArgs a) {
 
     // ---- stage the three rotated windows (16-byte chunks, channel chunk fastest) ----
     if constexpr (LT > 0) {
-      constexpr int LR = LT > 0 ? LT : 1;         // LT (never 0 on this branch)
-      constexpr int kWin = kTileM + 2 * LR;       // window pixels: kTileM / LT + 2 whole rows
-      constexpr int kPer = kWin * 4 / 128;        // chunks per thread
-      const int y0 = p0 / LR;                     // first output row of the tile
-      uint4 v4[kPer];
 #pragma unroll
-      for (int j = 0; j < kPer; ++j) {
-        // a quarter-warp (8 lanes) takes one 16-byte channel chunk of 8
-        // consecutive pixels: each rotated-copy store is one 128-byte row per
-        // quarter-warp (no bank conflict); the warp still reads 512 contiguous bytes
+      for (int j = 0; j < kPerW; ++j) {  // the registers hold this tile's window
         const int c = (tid & 31) >> 3, w = j * 32 + (tid >> 5) * 8 + (tid & 7);
-        int row = y0 - 1 + w / LR;
-        row = row < 0 ? row + LR : (row >= LR ? row - LR : row);
-        v4[j] = *reinterpret_cast<const uint4 *>(x + ((size_t)row * LR + (w % LR)) * kC + 8 * c);
-      }
-#pragma unroll
-      for (int j = 0; j < kPer; ++j) {
-        // a quarter-warp (8 lanes) takes one 16-byte channel chunk of 8
-        // consecutive pixels: each rotated-copy store is one 128-byte row per
-        // quarter-warp (no bank conflict); the warp still reads 512 contiguous bytes
-        const int c = (tid & 31) >> 3, w = j * 32 + (tid >> 5) * 8 + (tid & 7);
-        const int col = w % LR, rbase = w - col;
+        const int col = w % LR0, rbase = w - col;
 #pragma unroll
         for (int v = 0; v < 3; ++v) {  // copy v holds, at column col', input column col' + v - 1
-          const int cd = (col - (v - 1) + LR) % LR;
+          const int cd = (col - (v - 1) + LR0) % LR0;
           *reinterpret_cast<uint4 *>(sA + v * vstride + c * lbo + (uint32_t)(rbase + cd) * 16) =
               v4[j];
         }
@@ -427,6 +433,10 @@ __global__ void __launch_bounds__(128) k_conv_win(ConvArgs a) {
                     (tap | j) ? 1u : 0u);
       }
       umma_commit(smem_u32(mbar));
+    }
+    if constexpr (LT > 0) {  // the next tile's loads overlap this tile's MMA and epilogue
+      const int nt = tile + (int)gridDim.x;
+      if (nt < a.ntiles) load_window(nt);
     }
     // One thread polls the MMA barrier; the CTA barrier passes the result on
     // (127 spinning threads would keep the shared-memory pipe busy).

@@ -303,8 +303,13 @@ __device__ __forceinline__ void row_attempt(uint32_t &s, Rng &rg, const char *la
   } else if constexpr (R == 2) {
     wc = *reinterpret_cast<const uint32_t *>(latb + offc);
     const uint32_t wx = *reinterpret_cast<const uint32_t *>(latb + (offc ^ 128u));
-    lo = (b == 0u) ? wx : wc;
-    hi = (b == 31u) ? wx : wc;
+    // The row is the circular 64 bits (wx:wc) seen from the site's word: for
+    // b >= 3 the bits b-1..b+1 sit in (wx:wc) >> (b-3) (b = 31 reaches wx bit
+    // 0); for b < 3 the left neighbour wraps to the top of wx, so the pair is
+    // read as (wc:wx), whose shift by b+29 lands on the same bits.
+    const bool wrap = b < 3u;
+    lo = wrap ? wx : wc;
+    hi = wrap ? wc : wx;
   } else {
     const uint32_t wi = (offc >> 7) & (uint32_t)(R - 1);
     const uint32_t offl = (b == 0u) ? (wi == 0u ? offc + 128u * (R - 1) : offc - 128u) : offc;
