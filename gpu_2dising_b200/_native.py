@@ -27,6 +27,7 @@ GASP_ERR_TIMEOUT = 9
 
 OPT_SWEEP_VARIANT = 1
 OPT_WARPS_PER_CTA = 2
+OPT_TAIL_REPLICAS = 3
 
 BATCH_PLAIN = 0
 BATCH_GRAPH = 1
@@ -44,7 +45,8 @@ EXPORTED = (
     "gasp_set_stream", "gasp_init_grid", "gasp_free_grid", "gasp_grids_upload",
     "gasp_grids_download", "gasp_grids_upload_inputs",
     "gasp_grids_upload_inputs_noalloc", "gasp_grids_shape", "gasp_grids_set_option", "gasp_init_rand",
-    "gasp_init_rand_mode", "gasp_mwc64x_seed_states", "gasp_free_rand",
+    "gasp_init_rand_mode", "gasp_mwc64x_seed_states", "gasp_acceptance_thresholds",
+    "gasp_mwc64x_lane_multipliers", "gasp_rng_read_states", "gasp_free_rand",
     "gasp_sweep", "gasp_sweep_trace_cpu", "gasp_magnetisation", "gasp_largest_cluster", "gasp_pack_frame",
     "gasp_frame_bytes", "gasp_mc_driver_gpu", "gasp_mc_driver_gpu_ex",
     "gasp_init_grids_uniform", "gasp_init_grids_from_file", "gasp_init_grids_from_array",
@@ -139,6 +141,13 @@ def _bind(lib):
         "gasp_init_rand_mode": (I, [I, I, C.c_ulonglong, I, C.POINTER(P)]),
         "gasp_mwc64x_seed_states": (I, [C.c_ulonglong, I, I,
                                         np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")]),
+        "gasp_acceptance_thresholds": (I, [P, C.c_double, C.c_double,
+                                           np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS"),
+                                           C.POINTER(I)]),
+        "gasp_mwc64x_lane_multipliers": (I, [np.ctypeslib.ndpointer(np.uint64, flags="C_CONTIGUOUS"),
+                                             np.ctypeslib.ndpointer(np.uint64, flags="C_CONTIGUOUS")]),
+        "gasp_rng_read_states": (I, [P, np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS"),
+                                     C.c_longlong]),
         "gasp_free_rand": (I, [P]),
         "gasp_sweep": (I, [P, P, C.c_double, C.c_double, I, I]),
         "gasp_sweep_trace_cpu": (I, [P, _f64p, C.c_double, C.c_double, I]),

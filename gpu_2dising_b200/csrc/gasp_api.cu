@@ -52,6 +52,10 @@ struct TableBlock {
   int flags[4];
 };
 
+// Committor shooting on the MWC64X stream switches to the one-warp-per-replica
+// sweep once at most this many replicas are undecided (GASP_OPT_TAIL_REPLICAS).
+constexpr int kTailReplicasDefault = 4096;
+
 struct GridsExtra {
   TableBlock *d_tab = nullptr;
   double beta = NAN, h = NAN;
@@ -66,6 +70,7 @@ struct GridsExtra {
   int mask_ok = 0;          // <= 6 classes with P <= 1 (see k_sweep_rows<kMask>)
   int variant = 0;          // GASP_OPT_SWEEP_VARIANT
   int warps_per_cta = 1;    // GASP_OPT_WARPS_PER_CTA
+  int tail_replicas = kTailReplicasDefault;  // GASP_OPT_TAIL_REPLICAS
 };
 
 // Extra state kept beside the public struct (allocated with it).
@@ -377,12 +382,16 @@ int gasp_grids_download(gasp_grids_t *g, int *host_grids) {
 int gasp_grids_set_option(gasp_grids_t *g, int option, int value) {
   if (!g) return GASP_ERR_INVALID;
   GridsExtra &x = impl(g)->x;
-  if (option == GASP_OPT_SWEEP_VARIANT && value >= 0 && value <= 5) {
+  if (option == GASP_OPT_SWEEP_VARIANT && value >= 0 && value <= 6) {
     x.variant = value;
     return GASP_OK;
   }
   if (option == GASP_OPT_WARPS_PER_CTA && value >= 1 && value <= 8) {
     x.warps_per_cta = value;
+    return GASP_OK;
+  }
+  if (option == GASP_OPT_TAIL_REPLICAS && value >= 0) {
+    x.tail_replicas = value;
     return GASP_OK;
   }
   set_error("unknown option %d or bad value %d", option, value);
@@ -445,6 +454,21 @@ void mwc_seed_states(uint64_t seed, int ngrids, int stride, std::vector<uint32_t
 
 }  // namespace
 
+const TailParams &gasp::mwc_lane_params() {
+  static const TailParams t = [] {
+    TailParams q;
+    const uint64_t A = kMwcA;
+    const uint64_t M = (A << 32) - 1;
+    const uint64_t Ainv = 1ull << 32;  // A * 2^32 = M + 1
+    for (int j = 0; j < 32; ++j) {
+      q.mul[j] = powmod64(A, (uint64_t)j << 35, M);
+      q.inv[j] = powmod64(Ainv, (uint64_t)j << 35, M);
+    }
+    return q;
+  }();
+  return t;
+}
+
 extern "C" {
 
 int gasp_init_rand_mode(int ngrids, int threads_per_block, unsigned long long seed, int kind,
@@ -489,6 +513,44 @@ int gasp_init_rand_mode(int ngrids, int threads_per_block, unsigned long long se
     return rc;
   }
   *rng_out = r;
+  return GASP_OK;
+}
+
+int gasp_acceptance_thresholds(gasp_grids_t *g, double beta, double h, uint32_t *thr10,
+                               int *float_compare) {
+  if (!g || !thr10) return GASP_ERR_INVALID;
+  int rc = check_device_of(g->device);
+  if (rc) return rc;
+  if ((rc = ensure_tables(g, beta, h))) return rc;
+  GridsExtra &x = impl(g)->x;
+  cudaStream_t s = current_stream();
+  GASP_CUDA(cudaMemcpyAsync(thr10, x.d_tab->thr, 10 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  GASP_CUDA(cudaStreamSynchronize(s));
+  if (float_compare) *float_compare = x.float_cmp;
+  return GASP_OK;
+}
+
+int gasp_mwc64x_lane_multipliers(uint64_t *mul32, uint64_t *inv32) {
+  if (!mul32 || !inv32) return GASP_ERR_INVALID;
+  const TailParams &t = mwc_lane_params();
+  memcpy(mul32, t.mul, sizeof t.mul);
+  memcpy(inv32, t.inv, sizeof t.inv);
+  return GASP_OK;
+}
+
+int gasp_rng_read_states(const gasp_rng_t *r, uint32_t *out, long long nwords) {
+  if (!r || !out) return GASP_ERR_INVALID;
+  const long long need = (long long)(r->kind == kRngMwc ? kMwcWords : kRngWords) * r->stride;
+  if (nwords < need) {
+    set_error("gasp_rng_read_states: %lld words needed, %lld given", need, nwords);
+    return GASP_ERR_INVALID;
+  }
+  int rc = check_device_of(r->device);
+  if (rc) return rc;
+  cudaStream_t s = current_stream();
+  GASP_CUDA(cudaMemcpyAsync(out, r->d_state, (size_t)need * sizeof(uint32_t),
+                            cudaMemcpyDeviceToHost, s));
+  GASP_CUDA(cudaStreamSynchronize(s));
   return GASP_OK;
 }
 
@@ -916,6 +978,18 @@ int committor_on_device(gasp_grids_t *g, gasp_rng_t *r, int tot, int mag_int, in
   long long polls_issued = 0, polls_seen = 0;
   bool done = n0 == 0;
   int checks = 0;
+  // Once few replicas are undecided, each gets a warp of its own
+  // (k_sweep_tail, production stream only).  Both kernels are enqueued every
+  // interval and each checks the device count, so the switch happens at the
+  // same interval whatever the host's timing.
+  const bool tail_ok = r->kind == kRngMwc && x.tail_replicas > 0 && !g->global_lattice &&
+                       g->L >= 3 && g->L <= kTailMaxL;
+  SweepLaunch q = p;
+  if (tail_ok) {
+    p.tail_split = q.tail_split = x.tail_replicas;
+    q.variant = 6;
+    q.n_active = x.tail_replicas < ngrids ? x.tail_replicas : ngrids;
+  }
   for (int isweep = 0; isweep < tot && !done; isweep += spc) {
     if (isweep % mag_int == 0) {
       // sweeps from this check to the next one (or to the end of the run)
@@ -933,6 +1007,7 @@ int committor_on_device(gasp_grids_t *g, gasp_rng_t *r, int tot, int mag_int, in
       }
     }
     if ((rc = launch_sweep_exact(p, s))) return rc;
+    if (tail_ok && (rc = launch_sweep_exact(q, s))) return rc;
     // look at finished polls; wait only when too far ahead
     while (polls_seen < polls_issued) {
       const int slot = (int)(polls_seen % kRing);

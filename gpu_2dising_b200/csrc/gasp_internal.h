@@ -35,6 +35,17 @@ constexpr uint32_t kMwcA = 4294883355u;
 constexpr int kMwcWords = 2;  // SoA: x at [0*stride + r], c at [1*stride + r]
 enum RngKind { kRngXorwow = 0, kRngMwc = 1 };
 
+// Lane substreams of the one-warp-per-replica sweep (gasp_tail.cu): lane j
+// starts at the replica's state X times mul[j] = A^(j * 2^35) mod M; a lane's
+// end state times inv[j] = A^-(j * 2^35) mod M maps back to the replica's own
+// stream.  Built once on the host (gasp_api.cu).
+struct TailParams {
+  uint64_t mul[32];
+  uint64_t inv[32];
+};
+const TailParams &mwc_lane_params();
+constexpr int kTailMaxL = 512;  // shared lattice + bitmap: 2 * W words per warp
+
 void set_error(const char *fmt, ...);
 int cuda_fail(cudaError_t e, const char *what, const char *file, int line);
 
@@ -76,6 +87,10 @@ struct SweepLaunch {
   const int *n_active_dev;// optional device count overriding n_active (graph replays)
   int lattice_in_global;  // L beyond shared memory: sweep the lattice in place in HBM
   int mask_ok;            // at most 6 classes can reject (the acceptance-mask row kernel applies)
+  int tail_split;         // > 0: with n live replicas, the one-warp-per-replica kernel runs
+                          // only when n <= tail_split and the other kernels only when
+                          // n > tail_split (both are enqueued; the choice is made on the
+                          // device, so runs do not depend on host timing)
 };
 
 // Sweep parameters of a replica set + RNG whose tables are ready
@@ -99,6 +114,9 @@ int launch_rng_init(uint32_t *rng, int ngrids, int stride, unsigned long long se
 int launch_build_thresholds(const float *d_pacc20, uint32_t *d_thr10, int *d_flags, cudaStream_t s);
 int launch_sweep_exact(const SweepLaunch &p, cudaStream_t s);
 int launch_sweep_trace_cpu(const SweepLaunch &p, cudaStream_t s);
+// One warp per replica, MWC64X stream only (gasp_tail.cu); p.n_active is the
+// launch shape (an upper bound of *p.n_active_dev when that is set).
+int launch_sweep_tail(const SweepLaunch &p, cudaStream_t s);
 int launch_measure(const uint32_t *lat, int L, int ngrids, float *mag, cudaStream_t s);
 int launch_pack_grids(const int *grids32, uint32_t *lat, int L, int ngrids, cudaStream_t s,
                       int per_input = 0);

@@ -103,6 +103,13 @@ struct RngPolicy<kRngMwc> {
   }
 };
 
+// Replicas to sweep: the device count when there is one, zero when a
+// one-warp-per-replica launch takes over at this count (p.tail_split).
+__device__ __forceinline__ int live_count(const SweepLaunch &p) {
+  const int n = p.n_active_dev ? *p.n_active_dev : p.n_active;
+  return p.tail_split > 0 && n <= p.tail_split ? 0 : n;
+}
+
 // Shared-memory staging of one tile (identity order) or of 32 listed replicas.
 __device__ __forceinline__ void stage_in(uint32_t *lat_s, const SweepLaunch &p, int W,
                                          int tile, int lane, bool live, int rep) {
@@ -158,7 +165,7 @@ __global__ void __launch_bounds__(256) k_sweep_exact(SweepLaunch p) {
   if (threadIdx.x < 10) thr_s[threadIdx.x] = p.thr[threadIdx.x];
   if (threadIdx.x < 20) pacc_s[threadIdx.x] = p.pacc_f[threadIdx.x];
 
-  const int n_act = p.n_active_dev ? *p.n_active_dev : p.n_active;
+  const int n_act = live_count(p);
   const int tile = blockIdx.x * nwarps + warp;
   const int slot = tile * kTile + lane;
   const bool tile_live = tile * kTile < n_act;
@@ -223,7 +230,7 @@ __global__ void __launch_bounds__(128) k_sweep_global(SweepLaunch p) {
   if (threadIdx.x < 10) thr_s[threadIdx.x] = p.thr[threadIdx.x];
   if (threadIdx.x < 20) pacc_s[threadIdx.x] = p.pacc_f[threadIdx.x];
   __syncthreads();
-  const int n_act = p.n_active_dev ? *p.n_active_dev : p.n_active;
+  const int n_act = live_count(p);
   const int slot = blockIdx.x * blockDim.x + threadIdx.x;
   if (slot >= n_act) return;
   const int rep = p.active ? p.active[slot] : slot;
@@ -514,7 +521,7 @@ __global__ void __launch_bounds__(32) k_sweep_rows_pair(SweepLaunch p) {
     thrP[lane] = p.thr[cls];
     paccP[lane] = p.pacc_f[2 * cls];
   }
-  const int n_act = p.n_active_dev ? *p.n_active_dev : p.n_active;
+  const int n_act = live_count(p);
   const int tile = blockIdx.x;
   if (tile * kTile >= n_act) return;  // whole CTA (one warp) idle this batch
   const int slot = tile * kTile + lane;
@@ -606,7 +613,7 @@ __global__ void __launch_bounds__(32) k_sweep_rows(SweepLaunch p) {
 #pragma unroll
     for (int i = 0; i < 6; ++i) S[i] = sortS[i];
   }
-  const int n_act = p.n_active_dev ? *p.n_active_dev : p.n_active;
+  const int n_act = live_count(p);
   const int tile = blockIdx.x;
   if (tile * kTile >= n_act) return;  // whole CTA (one warp) idle this batch
   const int slot = tile * kTile + lane;
@@ -660,7 +667,7 @@ __global__ void __launch_bounds__(256) k_sweep_trace_cpu(SweepLaunch p) {
   const int nwarps = blockDim.x >> 5;
   double *pacc_s = reinterpret_cast<double *>(smem);  // [20] (160 B < header)
   if (threadIdx.x < 20) pacc_s[threadIdx.x] = p.pacc_cpu[threadIdx.x];
-  const int n_act = p.n_active_dev ? *p.n_active_dev : p.n_active;
+  const int n_act = live_count(p);
   const int tile = blockIdx.x * nwarps + warp;
   const int slot = tile * kTile + lane;
   const bool tile_live = tile * kTile < n_act;
@@ -832,6 +839,7 @@ int dispatch_kind(const SweepLaunch &p, cudaStream_t s) {
     GASP_CUDA(cudaGetLastError());
     return GASP_OK;
   }
+  if (p.variant == 6) return launch_sweep_tail(p, s);  // one warp per replica (MWC64X)
   if (p.variant == 1) {  // the generic kernel, kept selectable for comparisons
     return launch_tiles(p.L == 64 ? k_sweep_exact<64, F, K> : k_sweep_exact<0, F, K>, p, s);
   }

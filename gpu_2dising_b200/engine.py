@@ -67,6 +67,18 @@ class RngStates:
     def handle(self):
         return self._h
 
+    @property
+    def stride(self):
+        return (self.ngrids + 31) // 32 * 32
+
+    def read_states(self):
+        """Device states as (words, stride) uint32: MWC64X x / carry rows, or
+        the six XORWOW words."""
+        words = 2 if self.kind == "mwc64x" else 6
+        out = np.zeros(words * self.stride, np.uint32)
+        check(lib().gasp_rng_read_states(self._h, out, out.size), "gasp_rng_read_states")
+        return out.reshape(words, self.stride)
+
     def close(self):
         if self._h:
             lib().gasp_free_rand(self._h)
@@ -108,8 +120,19 @@ class DeviceGrids:
               "gasp_grids_upload_inputs")
 
     def set_option(self, option, value):
-        """Launch tuning (results never depend on it): see gasp_grids_set_option."""
+        """Launch tuning, see gasp_grids_set_option.  Results never depend on
+        it, except that sweep variant 6 and the committor tail threshold assign
+        the MWC64X stream's draws differently (same dynamics)."""
         check(lib().gasp_grids_set_option(self._h, int(option), int(value)), "gasp_grids_set_option")
+
+    def thresholds(self, beta, h):
+        """(thr uint32[10], float_compare): the integer acceptance test of the
+        sweep kernels, u <= thr[5*(spin up) + (# up neighbours)]."""
+        thr = np.zeros(10, np.uint32)
+        fc = C.c_int(0)
+        check(lib().gasp_acceptance_thresholds(self._h, float(beta), float(h), thr, C.byref(fc)),
+              "gasp_acceptance_thresholds")
+        return thr, bool(fc.value)
 
     def download(self):
         out = np.empty(self.L * self.L * self.ngrids, np.int32)

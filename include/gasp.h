@@ -111,16 +111,27 @@ int gasp_grids_upload_inputs_noalloc(gasp_grids_t *grids, const int *inputs, int
 int gasp_grids_shape(const gasp_grids_t *grids, int *L_out, int *ngrids_out);
 
 /* Launch tuning of a set (no reference counterpart; results never depend on
- * it).  GASP_OPT_SWEEP_VARIANT: 0 the fastest kernel for L (default: for
+ * it, except that variant 6 and GASP_OPT_TAIL_REPLICAS assign the MWC64X
+ * stream's draws to attempts differently: same dynamics, other trajectories).  GASP_OPT_SWEEP_VARIANT: 0 the fastest kernel for L (default: for
  * L = 32, 64, 128 the row kernel writing the centre word back on every
  * attempt, no divergent branch), 1 the generic kernel, 2 the row kernel with a
  * store only on acceptance, 3 the row kernel with pairwise
  * speculation of consecutive attempts, 4 the row kernel with the acceptance
  * decided by a per-draw mask of accepted neighbourhoods (falls back to 2 when
  * more than six classes can reject), 5 the generic kernel (L other than 32,
- * 64, 128) writing the centre word back on every attempt.  GASP_OPT_WARPS_PER_CTA: tiles per
- * CTA of the generic kernel (1..8). */
-enum { GASP_OPT_SWEEP_VARIANT = 1, GASP_OPT_WARPS_PER_CTA = 2 };
+ * 64, 128) writing the centre word back on every attempt, 6 one warp per
+ * replica (MWC64X stream only, 3 <= L <= 512; GASP_ERR_UNSUPPORTED otherwise):
+ * the warp applies up to 32 queued attempts of its replica per step, all
+ * those that touch no site or neighbour of another, in the order drawn --
+ * the same dynamics as the other variants with a different assignment of
+ * draws, and ~20x less time per sweep of a single replica, at a quarter of
+ * the throughput per SM when many replicas are live.
+ * GASP_OPT_WARPS_PER_CTA: tiles per CTA of the generic kernel (1..8).
+ * GASP_OPT_TAIL_REPLICAS: device-side committor shooting (itask 1 with
+ * compaction) on the MWC64X stream sweeps with variant 6 once at most this
+ * many replicas are undecided (default 4096; 0: never).  No effect on the
+ * XORWOW stream, whose trajectories stay bit-identical to the reference's. */
+enum { GASP_OPT_SWEEP_VARIANT = 1, GASP_OPT_WARPS_PER_CTA = 2, GASP_OPT_TAIL_REPLICAS = 3 };
 int gasp_grids_set_option(gasp_grids_t *grids, int option, int value);
 
 /* ------------------------------------------------------------ RNG states */
@@ -145,6 +156,24 @@ int gasp_init_rand_mode(int ngrids, int threads_per_block, unsigned long long se
 /* Host-only: the MWC64X start states gasp_init_rand_mode uploads, x of
  * replica r at out[r] and carry at out[stride + r] (2*stride words). */
 int gasp_mwc64x_seed_states(unsigned long long seed, int ngrids, int stride, uint32_t *out);
+/* The integer acceptance thresholds the sweep kernels use for (beta, h) on
+ * this set's device: an attempt at class c = 5*(spin up) + (# up neighbours)
+ * accepts iff its raw 32-bit draw u <= thr10[c], which is exactly
+ * curand_uniform-style "u2 < P" of the reference's float table.
+ * *float_compare (optional) is set when some class can never accept and the
+ * kernels compare in float instead. */
+int gasp_acceptance_thresholds(gasp_grids_t *grids, double beta, double h, uint32_t *thr10,
+                               int *float_compare);
+/* Host-only: the lane substream multipliers of sweep variant 6: lane j of a
+ * replica with MWC64X state X = x*A + c starts at X * mul32[j] mod M
+ * (mul32[j] = A^(j*2^35)); inv32[j] = A^-(j*2^35) mod M.  A = 4294883355,
+ * M = A*2^32 - 1. */
+int gasp_mwc64x_lane_multipliers(uint64_t *mul32, uint64_t *inv32);
+/* Copies an RNG set's device states to the host: the XORWOW layout of
+ * gasp_init_rand (6 words per replica) or the MWC64X layout of
+ * gasp_mwc64x_seed_states (x at [r], carry at [stride + r]), stride = ngrids
+ * rounded up to 32.  nwords must cover words * stride. */
+int gasp_rng_read_states(const gasp_rng_t *rng, uint32_t *out, long long nwords);
 int gasp_free_rand(gasp_rng_t *rng);
 
 /* ------------------------------------------------------------ kernels */

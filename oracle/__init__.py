@@ -35,6 +35,8 @@ _i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
 _f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
 _f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 _u8p = np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")
+_u32p = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
+_u64p = np.ctypeslib.ndpointer(dtype=np.uint64, flags="C_CONTIGUOUS")
 
 _lib = None
 
@@ -68,6 +70,12 @@ def lib():
         L.orc_bootstrap_errbar.restype = C.c_double
         L.orc_srand.argtypes = [C.c_uint]
         L.orc_committor_from_fates.argtypes = [C.c_int, C.c_int, _i32p, _f32p]
+        L.orc_sweep_mwc.argtypes = [C.c_int, _i32p, C.c_longlong, C.POINTER(C.c_uint32),
+                                    C.POINTER(C.c_uint32), _u32p]
+        L.orc_sweep_mwc.restype = C.c_longlong
+        L.orc_sweep_tail.argtypes = [C.c_int, _i32p, C.c_int, C.POINTER(C.c_uint32),
+                                     C.POINTER(C.c_uint32), _u32p, _u64p, _u64p, C.c_void_p]
+        L.orc_sweep_tail.restype = C.c_longlong
         _lib = L
     return _lib
 
@@ -101,6 +109,30 @@ def sweep_gpu_stream(L, grid, ustream, P):
     n = ustream.size // 2
     lib().orc_sweep_gpu_stream(L, grid, n, ustream, np.ascontiguousarray(P, np.float32))
     return n
+
+
+def sweep_mwc(L, grid, nattempts, x, c, thr):
+    """In-place sweep of one int32 grid on one MWC64X stream (production
+    row kernels); returns the stream state (x, c) afterwards."""
+    xs, cs = C.c_uint32(int(x)), C.c_uint32(int(c))
+    lib().orc_sweep_mwc(L, grid, int(nattempts), C.byref(xs), C.byref(cs),
+                        np.ascontiguousarray(thr, np.uint32))
+    return xs.value, cs.value
+
+
+def sweep_tail(L, grid, nsweeps, x, c, thr, mul, inv, record=False):
+    """In-place one-warp-per-replica sweep (variant 6) of one int32 grid,
+    restated serially; returns (x, c) afterwards and, with record=True, the
+    applied (site, u) pairs in order as uint32[n, 2]."""
+    xs, cs = C.c_uint32(int(x)), C.c_uint32(int(c))
+    order = np.zeros((nsweeps * L * L, 2), np.uint32) if record else None
+    n = lib().orc_sweep_tail(L, grid, int(nsweeps), C.byref(xs), C.byref(cs),
+                             np.ascontiguousarray(thr, np.uint32),
+                             np.ascontiguousarray(mul, np.uint64),
+                             np.ascontiguousarray(inv, np.uint64),
+                             order.ctypes.data_as(C.c_void_p) if record else None)
+    assert n == nsweeps * L * L
+    return (xs.value, cs.value, order) if record else (xs.value, cs.value)
 
 
 def magnetisation_gpu(L, grids):

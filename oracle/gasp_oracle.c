@@ -244,3 +244,152 @@ void orc_committor_from_fates(int ngrids, int ninputs, const int *fate, float *p
     pB[i] = (float)nB / (float)(sub - nF);
   }
 }
+
+/* ------------------------------------------------------------------------
+ * Production stream (MWC64X) sweeps.  No reference counterpart: the
+ * reference has only cuRAND XORWOW.  Attempt semantics follow
+ * src/mc_gpu.cu:311-340 (random site, accept on a uniform draw below the
+ * table entry) with integer draws: site = (r * N) >> 32 of a 32-bit draw r,
+ * accept iff the next draw u <= thr[5*(spin up) + (# up neighbours)], where
+ * thr[] comes from the product's gasp_acceptance_thresholds.
+ * ---------------------------------------------------------------------- */
+#define ORC_MWC_A 4294883355ull
+
+static inline uint32_t orc_mwc_next(uint32_t *x, uint32_t *c) {
+  uint32_t r = *x ^ *c;
+  uint64_t t = (uint64_t)(*x) * ORC_MWC_A + *c;
+  *x = (uint32_t)t;
+  *c = (uint32_t)(t >> 32);
+  return r;
+}
+
+static inline void orc_apply_int(int L, int *grid, uint32_t s, uint32_t u, const uint32_t thr[10]) {
+  int row = (int)s / L, col = (int)s % L;
+  int up = 0;
+  up += grid[L * ((row + 1) % L) + col] > 0;
+  up += grid[L * ((row + L - 1) % L) + col] > 0;
+  up += grid[L * row + (col + 1) % L] > 0;
+  up += grid[L * row + (col + L - 1) % L] > 0;
+  int cls = 5 * (grid[s] > 0) + up;
+  if (u <= thr[cls]) grid[s] = -grid[s];
+}
+
+/* One replica, one MWC64X stream (x, c updated in place), attempts applied
+ * one at a time: the row kernels' production mode. */
+long long orc_sweep_mwc(int L, int *grid, long long nattempts, uint32_t *x, uint32_t *c,
+                        const uint32_t thr[10]) {
+  const uint64_t N = (uint64_t)L * L;
+  for (long long a = 0; a < nattempts; ++a) {
+    uint32_t s = (uint32_t)(((uint64_t)orc_mwc_next(x, c) * N) >> 32);
+    uint32_t u = orc_mwc_next(x, c);
+    orc_apply_int(L, grid, s, u, thr);
+  }
+  return nattempts;
+}
+
+static inline uint64_t orc_mulmod(uint64_t a, uint64_t b, uint64_t m) {
+  return (uint64_t)((unsigned __int128)a * b % m);
+}
+
+static inline int orc_adjacent(int L, uint32_t a, uint32_t b) {
+  int ra = (int)a / L, ca = (int)a % L, rb = (int)b / L, cb = (int)b % L;
+  if (ra == rb) return cb == (ca + 1) % L || ca == (cb + 1) % L;
+  if (ca == cb) return rb == (ra + 1) % L || ra == (rb + 1) % L;
+  return 0;
+}
+
+/* The one-warp-per-replica sweep (sweep variant 6), restated serially: the
+ * window of 32 pending attempts (lane l at position (l - head) mod 32), the
+ * rule fixing how many are applied per round (up to and including the first
+ * position whose site, or a neighbour of it, holds another pending attempt),
+ * which lane's substream draws each new attempt (every lane keeps its next
+ * attempt drawn one assignment ahead), and the replica's stream state
+ * afterwards.  Attempts are applied one at a time in window order; the kernel
+ * applies each round's at once, which must give the same lattice.
+ * x/c: the replica's state (in/out); mul/inv: gasp_mwc64x_lane_multipliers.
+ * order (optional, 2 * nsweeps * L*L words) receives (site, u) of every
+ * attempt in the order applied. */
+long long orc_sweep_tail(int L, int *grid, int nsweeps, uint32_t *x, uint32_t *c,
+                         const uint32_t thr[10], const uint64_t mul[32], const uint64_t inv[32],
+                         uint32_t *order) {
+  const uint64_t A = ORC_MWC_A, M = (A << 32) - 1;
+  const uint64_t N = (uint64_t)L * L;
+  const long long Q = (long long)nsweeps * (long long)N;
+  uint32_t lx[32], lc[32], site[32], uu[32], nsite[32], nuu[32];
+  unsigned nd[32];
+  int valid[32], flag[32];
+  const uint64_t X = (uint64_t)(*x) * A + *c;
+  for (int j = 0; j < 32; ++j) {
+    uint64_t Xj = orc_mulmod(X, mul[j], M);
+    lx[j] = (uint32_t)(Xj / A);
+    lc[j] = (uint32_t)(Xj % A);
+    nsite[j] = (uint32_t)(((uint64_t)orc_mwc_next(&lx[j], &lc[j]) * N) >> 32);
+    nuu[j] = orc_mwc_next(&lx[j], &lc[j]);
+    nd[j] = 2;
+  }
+#define ORC_TAIL_TAKE(j)                                                          \
+  do {                                                                            \
+    site[j] = nsite[j];                                                           \
+    uu[j] = nuu[j];                                                               \
+    nsite[j] = (uint32_t)(((uint64_t)orc_mwc_next(&lx[j], &lc[j]) * N) >> 32);    \
+    nuu[j] = orc_mwc_next(&lx[j], &lc[j]);                                        \
+    nd[j] += 2;                                                                   \
+  } while (0)
+  long long drawn = Q < 32 ? Q : 32, done = 0, applied = 0;
+  for (int j = 0; j < 32; ++j) {
+    valid[j] = j < drawn;
+    if (valid[j]) ORC_TAIL_TAKE(j);
+  }
+  int head = 0;
+  long long pend = drawn;
+  while (done < Q) {
+    for (int j = 0; j < 32; ++j) {
+      flag[j] = 0;
+      if (!valid[j]) continue;
+      for (int i = 0; i < 32; ++i)
+        if (i != j && valid[i] && (site[i] == site[j] || orc_adjacent(L, site[i], site[j])))
+          flag[j] = 1;
+    }
+    long long k = 32;
+    for (int p = 0; p < 32; ++p) {
+      int j = (head + p) & 31;
+      if (flag[j]) {
+        k = p + 1;
+        break;
+      }
+    }
+    if (k > pend) k = pend;
+    for (int p = 0; p < k; ++p) {
+      int j = (head + p) & 31;
+      orc_apply_int(L, grid, site[j], uu[j], thr);
+      if (order) {
+        order[2 * applied] = site[j];
+        order[2 * applied + 1] = uu[j];
+      }
+      ++applied;
+    }
+    done += k;
+    head = (int)((head + k) & 31);
+    pend -= k;
+    long long room = 32 - pend, left = Q - drawn;
+    long long nnew = room < left ? room : left;
+    for (int j = 0; j < 32; ++j) {
+      int p2 = (j - head) & 31;
+      if (p2 >= pend) {
+        valid[j] = p2 - pend < nnew;
+        if (valid[j]) ORC_TAIL_TAKE(j);
+      }
+    }
+    pend += nnew;
+    drawn += nnew;
+  }
+#undef ORC_TAIL_TAKE
+  int js = 0;
+  for (int j = 1; j < 32; ++j)
+    if (nd[j] > nd[js]) js = j;
+  uint64_t Xe = (uint64_t)lx[js] * A + lc[js];
+  uint64_t Xb = orc_mulmod(Xe, inv[js], M);
+  *x = (uint32_t)(Xb / A);
+  *c = (uint32_t)(Xb % A);
+  return applied;
+}

@@ -31,6 +31,20 @@ long long orc_sweep_cpu_stream(int L, int *grid, long long nattempts,
 long long orc_sweep_gpu_stream(int L, int *grid, long long nattempts,
                                const float *ustream, const float P[20]);
 
+/* Production stream (MWC64X; no reference counterpart).  One replica, one
+ * stream (x, c in/out): site = (r * L*L) >> 32 of a draw r, accept iff the
+ * next draw u <= thr[5*(spin up) + (# up neighbours)]; attempts in order. */
+long long orc_sweep_mwc(int L, int *grid, long long nattempts, uint32_t *x, uint32_t *c,
+                        const uint32_t thr[10]);
+/* The one-warp-per-replica sweep (variant 6) restated serially: 32 lane
+ * substreams (X * mul[j] mod M), the window and conflict rule that fix which
+ * lane draws each attempt, attempts applied one at a time in window order,
+ * and the replica's state afterwards (x, c in/out).  order (optional) gets
+ * (site, u) of every attempt in the order applied.  Returns attempts. */
+long long orc_sweep_tail(int L, int *grid, int nsweeps, uint32_t *x, uint32_t *c,
+                         const uint32_t thr[10], const uint64_t mul[32], const uint64_t inv[32],
+                         uint32_t *order);
+
 /* Magnetisation, GPU flavour: float running sum / (float)(L*L)
  * (src/mc_gpu.cu:437-455). */
 float orc_magnetisation_gpu(int L, const int *grid);
