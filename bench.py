@@ -466,6 +466,54 @@ def run_cluster(args):
     print(json.dumps(line), flush=True)
 
 
+def run_tail(args):
+    """The end of a committor run: few undecided L=64 replicas on the
+    production stream.  Per replica count, the time of one sweep with the row
+    kernel (one lane per replica, variant 0) and with one warp per replica
+    (variant 6), CUDA events on the library's stream, 10 sweeps per launch as
+    in committor shooting."""
+    import torch
+    from gpu_2dising_b200 import _native as nat, engine
+    engine.init_device(0)
+    stream = torch.cuda.Stream()
+    engine.set_stream(stream.cuda_stream)
+    counts = [args.tail_replicas] if args.tail_replicas else [32, 148, 592, 2368, 4736, 9472,
+                                                                18944]
+    per_launch = 10
+    out = {}
+    with torch.cuda.stream(stream):
+        for n in counts:
+            row = {}
+            for v in (0, 6):
+                dg = engine.DeviceGrids(L, n, -np.ones((n, L, L), np.int32))
+                dg.set_option(nat.OPT_SWEEP_VARIANT, v)
+                rng = engine.RngStates(n, SEED + n, kind="mwc64x")
+                for _ in range(args.warmup):
+                    dg.sweep(rng, BETA, H, per_launch)
+                torch.cuda.synchronize()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                for _ in range(args.steps):
+                    dg.sweep(rng, BETA, H, per_launch)
+                e1.record(stream)
+                torch.cuda.synchronize()
+                ms = e0.elapsed_time(e1) / (args.steps * per_launch)
+                row[f"variant{v}"] = {"ms_per_sweep": ms,
+                                      "attempts_per_s": n * L * L / (ms / 1e3)}
+                dg.close()
+                rng.close()
+            row["speedup"] = row["variant0"]["ms_per_sweep"] / row["variant6"]["ms_per_sweep"]
+            out[str(n)] = row
+    first = out[str(counts[0])]
+    line = {"metric": "sweep time of few replicas, one warp per replica vs one lane per replica",
+            "value": first["variant6"]["ms_per_sweep"], "unit": "ms/sweep", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,
+            "speedup_vs_row_kernel": first["speedup"], "by_replicas": out,
+            "config": {"workload": f"L=64 all-down replicas, beta=0.54, h=0.07, MWC64X stream, "
+                                   f"{per_launch} sweeps per launch; replica counts {counts}"}}
+    print(json.dumps(line), flush=True)
+
+
 def run_rate(args):
     """The full production swarm of the headline workload (L=64, 32768
     replicas, beta=0.54, h=0.07, 50 000 sweeps, checks every 100, dumps every
@@ -541,11 +589,13 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--workload", default="swarm",
                     choices=["swarm", "batched", "committor", "surrogate", "cnn", "rate",
-                             "cluster"],
+                             "cluster", "tail"],
                     help="swarm: the headline single-group swarm; batched: uneven groups; "
                          "committor: seeded droplet shooting")
     ap.add_argument("--cnn-grids", type=int, default=100000)
     ap.add_argument("--rate-sweeps", type=int, default=50000)
+    ap.add_argument("--tail-replicas", type=int, default=0,
+                    help="tail workload: one replica count (default: a range)")
     ap.add_argument("--committor-inputs", type=int, default=64)
     ap.add_argument("--committor-shots", type=int, default=4096)
     ap.add_argument("--committor-check", type=int, default=10)
@@ -582,6 +632,8 @@ def main():
     elif args.workload == "rate":
         if rank == 0:
             run_rate(args)
+    elif args.workload == "tail":
+        run_tail(args)
     elif args.workload == "cluster":
         if rank == 0:
             run_cluster(args)

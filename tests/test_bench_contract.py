@@ -37,5 +37,5 @@ def test_bench_lists_its_workloads():
     r = subprocess.run([sys.executable, "bench.py", "--help"], cwd=REPO, capture_output=True,
                        text=True, timeout=120)
     assert r.returncode == 0
-    for w in ("swarm", "batched", "committor", "surrogate", "cnn", "rate", "cluster"):
+    for w in ("swarm", "batched", "committor", "surrogate", "cnn", "rate", "cluster", "tail"):
         assert w in r.stdout
