@@ -381,6 +381,8 @@ def run_committor(args):
     t0 = time.perf_counter()
     dg = engine.DeviceGrids(L, n)
     dg.upload_inputs(inputs)
+    if args.committor_tail >= 0:  # 3 = GASP_OPT_TAIL_REPLICAS (MWC64X stream only)
+        dg.set_option(3, args.committor_tail)
     rng = engine.RngStates(n, SEED, kind=args.rng)
     res, fates, drv_s, attempts = engine.run_driver(
         dg, rng, BETA, H, 20000, args.committor_check, 20000, itask=1, dn_thr=-0.93,
@@ -397,7 +399,9 @@ def run_committor(args):
         "config": {"workload": f"{ngrid_in} droplet grids L=64 (r~U[4,12], 2% flips), "
                                f"{shots} shots each, beta=0.54, h=0.07, dn=-0.93, up=0.9, "
                                "cap 20000 sweeps, compaction on",
-                   "check_int": args.committor_check, "rng": args.rng},
+                   "check_int": args.committor_check, "rng": args.rng,
+                   "tail_replicas": (args.committor_tail if args.committor_tail >= 0
+                                     else "default")},
     }
     print(json.dumps(line), flush=True)
 
@@ -599,6 +603,9 @@ def main():
     ap.add_argument("--committor-inputs", type=int, default=64)
     ap.add_argument("--committor-shots", type=int, default=4096)
     ap.add_argument("--committor-check", type=int, default=10)
+    ap.add_argument("--committor-tail", type=int, default=-1,
+                    help="live replicas at which MWC64X shooting switches to one warp per "
+                         "replica (-1: library default, 0: never)")
     ap.add_argument("--surrogate-train", type=int, default=20000)
     ap.add_argument("--surrogate-test", type=int, default=2000)
     ap.add_argument("--surrogate-screen", type=int, default=100000)

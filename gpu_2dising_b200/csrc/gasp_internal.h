@@ -117,6 +117,8 @@ int launch_sweep_trace_cpu(const SweepLaunch &p, cudaStream_t s);
 // One warp per replica, MWC64X stream only (gasp_tail.cu); p.n_active is the
 // launch shape (an upper bound of *p.n_active_dev when that is set).
 int launch_sweep_tail(const SweepLaunch &p, cudaStream_t s);
+// Multispin shared-site sweep, MWC64X stream, no active list (gasp_shared.cu).
+int launch_sweep_shared(const SweepLaunch &p, cudaStream_t s);
 int launch_measure(const uint32_t *lat, int L, int ngrids, float *mag, cudaStream_t s);
 int launch_pack_grids(const int *grids32, uint32_t *lat, int L, int ngrids, cudaStream_t s,
                       int per_input = 0);

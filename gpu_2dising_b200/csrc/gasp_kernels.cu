@@ -839,7 +839,8 @@ int dispatch_kind(const SweepLaunch &p, cudaStream_t s) {
     GASP_CUDA(cudaGetLastError());
     return GASP_OK;
   }
-  if (p.variant == 6) return launch_sweep_tail(p, s);  // one warp per replica (MWC64X)
+  if (p.variant == 6) return launch_sweep_tail(p, s);    // one warp per replica (MWC64X)
+  if (p.variant == 7) return launch_sweep_shared(p, s);  // shared site per tile (MWC64X)
   if (p.variant == 1) {  // the generic kernel, kept selectable for comparisons
     return launch_tiles(p.L == 64 ? k_sweep_exact<64, F, K> : k_sweep_exact<0, F, K>, p, s);
   }

@@ -124,8 +124,13 @@ int gasp_grids_shape(const gasp_grids_t *grids, int *L_out, int *ngrids_out);
  * the warp applies up to 32 queued attempts of its replica per step, all
  * those that touch no site or neighbour of another, in the order drawn --
  * the same dynamics as the other variants with a different assignment of
- * draws, and ~20x less time per sweep of a single replica, at a quarter of
- * the throughput per SM when many replicas are live.
+ * draws, and ~5x less time per sweep of a single replica, at a quarter of
+ * the throughput per SM when many replicas are live; 7 the multispin
+ * shared-site sweep (MWC64X stream only, integer thresholds, no active
+ * list; GASP_ERR_UNSUPPORTED otherwise): the 32 replicas of a tile share each
+ * attempt's site, held as one word per site, neighbour counts by bitwise
+ * full adders, per-replica acceptance draws, a ballot flip mask -- replicas
+ * of a tile are correlated; about half the throughput of variant 0.
  * GASP_OPT_WARPS_PER_CTA: tiles per CTA of the generic kernel (1..8).
  * GASP_OPT_TAIL_REPLICAS: device-side committor shooting (itask 1 with
  * compaction) on the MWC64X stream sweeps with variant 6 once at most this

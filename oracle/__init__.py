@@ -76,6 +76,8 @@ def lib():
         L.orc_sweep_tail.argtypes = [C.c_int, _i32p, C.c_int, C.POINTER(C.c_uint32),
                                      C.POINTER(C.c_uint32), _u32p, _u64p, _u64p, C.c_void_p]
         L.orc_sweep_tail.restype = C.c_longlong
+        L.orc_sweep_shared.argtypes = [C.c_int, C.c_int, _i32p, C.c_int, _u32p, _u32p, _u32p]
+        L.orc_sweep_shared.restype = C.c_longlong
         _lib = L
     return _lib
 
@@ -133,6 +135,19 @@ def sweep_tail(L, grid, nsweeps, x, c, thr, mul, inv, record=False):
                              order.ctypes.data_as(C.c_void_p) if record else None)
     assert n == nsweeps * L * L
     return (xs.value, cs.value, order) if record else (xs.value, cs.value)
+
+
+def sweep_shared(L, grids, nsweeps, x, c, thr):
+    """In-place shared-site sweep (variant 7) of one tile of <= 32 int32
+    grids; returns the streams (x, c) afterwards as uint32 arrays."""
+    g = np.ascontiguousarray(grids, np.int32)
+    assert g.ndim == 3 and g.shape[0] <= 32
+    xs = np.array(x, np.uint32)
+    cs = np.array(c, np.uint32)
+    lib().orc_sweep_shared(L, g.shape[0], g.reshape(-1), int(nsweeps), xs, cs,
+                           np.ascontiguousarray(thr, np.uint32))
+    grids[...] = g
+    return xs, cs
 
 
 def magnetisation_gpu(L, grids):

@@ -393,3 +393,28 @@ long long orc_sweep_tail(int L, int *grid, int nsweeps, uint32_t *x, uint32_t *c
   *c = (uint32_t)(Xb % A);
   return applied;
 }
+
+/* The multispin shared-site sweep (sweep variant 7) restated serially for
+ * one tile of nrep <= 32 replicas (grids [nrep][L*L], streams x/c in/out):
+ * sites come in batches -- at the start of a batch each replica draws one
+ * site from its own stream, and attempt j of the batch uses replica j's site;
+ * every replica then draws its acceptance and flips on u <= thr[class]. */
+long long orc_sweep_shared(int L, int nrep, int *grids, int nsweeps, uint32_t *x, uint32_t *c,
+                           const uint32_t thr[10]) {
+  const uint64_t N = (uint64_t)L * L;
+  const long long Q = (long long)nsweeps * (long long)N;
+  uint32_t sites[32];
+  int j = 0;
+  for (long long a = 0; a < Q; ++a) {
+    if (j == 0)
+      for (int r = 0; r < nrep; ++r)
+        sites[r] = (uint32_t)(((uint64_t)orc_mwc_next(&x[r], &c[r]) * N) >> 32);
+    const uint32_t s = sites[j];
+    j = j + 1 == nrep ? 0 : j + 1;
+    for (int r = 0; r < nrep; ++r) {
+      uint32_t u = orc_mwc_next(&x[r], &c[r]);
+      orc_apply_int(L, grids + (size_t)r * N, s, u, thr);
+    }
+  }
+  return Q;
+}

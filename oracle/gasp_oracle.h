@@ -45,6 +45,13 @@ long long orc_sweep_tail(int L, int *grid, int nsweeps, uint32_t *x, uint32_t *c
                          const uint32_t thr[10], const uint64_t mul[32], const uint64_t inv[32],
                          uint32_t *order);
 
+/* The multispin shared-site sweep (variant 7) restated serially for one tile
+ * of nrep <= 32 replicas: per batch of nrep attempts each replica draws one
+ * site and attempt j uses replica j's; then every replica draws its
+ * acceptance.  grids [nrep][L*L], x/c [nrep] in/out.  Returns attempts. */
+long long orc_sweep_shared(int L, int nrep, int *grids, int nsweeps, uint32_t *x, uint32_t *c,
+                           const uint32_t thr[10]);
+
 /* Magnetisation, GPU flavour: float running sum / (float)(L*L)
  * (src/mc_gpu.cu:437-455). */
 float orc_magnetisation_gpu(int L, const int *grid);

@@ -196,3 +196,47 @@ def test_serial_mwc_oracle_consumes_two_draws_per_attempt():
     for _ in range(200):
         xs, cs, _ = _mwc(xs, cs)
     assert (x, c) == (xs, cs)
+
+
+def python_shared(L, grids, nsweeps, xs, cs, thr):
+    """Independent statement of the shared-site sweep (variant 7) on a tile."""
+    n, N = grids.shape[0], L * L
+    xs, cs = [int(v) for v in xs], [int(v) for v in cs]
+    j, sites = 0, [0] * n
+    for _ in range(nsweeps * N):
+        if j == 0:
+            for r in range(n):
+                xs[r], cs[r], v = _mwc(xs[r], cs[r])
+                sites[r] = (v * N) >> 32
+        s = sites[j]
+        j = (j + 1) % n
+        for r in range(n):
+            xs[r], cs[r], u = _mwc(xs[r], cs[r])
+            _apply(L, grids[r], s, u, thr)
+    return xs, cs
+
+
+def test_shared_site_oracle_matches_python_statement():
+    L, n, thr = 6, 5, _thr()
+    rs = np.random.default_rng(9)
+    g0 = np.where(rs.random((n, L, L)) < 0.4, 1, -1).astype(np.int32)
+    x0 = rs.integers(1, 2 ** 32 - 1, n).astype(np.uint32)
+    c0 = rs.integers(0, A - 1, n).astype(np.uint32)
+    g1 = g0.copy()
+    x1, c1 = oracle.sweep_shared(L, g1, 3, x0, c0, thr)
+    g2 = g0.copy()
+    x2, c2 = python_shared(L, g2, 3, x0, c0, thr)
+    assert np.array_equal(g1, g2)
+    assert [int(v) for v in x1] == x2 and [int(v) for v in c1] == c2
+
+
+def test_shared_site_tile_of_one_is_the_serial_sweep():
+    """A one-replica tile draws site then acceptance per attempt: exactly the
+    one-stream serial sweep."""
+    L, thr = 8, _thr()
+    g = np.where(np.random.default_rng(4).random((1, L, L)) < 0.5, 1, -1).astype(np.int32)
+    g2 = g[0].copy().reshape(-1)
+    xs, cs = oracle.sweep_shared(L, g, 4, [77], [7], thr)
+    x2, c2 = oracle.sweep_mwc(L, g2, 4 * L * L, 77, 7, thr)
+    assert np.array_equal(g[0].reshape(-1), g2)
+    assert (int(xs[0]), int(cs[0])) == (x2, c2)
