@@ -108,6 +108,46 @@ int refgpu_run_kernels(int L, int ngrids, int tpb, int method, unsigned long lon
   return 0;
 }
 
+// Device time of the reference's own sweep kernels: `ncalls` launches of
+// `method` (nsweeps each, launch shape of the reference driver) on ngrids
+// all-down L x L grids seeded as gpuInitRand, after one untimed launch.
+// ms_per_call receives the mean CUDA-event time of one launch.
+int refgpu_time_kernels(int L, int ngrids, int tpb, int method, unsigned long long seed,
+                        double beta, double h, int nsweeps, int ncalls, double *ms_per_call) {
+  int npad = padded_ngrids(ngrids);
+  size_t n = (size_t)L * L;
+  int *d_grids = nullptr, *d_nbr = nullptr;
+  curandState *d_state = nullptr;
+  std::vector<int> init(n * ngrids, -1);
+  HCHECK(cudaMalloc(&d_grids, n * npad * sizeof(int)));
+  HCHECK(cudaMemset(d_grids, 0, n * npad * sizeof(int)));
+  HCHECK(cudaMemcpy(d_grids, init.data(), n * ngrids * sizeof(int), cudaMemcpyHostToDevice));
+  HCHECK(cudaMalloc(&d_nbr, n * 4 * sizeof(int)));
+  preComputeNeighbours_gpu(L, d_grids, d_nbr);
+  gpuInitRand(ngrids, tpb, (unsigned long)seed, &d_state);
+  preComputeProbs_gpu(beta, h);
+  int rc = launch_reference_sweep(method, L, ngrids, tpb, d_state, d_grids, d_nbr, beta, h, nsweeps);
+  if (rc != 0) return rc;
+  cudaEvent_t e0, e1;
+  HCHECK(cudaEventCreate(&e0));
+  HCHECK(cudaEventCreate(&e1));
+  double total = 0.0;
+  for (int c = 0; c < ncalls; ++c) {
+    HCHECK(cudaEventRecord(e0));
+    rc = launch_reference_sweep(method, L, ngrids, tpb, d_state, d_grids, d_nbr, beta, h, nsweeps);
+    if (rc != 0) return rc;
+    HCHECK(cudaEventRecord(e1));
+    HCHECK(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    HCHECK(cudaEventElapsedTime(&ms, e0, e1));
+    total += ms;
+  }
+  *ms_per_call = total / ncalls;
+  cudaEventDestroy(e0); cudaEventDestroy(e1);
+  cudaFree(d_grids); cudaFree(d_nbr); cudaFree(d_state);
+  return 0;
+}
+
 // The first n curand_uniform draws of each replica's stream, seeded as
 // gpuInitRand does (subsequence = replica index).  out: [ngrids][n].
 int refgpu_uniform_stream(unsigned long long seed, int ngrids, int n, float *out) {
