@@ -56,7 +56,8 @@ EXPORTED = (
     "gasp_checkpoint_load",
     "gasp_batch_create", "gasp_batch_free", "gasp_batch_swarm", "gasp_batch_autotune",
     "gasp_cnn_param_count", "gasp_cnn_create", "gasp_cnn_free", "gasp_cnn_set_params",
-    "gasp_cnn_get_params", "gasp_cnn_predict", "gasp_cnn_gradients", "gasp_cnn_train_step",
+    "gasp_cnn_get_params", "gasp_cnn_predict", "gasp_cnn_predict_ex", "gasp_cnn_gradients",
+    "gasp_cnn_train_step",
 )
 
 
@@ -187,6 +188,7 @@ def _bind(lib):
         "gasp_cnn_set_params": (I, [P, _f32p]),
         "gasp_cnn_get_params": (I, [P, _f32p]),
         "gasp_cnn_predict": (I, [P, _i8p, I, _f32p]),
+        "gasp_cnn_predict_ex": (I, [P, _i8p, I, _f32p, _f32p]),
         "gasp_cnn_gradients": (I, [P, _i8p, _f32p, I, C.POINTER(C.c_float), _f32p]),
         "gasp_cnn_train_step": (I, [P, _i8p, _f32p, I, C.c_float, C.POINTER(C.c_float)]),
     }

@@ -644,6 +644,26 @@ __global__ void __launch_bounds__(256) k_conv_dw32(int L, int B, const __nv_bflo
 // Head: mean pool -> linear -> sigmoid -> cross-entropy; one warp per image,
 // lane = channel.  Writes q, adds the mean loss, the head's gradients and
 // dmean[b][c] = dL/d(pooled mean).
+// Magnetisation of int8 +-1 grids, one warp per grid: 16-byte loads summed
+// four bytes at a time with __dp4a; (float)sum / (float)N as the sweep
+// kernels compute it (the sum is exact).  N is a multiple of 128.
+__global__ void k_spin_mag(const int8_t *spins, int N, int batch, float *mag) {
+  const int g = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (g >= batch) return;
+  const int4 *src = reinterpret_cast<const int4 *>(spins + (size_t)g * N);
+  int acc = 0;
+  for (int i = lane; i < N / 16; i += 32) {
+    const int4 v = src[i];
+    acc = __dp4a(v.x, 0x01010101, acc);
+    acc = __dp4a(v.y, 0x01010101, acc);
+    acc = __dp4a(v.z, 0x01010101, acc);
+    acc = __dp4a(v.w, 0x01010101, acc);
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if (lane == 0) mag[g] = (float)acc / (float)N;
+}
+
 __global__ void k_head(int B, int N, const float *pool, const float *params, const float *labels,
                        float *q_out, float *loss, float *grad, float *dmean) {
   const int b = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -721,6 +741,7 @@ struct gasp_cnn {
   __nv_bfloat16 *d_w1, *d_w, *d_wt;
   int8_t *d_spins;
   float *d_labels, *d_q, *d_pool, *d_dmean, *d_loss;
+  float *d_mag;             // magnetisation of each predicted grid
   __nv_bfloat16 *d_act[4];  // a1..a4
   __nv_bfloat16 *d_dz[2];   // ping-pong data gradients
   int *d_err;
@@ -897,6 +918,7 @@ int gasp_cnn_create(int L, int max_batch, gasp_cnn_t **out) {
   A((void **)&c->d_spins, (size_t)max_batch * c->N);
   A((void **)&c->d_labels, (size_t)max_batch * sizeof(float));
   A((void **)&c->d_q, (size_t)max_batch * sizeof(float));
+  A((void **)&c->d_mag, (size_t)max_batch * sizeof(float));
   A((void **)&c->d_pool, (size_t)max_batch * kC * sizeof(float));
   A((void **)&c->d_dmean, (size_t)max_batch * kC * sizeof(float));
   A((void **)&c->d_loss, sizeof(float));
@@ -918,7 +940,7 @@ int gasp_cnn_create(int L, int max_batch, gasp_cnn_t **out) {
 int gasp_cnn_free(gasp_cnn_t *c) {
   if (!c) return GASP_OK;
   void *ptrs[] = {c->d_params, c->d_grad, c->d_m, c->d_v, c->d_w1, c->d_w, c->d_wt, c->d_spins,
-                  c->d_labels, c->d_q, c->d_pool, c->d_dmean, c->d_loss, c->d_err,
+                  c->d_labels, c->d_q, c->d_mag, c->d_pool, c->d_dmean, c->d_loss, c->d_err,
                   c->d_act[0], c->d_act[1], c->d_act[2], c->d_act[3], c->d_dz[0], c->d_dz[1]};
   for (void *p : ptrs) cudaFree(p);
   delete c;
@@ -940,7 +962,8 @@ int gasp_cnn_get_params(gasp_cnn_t *c, float *params) {
   return GASP_OK;
 }
 
-int gasp_cnn_predict(gasp_cnn_t *c, const int8_t *spins, int batch, float *q_out) {
+int gasp_cnn_predict_ex(gasp_cnn_t *c, const int8_t *spins, int batch, float *q_out,
+                        float *mag_out) {
   if (!c || !spins || !q_out || batch <= 0 || batch > c->max_batch) return GASP_ERR_INVALID;
   cudaStream_t s = current_stream();
   int rc;
@@ -950,7 +973,17 @@ int gasp_cnn_predict(gasp_cnn_t *c, const int8_t *spins, int batch, float *q_out
                                          nullptr, nullptr, nullptr);
   GASP_CUDA(cudaGetLastError());
   GASP_CUDA(cudaMemcpyAsync(q_out, c->d_q, (size_t)batch * sizeof(float), cudaMemcpyDeviceToHost, s));
+  if (mag_out) {
+    k_spin_mag<<<(batch + 7) / 8, 256, 0, s>>>(c->d_spins, c->N, batch, c->d_mag);
+    GASP_CUDA(cudaGetLastError());
+    GASP_CUDA(cudaMemcpyAsync(mag_out, c->d_mag, (size_t)batch * sizeof(float),
+                              cudaMemcpyDeviceToHost, s));
+  }
   return cnn_check_err(c, s);
+}
+
+int gasp_cnn_predict(gasp_cnn_t *c, const int8_t *spins, int batch, float *q_out) {
+  return gasp_cnn_predict_ex(c, spins, batch, q_out, nullptr);
 }
 
 int gasp_cnn_gradients(gasp_cnn_t *c, const int8_t *spins, const float *labels, int batch,

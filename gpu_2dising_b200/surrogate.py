@@ -66,16 +66,25 @@ class CommittorCNN:
         g = np.ascontiguousarray(grids, np.int8).reshape(-1, self.L, self.L)
         return g
 
-    def predict(self, grids):
+    def predict(self, grids, with_mag=False):
+        """pB estimates of int8 grids; with_mag=True also returns each grid's
+        magnetisation, computed on the device from the same upload."""
         g = self._spins(grids)
         out = np.empty(g.shape[0], np.float32)
+        mag = np.empty(g.shape[0], np.float32) if with_mag else None
         for i in range(0, g.shape[0], self.max_batch):
             chunk = np.ascontiguousarray(g[i:i + self.max_batch])
-            q = np.empty(chunk.shape[0], np.float32)
-            check(lib().gasp_cnn_predict(self._h, chunk.reshape(-1), chunk.shape[0], q),
-                  "gasp_cnn_predict")
-            out[i:i + chunk.shape[0]] = q
-        return out
+            n = chunk.shape[0]
+            q = np.empty(n, np.float32)
+            if with_mag:
+                m = np.empty(n, np.float32)
+                check(lib().gasp_cnn_predict_ex(self._h, chunk.reshape(-1), n, q, m),
+                      "gasp_cnn_predict_ex")
+                mag[i:i + n] = m
+            else:
+                check(lib().gasp_cnn_predict(self._h, chunk.reshape(-1), n, q), "gasp_cnn_predict")
+            out[i:i + n] = q
+        return (out, mag) if with_mag else out
 
     def gradients(self, grids, labels):
         g = self._spins(grids)
@@ -221,12 +230,19 @@ def harvest_snapshots(n, L=64, beta=0.54, h=0.07, replicas=32768, tot=12000, eve
     return np.stack(out[:n]) if out else np.zeros((0, L, L), np.int8)
 
 
-def screen(cnn, grids, beta, h, fallback_shots=128, band=0.1, **shoot_kw):
-    """Surrogate pB for every grid; grids predicted within `band` of 0.5 are
-    shot instead.  Returns (pB, fallback mask, seconds)."""
+def screen(cnn, grids, beta, h, fallback_shots=128, band=0.1, window=None, **shoot_kw):
+    """Surrogate pB for every grid; grids predicted within `band` of 0.5, and
+    (window=(lo, hi), the magnetisation range the network was trained on)
+    grids whose magnetisation lies outside it, are shot instead.  Returns
+    (pB, fallback mask, seconds)."""
     t0 = time.perf_counter()
-    pred = cnn.predict(grids).astype(np.float64)
-    near = np.abs(pred - 0.5) < band
+    if window is None:
+        pred = cnn.predict(grids).astype(np.float64)
+        near = np.abs(pred - 0.5) < band
+    else:
+        pred, mag = cnn.predict(grids, with_mag=True)
+        pred = pred.astype(np.float64)
+        near = (np.abs(pred - 0.5) < band) | (mag <= window[0]) | (mag >= window[1])
     out = pred.copy()
     if near.any():
         pb, _, _ = shoot(np.asarray(grids)[near], fallback_shots, beta, h, **shoot_kw)
@@ -262,7 +278,9 @@ def run_experiment(n_train=20000, train_shots=256, n_test=2000, test_shots=1024,
     t["train_s"] = time.perf_counter() - t0
     pred_te = net.predict(te).astype(np.float64)
     mae_surrogate = float(np.mean(np.abs(pred_te - y_te)))
-    scr_te, near_te, _ = screen(net, te, beta, h, fallback_shots=baseline_shots, seed=seed + 17)
+    window = (-0.93, -0.65)  # the harvest window: the network's training distribution
+    scr_te, near_te, _ = screen(net, te, beta, h, fallback_shots=baseline_shots, window=window,
+                                seed=seed + 17)
     mae_screened = float(np.mean(np.abs(scr_te - y_te)))
     # the screening question: is pB in [0.3, 0.7]?
     want, got = (y_te >= 0.3) & (y_te <= 0.7), (scr_te >= 0.3) & (scr_te <= 0.7)
@@ -287,7 +305,8 @@ def run_experiment(n_train=20000, train_shots=256, n_test=2000, test_shots=1024,
         st_fb, st_sh, t_scr = {}, {}, []
         for rep in range(3):
             _, near_sc, ts = screen(net, sc, beta, h, fallback_shots=baseline_shots,
-                                    seed=seed + 23 + 101 * rep, cap=cap, stats=st_fb)
+                                    window=window, seed=seed + 23 + 101 * rep, cap=cap,
+                                    stats=st_fb)
             t_scr.append(ts)
         t_scr_med = float(np.median(t_scr))
         _, a_sh, t_sh = shoot(sc, baseline_shots, beta, h, seed=seed + 29, cap=cap, stats=st_sh)

@@ -360,6 +360,10 @@ int gasp_cnn_free(gasp_cnn_t *cnn);
 int gasp_cnn_set_params(gasp_cnn_t *cnn, const float *params);  /* also resets Adam */
 int gasp_cnn_get_params(gasp_cnn_t *cnn, float *params);
 int gasp_cnn_predict(gasp_cnn_t *cnn, const int8_t *spins, int batch, float *q_out);
+/* The same, and (mag_out non-NULL) each grid's magnetisation from the
+ * uploaded spins, for out-of-distribution checks before trusting q. */
+int gasp_cnn_predict_ex(gasp_cnn_t *cnn, const int8_t *spins, int batch, float *q_out,
+                        float *mag_out);
 /* Loss (mean over the batch) and its gradient for labels in [0, 1]. */
 int gasp_cnn_gradients(gasp_cnn_t *cnn, const int8_t *spins, const float *labels, int batch,
                        float *loss_out, float *grad_out);

@@ -69,3 +69,24 @@ def test_training_learns():
     mae1 = hist[-1]["val_mae"]
     assert hist[-1]["loss"] < hist[0]["loss"]
     assert mae1 < 0.5 * mae0 and mae1 < 0.05, (mae0, hist)
+
+
+def test_predict_returns_magnetisation_and_screen_shoots_out_of_window_grids():
+    """gasp_cnn_predict_ex gives each grid's magnetisation from the upload;
+    screening shoots grids outside the training window whatever the network
+    predicts."""
+    g, _ = _data(70, 5)  # more than one 32-grid batch of the 64-grid handle
+    net = surrogate.CommittorCNN(L, 64, surrogate.init_params(2))
+    q, m = net.predict(g, with_mag=True)
+    # the pooled sums are accumulated with float atomics, so the last bit of q
+    # may differ between calls
+    assert np.allclose(q, net.predict(g), rtol=0, atol=1e-6)
+    assert np.array_equal(m, (g.reshape(70, -1).astype(np.int64).sum(axis=1) / (L * L))
+                          .astype(np.float32))
+    inside = np.full((2, L, L), -1, np.int8)
+    inside[:, :, :7] = 1  # m = -1 + 2*7/64, inside (-0.93, -0.65)
+    grids = np.concatenate([inside, np.ones((1, L, L), np.int8), -np.ones((1, L, L), np.int8)])
+    pb, shot, _ = surrogate.screen(net, grids, 0.54, 0.07, fallback_shots=16, band=0.0,
+                                   window=(-0.93, -0.65), seed=4)
+    assert shot.tolist() == [False, False, True, True]
+    assert pb[2] == 1.0 and pb[3] == 0.0  # all up is in B, all down in A at once
