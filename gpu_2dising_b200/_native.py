@@ -188,7 +188,7 @@ def _bind(lib):
         "gasp_cnn_set_params": (I, [P, _f32p]),
         "gasp_cnn_get_params": (I, [P, _f32p]),
         "gasp_cnn_predict": (I, [P, _i8p, I, _f32p]),
-        "gasp_cnn_predict_ex": (I, [P, _i8p, I, _f32p, _f32p]),
+        "gasp_cnn_predict_ex": (I, [P, _i8p, I, _f32p, C.c_void_p]),
         "gasp_cnn_gradients": (I, [P, _i8p, _f32p, I, C.POINTER(C.c_float), _f32p]),
         "gasp_cnn_train_step": (I, [P, _i8p, _f32p, I, C.c_float, C.POINTER(C.c_float)]),
     }

@@ -742,6 +742,11 @@ struct gasp_cnn {
   int8_t *d_spins;
   float *d_labels, *d_q, *d_pool, *d_dmean, *d_loss;
   float *d_mag;             // magnetisation of each predicted grid
+  // chunked prediction (batches above max_batch): a second input buffer and
+  // a copy stream, so the next chunk's upload overlaps this chunk's network
+  int8_t *d_spins2;
+  cudaStream_t copy_stream;
+  cudaEvent_t ev_copied[2], ev_used[2];
   __nv_bfloat16 *d_act[4];  // a1..a4
   __nv_bfloat16 *d_dz[2];   // ping-pong data gradients
   int *d_err;
@@ -808,7 +813,7 @@ int launch_conv(const ConvArgs &a, int batch, cudaStream_t s) {
   return launch_persistent(k_conv_tc<MODE>, smem_max, smem, b, s);
 }
 
-int cnn_forward(gasp_cnn *c, int batch, cudaStream_t s) {
+int cnn_forward(gasp_cnn *c, int batch, cudaStream_t s, const int8_t *spins = nullptr) {
   int rc;
   const int B = batch;
   k_pack_weights<<<(3 * 9216 + 255) / 256, 256, 0, s>>>(c->d_params, c->d_w1, c->d_w, c->d_wt);
@@ -818,7 +823,7 @@ int cnn_forward(gasp_cnn *c, int batch, cudaStream_t s) {
   memset(&a, 0, sizeof a);
   a.L = c->L;
   a.err = c->d_err;
-  a.spins = c->d_spins;
+  a.spins = spins ? spins : c->d_spins;
   a.w = c->d_w1;
   a.bias = c->d_params + kOffB1;
   a.y = c->d_act[0];
@@ -843,6 +848,59 @@ int cnn_check_err(gasp_cnn *c, cudaStream_t s) {
     return GASP_ERR_TIMEOUT;
   }
   return GASP_OK;
+}
+
+// Prediction of more grids than one batch holds: chunks of max_batch through
+// two input buffers.  The copy stream uploads chunk i+1 (after the network of
+// chunk i-1 has read that buffer) while the current stream runs chunk i, so
+// the host-to-device copies hide behind the convolutions.
+int predict_chunked(gasp_cnn *c, const int8_t *spins, int batch, float *q_out, float *mag_out,
+                    cudaStream_t s) {
+  if (!c->copy_stream) {
+    GASP_CUDA(cudaMalloc(&c->d_spins2, (size_t)c->max_batch * c->N));
+    GASP_CUDA(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+    for (int i = 0; i < 2; ++i) {
+      GASP_CUDA(cudaEventCreateWithFlags(&c->ev_copied[i], cudaEventDisableTiming));
+      GASP_CUDA(cudaEventCreateWithFlags(&c->ev_used[i], cudaEventDisableTiming));
+    }
+  }
+  cudaStream_t cs = c->copy_stream;
+  int8_t *buf[2] = {c->d_spins, c->d_spins2};
+  const int mb = c->max_batch;
+  const int nch = (batch + mb - 1) / mb;
+  auto rows = [&](int i) { return batch - i * mb < mb ? batch - i * mb : mb; };
+  // earlier work on s may still read either buffer
+  for (int b = 0; b < 2; ++b) GASP_CUDA(cudaEventRecord(c->ev_used[b], s));
+  GASP_CUDA(cudaStreamWaitEvent(cs, c->ev_used[0], 0));
+  GASP_CUDA(cudaMemcpyAsync(buf[0], spins, (size_t)rows(0) * c->N, cudaMemcpyHostToDevice, cs));
+  GASP_CUDA(cudaEventRecord(c->ev_copied[0], cs));
+  int rc;
+  for (int i = 0; i < nch; ++i) {
+    const int b = i & 1, n = rows(i);
+    GASP_CUDA(cudaStreamWaitEvent(s, c->ev_copied[b], 0));
+    if ((rc = cnn_forward(c, n, s, buf[b]))) return rc;
+    k_head<<<(n + 7) / 8, 256, 0, s>>>(n, c->N, c->d_pool, c->d_params, nullptr, c->d_q, nullptr,
+                                       nullptr, nullptr);
+    GASP_CUDA(cudaGetLastError());
+    if (mag_out) {
+      k_spin_mag<<<(n + 7) / 8, 256, 0, s>>>(buf[b], c->N, n, c->d_mag);
+      GASP_CUDA(cudaGetLastError());
+    }
+    GASP_CUDA(cudaEventRecord(c->ev_used[b], s));
+    if (i + 1 < nch) {
+      const int nb = (i + 1) & 1;
+      GASP_CUDA(cudaStreamWaitEvent(cs, c->ev_used[nb], 0));
+      GASP_CUDA(cudaMemcpyAsync(buf[nb], spins + (size_t)(i + 1) * mb * c->N,
+                                (size_t)rows(i + 1) * c->N, cudaMemcpyHostToDevice, cs));
+      GASP_CUDA(cudaEventRecord(c->ev_copied[nb], cs));
+    }
+    GASP_CUDA(cudaMemcpyAsync(q_out + (size_t)i * mb, c->d_q, (size_t)n * sizeof(float),
+                              cudaMemcpyDeviceToHost, s));
+    if (mag_out)
+      GASP_CUDA(cudaMemcpyAsync(mag_out + (size_t)i * mb, c->d_mag, (size_t)n * sizeof(float),
+                                cudaMemcpyDeviceToHost, s));
+  }
+  return cnn_check_err(c, s);
 }
 
 // Forward + loss + all gradients (into d_grad) for the uploaded batch.
@@ -943,6 +1001,14 @@ int gasp_cnn_free(gasp_cnn_t *c) {
                   c->d_labels, c->d_q, c->d_mag, c->d_pool, c->d_dmean, c->d_loss, c->d_err,
                   c->d_act[0], c->d_act[1], c->d_act[2], c->d_act[3], c->d_dz[0], c->d_dz[1]};
   for (void *p : ptrs) cudaFree(p);
+  if (c->copy_stream) {
+    cudaStreamDestroy(c->copy_stream);
+    for (int i = 0; i < 2; ++i) {
+      cudaEventDestroy(c->ev_copied[i]);
+      cudaEventDestroy(c->ev_used[i]);
+    }
+  }
+  cudaFree(c->d_spins2);
   delete c;
   return GASP_OK;
 }
@@ -964,9 +1030,10 @@ int gasp_cnn_get_params(gasp_cnn_t *c, float *params) {
 
 int gasp_cnn_predict_ex(gasp_cnn_t *c, const int8_t *spins, int batch, float *q_out,
                         float *mag_out) {
-  if (!c || !spins || !q_out || batch <= 0 || batch > c->max_batch) return GASP_ERR_INVALID;
+  if (!c || !spins || !q_out || batch <= 0) return GASP_ERR_INVALID;
   cudaStream_t s = current_stream();
   int rc;
+  if (batch > c->max_batch) return predict_chunked(c, spins, batch, q_out, mag_out, s);
   if ((rc = cnn_upload(c, spins, nullptr, batch))) return rc;
   if ((rc = cnn_forward(c, batch, s))) return rc;
   k_head<<<(batch + 7) / 8, 256, 0, s>>>(batch, c->N, c->d_pool, c->d_params, nullptr, c->d_q,

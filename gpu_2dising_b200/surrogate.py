@@ -72,18 +72,11 @@ class CommittorCNN:
         g = self._spins(grids)
         out = np.empty(g.shape[0], np.float32)
         mag = np.empty(g.shape[0], np.float32) if with_mag else None
-        for i in range(0, g.shape[0], self.max_batch):
-            chunk = np.ascontiguousarray(g[i:i + self.max_batch])
-            n = chunk.shape[0]
-            q = np.empty(n, np.float32)
-            if with_mag:
-                m = np.empty(n, np.float32)
-                check(lib().gasp_cnn_predict_ex(self._h, chunk.reshape(-1), n, q, m),
-                      "gasp_cnn_predict_ex")
-                mag[i:i + n] = m
-            else:
-                check(lib().gasp_cnn_predict(self._h, chunk.reshape(-1), n, q), "gasp_cnn_predict")
-            out[i:i + n] = q
+        if g.shape[0]:
+            # one call: chunks of max_batch, uploads overlapped with the network
+            check(lib().gasp_cnn_predict_ex(self._h, g.reshape(-1), g.shape[0], out,
+                                            mag.ctypes.data if with_mag else None),
+                  "gasp_cnn_predict_ex")
         return (out, mag) if with_mag else out
 
     def gradients(self, grids, labels):

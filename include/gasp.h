@@ -360,8 +360,11 @@ int gasp_cnn_free(gasp_cnn_t *cnn);
 int gasp_cnn_set_params(gasp_cnn_t *cnn, const float *params);  /* also resets Adam */
 int gasp_cnn_get_params(gasp_cnn_t *cnn, float *params);
 int gasp_cnn_predict(gasp_cnn_t *cnn, const int8_t *spins, int batch, float *q_out);
-/* The same, and (mag_out non-NULL) each grid's magnetisation from the
- * uploaded spins, for out-of-distribution checks before trusting q. */
+/* The same for any number of grids, and (mag_out non-NULL) each grid's
+ * magnetisation from the uploaded spins, for out-of-distribution checks
+ * before trusting q.  Batches above max_batch run in chunks of max_batch
+ * whose uploads overlap the previous chunk's network (the first such call
+ * allocates a second input buffer and a copy stream). */
 int gasp_cnn_predict_ex(gasp_cnn_t *cnn, const int8_t *spins, int batch, float *q_out,
                         float *mag_out);
 /* Loss (mean over the batch) and its gradient for labels in [0, 1]. */

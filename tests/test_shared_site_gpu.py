@@ -20,9 +20,10 @@ def device():
     return engine.init_device(0)
 
 
-@pytest.mark.parametrize("L,nsweeps", [(64, 2), (32, 3), (128, 1), (48, 2), (20, 3), (5, 6)])
-def test_shared_site_kernel_matches_serial_oracle(L, nsweeps):
-    n = 70  # two full tiles and one of six
+@pytest.mark.parametrize("L,nsweeps,n", [(64, 2, 70), (32, 3, 70), (128, 1, 70), (48, 2, 70),
+                                         (20, 3, 70), (5, 6, 70), (3, 4, 1)])
+def test_shared_site_kernel_matches_serial_oracle(L, nsweeps, n):
+    # n = 70: two full tiles and one of six; n = 1: a tile of one replica
     rs = np.random.default_rng(L)
     frac = rs.uniform(0.1, 0.9, size=(n, 1, 1))
     g0 = np.where(rs.random((n, L, L)) < frac, 1, -1).astype(np.int32)

@@ -60,9 +60,9 @@ def test_production_kernels_match_serial_oracle(L, variant):
         assert mag[r] == oracle.magnetisation_gpu(L, g.reshape(1, L, L))[0]
 
 
-@pytest.mark.parametrize("L,nsweeps", [(64, 2), (48, 2), (20, 3), (128, 1), (5, 4)])
-def test_warp_per_replica_kernel_matches_serial_oracle(L, nsweeps):
-    n = 37
+@pytest.mark.parametrize("L,nsweeps,n", [(64, 2, 37), (48, 2, 37), (20, 3, 37), (128, 1, 37),
+                                         (5, 4, 37), (3, 5, 3), (64, 1, 1)])
+def test_warp_per_replica_kernel_matches_serial_oracle(L, nsweeps, n):
     g0, st0, thr, g1, st1, mag = _run(L, n, 6, nsweeps, seed=100 + L)
     mul, inv = _lane_tables()
     for r in range(n):
