@@ -924,8 +924,13 @@ int committor_on_device(gasp_grids_t *g, gasp_rng_t *r, int tot, int mag_int, in
     ~DevBuf() {
       if (p) cudaFree(p);
     }
-  } fates_b, small_b;
+  } fates_b, small_b, act2_b, cnt_b;
   GASP_CUDA(cudaMalloc(&fates_b.p, (size_t)ngrids * sizeof(int)));
+  // the compaction writes survivors to the other list of a ping-pong pair
+  GASP_CUDA(cudaMalloc(&act2_b.p, (size_t)ngrids * sizeof(int)));
+  GASP_CUDA(cudaMalloc(&cnt_b.p, (size_t)(fate_compact_blocks(ngrids) + 1) * sizeof(int)));
+  int *act[2] = {x.d_active, static_cast<int *>(act2_b.p)};
+  int cur = 0;
   GASP_CUDA(cudaMalloc(&small_b.p, 64));
   int *d_fates = static_cast<int *>(fates_b.p);
   int *d_n = static_cast<int *>(small_b.p);
@@ -995,9 +1000,12 @@ int committor_on_device(gasp_grids_t *g, gasp_rng_t *r, int tot, int mag_int, in
       // sweeps from this check to the next one (or to the end of the run)
       long long span = 0;
       for (int j = isweep; j < tot && (j == isweep || j % mag_int != 0); j += spc) span += spc;
-      if ((rc = launch_fate_compact(g->d_mag, d_fates, x.d_active, d_n, up, dn, d_att,
+      if ((rc = launch_fate_compact(g->d_mag, d_fates, act[cur], act[cur ^ 1], d_n,
+                                    static_cast<int *>(cnt_b.p), ngrids, up, dn, d_att,
                                     (long long)N * span, s)))
         return rc;
+      cur ^= 1;
+      p.active = q.active = act[cur];
       if (++checks % kPollEvery == 0) {
         const int slot = (int)(polls_issued % kRing);
         GASP_CUDA(cudaMemcpyAsync(const_cast<int *>(hpoll) + slot, d_n, sizeof(int),

@@ -96,54 +96,95 @@ __global__ void __launch_bounds__(kCheckThreads)
 
 // Committor check on the device (the driver's itask-1 check, src/mc_gpu.cu:
 // 744-750): every active replica whose colvar is above up_thr (B) or below
-// dn_thr (A) gets its fate and leaves the active list (stable, in place, as
-// k_check_compact).  *attempts grows by the attempts of the sweep that
-// follows (survivors x attempts_per_replica).
-__global__ void __launch_bounds__(kCheckThreads)
-    k_fate_compact(const float *colvar, int *fates, int *active, int *n_active, double up_thr,
-                   double dn_thr, long long *attempts, long long attempts_per_replica) {
+// dn_thr (A) gets its fate and leaves the active list, which is compacted
+// stably from active_in to active_out by many CTAs in two kernels.
+// k_fate_count: each CTA takes 4096 consecutive entries, records the fates
+// and counts its survivors (cnt[b]); CTA 0 also keeps the live count it saw
+// in cnt[nblocks], so the scatter needs no read of *n_active while CTA 0
+// rewrites it.  k_fate_scatter: each CTA sums the counts of the CTAs before
+// it and writes its survivors, in order, at that offset; CTA 0 sets the new
+// count and adds the attempts of the sweep that follows (survivors x
+// attempts_per_replica).
+constexpr int kFateThreads = 1024;
+constexpr int kFatePer = 4;
+constexpr int kFateChunk = kFateThreads * kFatePer;
+
+__device__ __forceinline__ bool fate_keep(float colvar, double up_thr, double dn_thr) {
+  const double m = (double)colvar;
+  return !(m > up_thr) && !(m < dn_thr);
+}
+
+__global__ void __launch_bounds__(kFateThreads)
+    k_fate_count(const float *colvar, int *fates, const int *active, const int *n_active,
+                 double up_thr, double dn_thr, int *cnt) {
   __shared__ int warp_sums[32];
-  __shared__ int round_total;
-  __shared__ int out_base;
+  __shared__ int total;
   const int n = *n_active;
-  if (threadIdx.x == 0) out_base = 0;
-  __syncthreads();
-  for (int start = 0; start < n; start += kCheckThreads * kCheckPerThread) {
-    int ids[kCheckPerThread];
-    int keep = 0;
-    const int first = start + threadIdx.x * kCheckPerThread;
+  const int first = blockIdx.x * kFateChunk + threadIdx.x * kFatePer;
+  int keep = 0;
 #pragma unroll
-    for (int j = 0; j < kCheckPerThread; ++j) {
-      const int i = first + j;
-      int id = -1;
-      if (i < n) {
-        id = active[i];
-        const double m = (double)colvar[id];
-        if (m > up_thr) {
-          fates[id] = 1;
-          id = -1;
-        } else if (m < dn_thr) {
-          fates[id] = 0;
-          id = -1;
-        } else {
-          keep++;
-        }
-      }
-      ids[j] = id;
+  for (int j = 0; j < kFatePer; ++j) {
+    const int i = first + j;
+    if (i < n) {
+      const int id = active[i];
+      const double m = (double)colvar[id];
+      if (m > up_thr) fates[id] = 1;
+      else if (m < dn_thr) fates[id] = 0;
+      else ++keep;
     }
-    const int off = block_exclusive_scan(keep, warp_sums, &round_total);
-    const int base = out_base;
-    int o = base + off;
-#pragma unroll
-    for (int j = 0; j < kCheckPerThread; ++j)
-      if (ids[j] >= 0) active[o++] = ids[j];
-    __syncthreads();
-    if (threadIdx.x == 0) out_base = base + round_total;
-    __syncthreads();
   }
+  block_exclusive_scan(keep, warp_sums, &total);
   if (threadIdx.x == 0) {
-    *n_active = out_base;
-    *attempts += (long long)out_base * attempts_per_replica;
+    cnt[blockIdx.x] = total;
+    if (blockIdx.x == 0) cnt[gridDim.x] = n;
+  }
+}
+
+__global__ void __launch_bounds__(kFateThreads)
+    k_fate_scatter(const float *colvar, const int *active_in, int *active_out, int *n_active,
+                   const int *cnt, double up_thr, double dn_thr, long long *attempts,
+                   long long attempts_per_replica) {
+  __shared__ int warp_sums[32];
+  __shared__ int total;
+  __shared__ int base;
+  const int n = cnt[gridDim.x];
+  const int lane = threadIdx.x & 31;
+  if (threadIdx.x < 32) {  // survivors of the CTAs before this one
+    int sum = 0;
+    for (int b = lane; b < (int)blockIdx.x; b += 32) sum += cnt[b];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    if (lane == 0) base = sum;
+  }
+  const int first = blockIdx.x * kFateChunk + threadIdx.x * kFatePer;
+  int ids[kFatePer];
+  int keep = 0;
+#pragma unroll
+  for (int j = 0; j < kFatePer; ++j) {
+    const int i = first + j;
+    ids[j] = -1;
+    if (i < n) {
+      const int id = active_in[i];
+      if (fate_keep(colvar[id], up_thr, dn_thr)) {
+        ids[j] = id;
+        ++keep;
+      }
+    }
+  }
+  const int off = block_exclusive_scan(keep, warp_sums, &total);  // also orders `base`
+  int o = base + off;
+#pragma unroll
+  for (int j = 0; j < kFatePer; ++j)
+    if (ids[j] >= 0) active_out[o++] = ids[j];
+  if (blockIdx.x == 0 && threadIdx.x < 32) {
+    int sum = 0;
+    for (int b = lane; b < (int)gridDim.x; b += 32) sum += cnt[b];
+#pragma unroll
+    for (int o2 = 16; o2 > 0; o2 >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o2);
+    if (lane == 0) {
+      *n_active = sum;
+      *attempts += (long long)sum * attempts_per_replica;
+    }
   }
 }
 
@@ -154,11 +195,18 @@ __global__ void k_iota(int *a, int n) {
 
 }  // namespace
 
-int launch_fate_compact(const float *colvar, int *fates, int *active, int *n_active,
-                        double up_thr, double dn_thr, long long *attempts,
-                        long long attempts_per_replica, cudaStream_t s) {
-  k_fate_compact<<<1, kCheckThreads, 0, s>>>(colvar, fates, active, n_active, up_thr, dn_thr,
-                                             attempts, attempts_per_replica);
+int fate_compact_blocks(int max_active) { return (max_active + kFateChunk - 1) / kFateChunk; }
+
+int launch_fate_compact(const float *colvar, int *fates, const int *active_in, int *active_out,
+                        int *n_active, int *cnt, int max_active, double up_thr, double dn_thr,
+                        long long *attempts, long long attempts_per_replica, cudaStream_t s) {
+  const int nblk = fate_compact_blocks(max_active);
+  if (nblk <= 0) return GASP_OK;
+  k_fate_count<<<nblk, kFateThreads, 0, s>>>(colvar, fates, active_in, n_active, up_thr, dn_thr,
+                                             cnt);
+  GASP_CUDA(cudaGetLastError());
+  k_fate_scatter<<<nblk, kFateThreads, 0, s>>>(colvar, active_in, active_out, n_active, cnt,
+                                               up_thr, dn_thr, attempts, attempts_per_replica);
   GASP_CUDA(cudaGetLastError());
   return GASP_OK;
 }

@@ -99,10 +99,14 @@ SweepLaunch launch_for(gasp_grids_t *g, gasp_rng_t *r);
 int prepare_tables(gasp_grids_t *g, double beta, double h);
 
 // Device-side committor check + compaction (gasp_batch.cu): fates of active
-// replicas past a threshold, survivors compacted, attempts accumulated.
-int launch_fate_compact(const float *colvar, int *fates, int *active, int *n_active,
-                        double up_thr, double dn_thr, long long *attempts,
-                        long long attempts_per_replica, cudaStream_t s);
+// replicas past a threshold, survivors copied in order from active_in to
+// active_out (distinct arrays), count and attempts updated on the device.
+// max_active bounds *n_active; cnt holds fate_compact_blocks(max_active) + 1
+// ints of scratch.
+int fate_compact_blocks(int max_active);
+int launch_fate_compact(const float *colvar, int *fates, const int *active_in, int *active_out,
+                        int *n_active, int *cnt, int max_active, double up_thr, double dn_thr,
+                        long long *attempts, long long attempts_per_replica, cudaStream_t s);
 
 // Device-side check + compaction of one replica group (gasp_batch.cu).
 int launch_check_compact(const float *mag, int *active, int *n_active, int ngrids,
