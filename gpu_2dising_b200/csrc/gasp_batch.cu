@@ -489,7 +489,7 @@ int gasp_batch_autotune(gasp_batch_t *b, int nsweeps, int *choice_out) {
     gasp_grids_t *gr = b->grids[g];
     if ((rc = prepare_tables(gr, b->groups[g].beta, b->groups[g].h))) break;
     const int L = b->groups[g].L;
-    const bool rows = (L == 32 || L == 64 || L == 128);
+    const bool rows = (L == 32 || L == 64 || L == 96 || L == 128);
     // candidates: (variant, warps_per_cta)
     std::vector<std::pair<int, int>> cand;
     if (rows) cand = {{0, 1}, {2, 1}};

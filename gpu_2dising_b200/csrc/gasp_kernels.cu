@@ -298,11 +298,19 @@ __device__ __forceinline__ void row_attempt(uint32_t &s, Rng &rg, const char *la
                                             float shrink) {
   constexpr int N = L * L;
   constexpr int R = L / 32;
+  constexpr bool kPow2 = (L & (L - 1)) == 0;
   constexpr uint32_t kMask = (uint32_t)(4 * N - 1) & ~127u;  // word part of a byte offset
   const uint32_t b = s & 31u;
-  const uint32_t offc = ((s << 2) & kMask) | lane4;
-  const uint32_t offu = ((offc - 128u * R) & kMask) | lane4;
-  const uint32_t offd = ((offc + 128u * R) & kMask) | lane4;
+  uint32_t offc, offu, offd;
+  if constexpr (kPow2) {
+    offc = ((s << 2) & kMask) | lane4;
+    offu = ((offc - 128u * R) & kMask) | lane4;
+    offd = ((offc + 128u * R) & kMask) | lane4;
+  } else {  // rows of R words, R not a power of two: wrap by compare (4N bytes per tile)
+    offc = ((s << 2) & ~127u) | lane4;
+    offu = offc >= 128u * R ? offc - 128u * R : offc + (4u * N - 128u * R);
+    offd = offc + 128u * R < 4u * N ? offc + 128u * R : offc - (4u * N - 128u * R);
+  }
   const uint32_t wu = *reinterpret_cast<const uint32_t *>(latb + offu);
   const uint32_t wd = *reinterpret_cast<const uint32_t *>(latb + offd);
   uint32_t wc, lo, hi;
@@ -326,7 +334,8 @@ __device__ __forceinline__ void row_attempt(uint32_t &s, Rng &rg, const char *la
       hi = (b == 31u) ? wx : wc;
     }
   } else {
-    const uint32_t wi = (offc >> 7) & (uint32_t)(R - 1);
+    // word of the site within its row
+    const uint32_t wi = kPow2 ? (offc >> 7) & (uint32_t)(R - 1) : (s >> 5) % (uint32_t)R;
     const uint32_t offl = (b == 0u) ? (wi == 0u ? offc + 128u * (R - 1) : offc - 128u) : offc;
     const uint32_t offr =
         (b == 31u) ? (wi == (uint32_t)(R - 1) ? offc - 128u * (R - 1) : offc + 128u) : offc;
@@ -567,7 +576,8 @@ __global__ void __launch_bounds__(32) k_sweep_rows_pair(SweepLaunch p) {
 template <int L, bool kStatic, bool kFloatCmp, int kRng, bool kMask = false,
           bool kStoreAlways = false>
 __global__ void __launch_bounds__(32) k_sweep_rows(SweepLaunch p) {
-  static_assert(L % 32 == 0 && (L & (L - 1)) == 0, "L must be a power of two >= 32");
+  static_assert(L % 32 == 0, "rows of whole words");
+  static_assert(!kMask || (L & (L - 1)) == 0, "the acceptance-mask kernel needs L a power of two");
   static_assert(!(kMask && kFloatCmp), "the acceptance mask needs integer thresholds");
   constexpr int N = L * L;
   constexpr int W = N / 32;
@@ -845,6 +855,7 @@ int dispatch_kind(const SweepLaunch &p, cudaStream_t s) {
     return launch_tiles(p.L == 64 ? k_sweep_exact<64, F, K> : k_sweep_exact<0, F, K>, p, s);
   }
   const size_t dyn128 = (size_t)words_per_replica(128) * kTile * sizeof(uint32_t);
+  const size_t dyn96 = (size_t)words_per_replica(96) * kTile * sizeof(uint32_t);
   if (p.variant == 3) {  // row kernel with pairwise speculation (measured slower)
     switch (p.L) {
       case 32: return launch_rows(k_sweep_rows_pair<32, true, F, K>, p, 0, s);
@@ -865,6 +876,7 @@ int dispatch_kind(const SweepLaunch &p, cudaStream_t s) {
     switch (p.L) {
       case 32: return launch_rows(k_sweep_rows<32, true, F, K, false, true>, p, 0, s);
       case 64: return launch_rows(k_sweep_rows<64, true, F, K, false, true>, p, 0, s);
+      case 96: return launch_rows(k_sweep_rows<96, false, F, K, false, true>, p, dyn96, s);
       case 128: return launch_rows(k_sweep_rows<128, false, F, K, false, true>, p, dyn128, s);
       default: break;
     }
@@ -876,7 +888,7 @@ int dispatch_kind(const SweepLaunch &p, cudaStream_t s) {
                                    : launch_tiles(k_sweep_exact<48, F, K>, p, s);
     case 64: return launch_rows(k_sweep_rows<64, true, F, K>, p, 0, s);
     case 96: return p.variant == 5 ? launch_tiles(k_sweep_exact<96, F, K, true>, p, s)
-                                   : launch_tiles(k_sweep_exact<96, F, K>, p, s);
+                                   : launch_rows(k_sweep_rows<96, false, F, K>, p, dyn96, s);
     case 128: return launch_rows(k_sweep_rows<128, false, F, K>, p, dyn128, s);
     default: return launch_tiles(k_sweep_exact<0, F, K>, p, s);
   }

@@ -113,13 +113,13 @@ int gasp_grids_shape(const gasp_grids_t *grids, int *L_out, int *ngrids_out);
 /* Launch tuning of a set (no reference counterpart; results never depend on
  * it, except that variant 6 and GASP_OPT_TAIL_REPLICAS assign the MWC64X
  * stream's draws to attempts differently: same dynamics, other trajectories).  GASP_OPT_SWEEP_VARIANT: 0 the fastest kernel for L (default: for
- * L = 32, 64, 128 the row kernel writing the centre word back on every
+ * L = 32, 64, 96, 128 the row kernel writing the centre word back on every
  * attempt, no divergent branch), 1 the generic kernel, 2 the row kernel with a
  * store only on acceptance, 3 the row kernel with pairwise
  * speculation of consecutive attempts, 4 the row kernel with the acceptance
  * decided by a per-draw mask of accepted neighbourhoods (falls back to 2 when
- * more than six classes can reject), 5 the generic kernel (L other than 32,
- * 64, 128) writing the centre word back on every attempt, 6 one warp per
+ * more than six classes can reject; L = 32, 64, 128 only), 5 the generic
+ * kernel writing the centre word back on every attempt, 6 one warp per
  * replica (MWC64X stream only, 3 <= L <= 512; GASP_ERR_UNSUPPORTED otherwise):
  * the warp applies up to 32 queued attempts of its replica per step, all
  * those that touch no site or neighbour of another, in the order drawn --
