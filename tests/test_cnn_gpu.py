@@ -60,6 +60,29 @@ def test_gradients_match_oracle():
             assert cos > 0.999, (name, cos)
 
 
+@pytest.mark.parametrize("Lo", [32, 128])
+def test_other_sizes_forward_and_gradients_match_oracle(Lo):
+    """The window convolutions at the other lattice sides with a row-aligned
+    tile (a 128-pixel tile is 4 rows of 32 or 1 row of 128): forward and the
+    loss gradient against the FP64 oracle."""
+    rs = np.random.default_rng(Lo)
+    f = rs.uniform(0.1, 0.9, size=3)
+    g = np.where(rs.random((3, Lo, Lo)) < f[:, None, None], 1, -1).astype(np.int8)
+    y = (1.0 / (1.0 + np.exp(-6.0 * g.reshape(3, -1).mean(axis=1)))).astype(np.float32)
+    params = surrogate.init_params(9)
+    params[-33:] = np.random.default_rng(1).normal(0, 0.5, 33).astype(np.float32)
+    net = surrogate.CommittorCNN(Lo, 4, params)
+    q = net.predict(g)
+    ref = ocnn.forward(params.astype(np.float64), g.astype(np.float64), bf16=True)["q"]
+    assert np.max(np.abs(q - ref)) < 2e-3, (q, ref)
+    loss, grad = net.gradients(g, y)
+    rloss, rgrad, _ = ocnn.loss_and_grads(params.astype(np.float64), g.astype(np.float64),
+                                          y.astype(np.float64), bf16=True)
+    assert abs(loss - rloss) < 1e-3 * max(1.0, abs(rloss))
+    rel = np.linalg.norm(grad - rgrad) / np.linalg.norm(rgrad)
+    assert rel < 2e-2, rel
+
+
 def test_training_learns():
     g, y = _data(512, 3)
     gv, yv = _data(128, 4)
