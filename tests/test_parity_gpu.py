@@ -55,6 +55,11 @@ CASES = [  # L, ngrids, method, init, beta, h, nsweeps, ncalls
     (20, 35, 2, "random", 0.50, -0.20, 2, 2),
     (96, 32, 2, "random", 0.44, 0.00, 1, 1),
     (128, 40, 2, "sparse", 0.55, 0.05, 1, 1),
+    (8, 33, 2, "random", 0.54, 0.07, 4, 2),
+    (8, 1, 1, "random", 0.40, 0.10, 3, 2),
+    (64, 1, 2, "random", 0.54, 0.07, 2, 2),
+    (96, 65, 0, "sparse", 0.54, -0.07, 1, 2),
+    (96, 1, 1, "random", 0.60, 0.10, 1, 1),
 ]
 
 
