@@ -364,6 +364,78 @@ __device__ __forceinline__ void row_attempt(uint32_t &s, Rng &rg, const char *la
   }
 }
 
+// row_attempt split in two for k_sweep_rows2: the probe (loads, pattern,
+// acceptance, the draws) returns the byte offset of the site's word and its new
+// value; the caller stores it.  Same arithmetic and draw order.
+template <int L, bool kFloatCmp, bool kLookahead, typename Rng>
+__device__ __forceinline__ void row_probe(uint32_t &s, Rng &rg, const char *latb, const char *thrb,
+                                          const char *paccb, uint32_t lane4, float shrink,
+                                          uint32_t &off_out, uint32_t &word_out) {
+  constexpr int N = L * L;
+  constexpr int R = L / 32;
+  constexpr bool kPow2 = (L & (L - 1)) == 0;
+  constexpr uint32_t kMask = (uint32_t)(4 * N - 1) & ~127u;  // word part of a byte offset
+  const uint32_t b = s & 31u;
+  uint32_t offc, offu, offd;
+  if constexpr (kPow2) {
+    offc = ((s << 2) & kMask) | lane4;
+    offu = ((offc - 128u * R) & kMask) | lane4;
+    offd = ((offc + 128u * R) & kMask) | lane4;
+  } else {  // rows of R words, R not a power of two: wrap by compare (4N bytes per tile)
+    offc = ((s << 2) & ~127u) | lane4;
+    offu = offc >= 128u * R ? offc - 128u * R : offc + (4u * N - 128u * R);
+    offd = offc + 128u * R < 4u * N ? offc + 128u * R : offc - (4u * N - 128u * R);
+  }
+  const uint32_t wu = *reinterpret_cast<const uint32_t *>(latb + offu);
+  const uint32_t wd = *reinterpret_cast<const uint32_t *>(latb + offd);
+  uint32_t wc, lo, hi;
+  if constexpr (R == 1) {
+    wc = *reinterpret_cast<const uint32_t *>(latb + offc);
+    lo = hi = wc;
+  } else if constexpr (R == 2) {
+    wc = *reinterpret_cast<const uint32_t *>(latb + offc);
+    const uint32_t wx = *reinterpret_cast<const uint32_t *>(latb + (offc ^ 128u));
+    if constexpr (Rng::kKind == kRngXorwow) {
+      // The row is the circular 64 bits (wx:wc) seen from the site's word: for
+      // b >= 3 the bits b-1..b+1 sit in (wx:wc) >> (b-3) (b = 31 reaches wx
+      // bit 0); for b < 3 the left neighbour wraps to the top of wx, so the
+      // pair is read as (wc:wx), whose shift by b+29 lands on the same bits.
+      // One compare instead of two: 4.23e11 vs 4.11e11 attempts/s.
+      const bool wrap = b < 3u;
+      lo = wrap ? wx : wc;
+      hi = wrap ? wc : wx;
+    } else {  // with the MWC64X stream the two-compare form schedules better (4.96e11 vs 4.89e11)
+      lo = (b == 0u) ? wx : wc;
+      hi = (b == 31u) ? wx : wc;
+    }
+  } else {
+    // word of the site within its row
+    const uint32_t wi = kPow2 ? (offc >> 7) & (uint32_t)(R - 1) : (s >> 5) % (uint32_t)R;
+    const uint32_t offl = (b == 0u) ? (wi == 0u ? offc + 128u * (R - 1) : offc - 128u) : offc;
+    const uint32_t offr =
+        (b == 31u) ? (wi == (uint32_t)(R - 1) ? offc - 128u * (R - 1) : offc + 128u) : offc;
+    lo = *reinterpret_cast<const uint32_t *>(latb + offl);
+    hi = *reinterpret_cast<const uint32_t *>(latb + offr);
+    wc = (b == 0u) ? hi : lo;
+  }
+  const uint32_t t = __funnelshift_r(lo, hi, b + 29u);  // bits 2,3,4: left, centre, right
+  const uint32_t u = __funnelshift_r(wu, wu, b + 27u);  // bit 5: up
+  const uint32_t d = __funnelshift_r(wd, wd, b + 26u);  // bit 6: down
+  const uint32_t p4 = (t & 0x1Cu) | (u & 0x20u) | (d & 0x40u);
+  const uint32_t x2 = rg.next();
+  const uint32_t sc = s;
+  if constexpr (kLookahead) s = rg.template site<N>(shrink, N);
+  bool acc;
+  if constexpr (kFloatCmp) {
+    acc = _curand_uniform(x2) < *reinterpret_cast<const float *>(paccb + p4);
+  } else {
+    acc = x2 <= *reinterpret_cast<const uint32_t *>(thrb + p4);
+  }
+  off_out = offc;
+  word_out = acc ? wc ^ (1u << (sc & 31u)) : wc;  // written back unchanged when rejected
+}
+
+
 // row_attempt with the threshold lookup taken off the dependency chain.  For
 // the raw acceptance draw x2, the accepted classes are those whose threshold
 // is >= x2; with the classes sorted by threshold that is a suffix of the
@@ -662,6 +734,85 @@ __global__ void __launch_bounds__(32) k_sweep_rows(SweepLaunch p) {
   stage_out(lat, p, W, tile, lane, live, rep);
 }
 
+// Two tiles per warp: each lane sweeps one replica of tile 2b and one of tile
+// 2b+1, the two attempts of a step probed before either is stored, so the
+// two replicas' dependency chains overlap in one thread (instruction-level
+// parallelism in place of a second warp on the scheduler).  Per replica the
+// attempts and draws are exactly those of k_sweep_rows.  Lanes without a
+// replica in the second tile sweep a zeroed scratch copy and store nothing
+// back.
+template <int L, bool kStatic, bool kFloatCmp, int kRng>
+__global__ void __launch_bounds__(32) k_sweep_rows2(SweepLaunch p) {
+  static_assert(L % 32 == 0, "rows of whole words");
+  constexpr int N = L * L;
+  constexpr int W = N / 32;
+  __shared__ __align__(16) uint32_t thrP[32];
+  __shared__ __align__(16) float paccP[32];
+  extern __shared__ __align__(16) uint32_t dyn[];
+  uint32_t *lat = LatticeStore<2 * W * kTile, kStatic>::get(dyn);
+
+  const int lane = threadIdx.x;
+  {
+    const int c = (lane >> 1) & 1;
+    const int cls = 5 * c + __popc(lane & 0x1D);
+    thrP[lane] = p.thr[cls];
+    paccP[lane] = p.pacc_f[2 * cls];
+  }
+  const int n_act = live_count(p);
+  const int tileA = 2 * blockIdx.x, tileB = tileA + 1;
+  if (tileA * kTile >= n_act) return;  // whole CTA idle this batch
+  const int slotA = tileA * kTile + lane, slotB = tileB * kTile + lane;
+  const bool liveA = slotA < n_act, liveB = slotB < n_act;
+  const int repA = liveA ? (p.active ? p.active[slotA] : slotA) : 0;
+  const int repB = liveB ? (p.active ? p.active[slotB] : slotB) : 0;
+  uint32_t *latA = lat, *latB = lat + W * kTile;
+  const bool tileB_live = tileB * kTile < n_act;
+  stage_in(latA, p, W, tileA, lane, liveA, repA);
+  if (tileB_live) {
+    stage_in(latB, p, W, tileB, lane, liveB, repB);
+  } else {
+    for (int w = 0; w < W; ++w) latB[w * kTile + lane] = 0u;
+  }
+  __syncwarp();
+
+  char *latbA = reinterpret_cast<char *>(latA);
+  char *latbB = reinterpret_cast<char *>(latB);
+  const char *thrb = reinterpret_cast<const char *>(thrP);
+  const char *paccb = reinterpret_cast<const char *>(paccP);
+  if (liveA && p.nsweeps > 0) {
+    RngPolicy<kRng> ra, rb;
+    ra.load(p.rng, p.rng_stride, repA);
+    if (liveB) rb.load(p.rng, p.rng_stride, repB);
+    else rb.load(p.rng, p.rng_stride, repA);  // a stand-in stream; nothing of B is kept
+    const float shrink = (1.0f - FLT_EPSILON) * (float)N;
+    const uint32_t lane4 = (uint32_t)lane << 2;
+    uint32_t sa = ra.template site<N>(shrink, N);
+    uint32_t sb = rb.template site<N>(shrink, N);
+    const int total = N * p.nsweeps;
+    uint32_t oa, wa, ob, wb;
+#pragma unroll 2
+    for (int a = 0; a < total - 1; ++a) {
+      row_probe<L, kFloatCmp, true>(sa, ra, latbA, thrb, paccb, lane4, shrink, oa, wa);
+      row_probe<L, kFloatCmp, true>(sb, rb, latbB, thrb, paccb, lane4, shrink, ob, wb);
+      *reinterpret_cast<uint32_t *>(latbA + oa) = wa;
+      *reinterpret_cast<uint32_t *>(latbB + ob) = wb;
+    }
+    row_probe<L, kFloatCmp, false>(sa, ra, latbA, thrb, paccb, lane4, shrink, oa, wa);
+    row_probe<L, kFloatCmp, false>(sb, rb, latbB, thrb, paccb, lane4, shrink, ob, wb);
+    *reinterpret_cast<uint32_t *>(latbA + oa) = wa;
+    *reinterpret_cast<uint32_t *>(latbB + ob) = wb;
+    ra.store(p.rng, p.rng_stride, repA);
+    if (liveB) rb.store(p.rng, p.rng_stride, repB);
+  }
+  __syncwarp();
+  epilogue_mag(latA + lane, p, N, W, liveA, repA);
+  stage_out(latA, p, W, tileA, lane, liveA, repA);
+  if (tileB_live) {
+    epilogue_mag(latB + lane, p, N, W, liveB, repB);
+    stage_out(latB, p, W, tileB, lane, liveB, repB);
+  }
+}
+
 // ---------------------------------------------------------------------------
 // CPU-trace sweep: mc_sweep_cpu arithmetic (src/mc_cpu.c:41-89) on a replayed
 // stream of doubles (row-u, col-u, xi) per attempt.
@@ -841,6 +992,18 @@ int launch_rows(Kern kern, const SweepLaunch &p, size_t dyn_smem, cudaStream_t s
   return GASP_OK;
 }
 
+// k_sweep_rows2: one warp per CTA and two tiles per warp.
+template <typename Kern>
+int launch_rows2(Kern kern, const SweepLaunch &p, size_t dyn_smem, cudaStream_t s) {
+  const int tiles = tiles_for(p.n_active);
+  if (tiles == 0) return GASP_OK;
+  if (dyn_smem > 0)
+    GASP_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_smem));
+  kern<<<(tiles + 1) / 2, 32, dyn_smem, s>>>(p);
+  GASP_CUDA(cudaGetLastError());
+  return GASP_OK;
+}
+
 template <bool F, int K>
 int dispatch_kind(const SweepLaunch &p, cudaStream_t s) {
   if (p.lattice_in_global) {
@@ -848,6 +1011,16 @@ int dispatch_kind(const SweepLaunch &p, cudaStream_t s) {
     k_sweep_global<F, K><<<(p.n_active + 127) / 128, 128, 0, s>>>(p);
     GASP_CUDA(cudaGetLastError());
     return GASP_OK;
+  }
+  if (p.variant == 8) {  // two tiles per warp
+    switch (p.L) {
+      case 32: return launch_rows2(k_sweep_rows2<32, true, F, K>, p, 0, s);
+      case 64: return launch_rows2(k_sweep_rows2<64, false, F, K>, p,
+                                   2 * (size_t)words_per_replica(64) * kTile * 4, s);
+      case 128: return launch_rows2(k_sweep_rows2<128, false, F, K>, p,
+                                    2 * (size_t)words_per_replica(128) * kTile * 4, s);
+      default: break;  // other L: the default kernels
+    }
   }
   if (p.variant == 6) return launch_sweep_tail(p, s);    // one warp per replica (MWC64X)
   if (p.variant == 7) return launch_sweep_shared(p, s);  // shared site per tile (MWC64X)

@@ -130,7 +130,9 @@ int gasp_grids_shape(const gasp_grids_t *grids, int *L_out, int *ngrids_out);
  * list; GASP_ERR_UNSUPPORTED otherwise): the 32 replicas of a tile share each
  * attempt's site, held as one word per site, neighbour counts by bitwise
  * full adders, per-replica acceptance draws, a ballot flip mask -- replicas
- * of a tile are correlated; about half the throughput of variant 0.
+ * of a tile are correlated; about half the throughput of variant 0; 8 the
+ * row kernel with two tiles per warp (L = 32, 64, 128; each lane runs the
+ * two replicas' attempts interleaved; bit-identical to 0, measured slower).
  * GASP_OPT_WARPS_PER_CTA: tiles per CTA of the generic kernel (1..8).
  * GASP_OPT_TAIL_REPLICAS: device-side committor shooting (itask 1 with
  * compaction) on the MWC64X stream sweeps with variant 6 once at most this

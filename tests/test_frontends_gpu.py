@@ -159,15 +159,16 @@ def test_cli_committor_reads_gridinput(ref_gpu, tmp_path):
 @pytest.mark.parametrize("beta,h", [(0.45, 0.1), (0.5, 0.0), (1e-9, 0.1)])
 def test_kernel_variants_agree(L, kind, beta, h):
     """The generic (with and without the every-attempt store), row,
-    pairwise-speculative and acceptance-mask kernels give identical results for
-    both RNG kinds.  h = 0 leaves six classes that can
+    pairwise-speculative, acceptance-mask and two-tiles-per-warp kernels give
+    identical results for both RNG kinds (96 replicas: the last warp of the
+    two-tile kernel has one tile).  h = 0 leaves six classes that can
     reject (the most the mask kernel takes); at beta = 1e-9 every P rounds to
     1.0, ten classes can reject and the mask variant falls back to the row
     kernel."""
     ng, seed = 96, 31 + L
     g0 = np.where(np.random.default_rng(seed).random((ng, L, L)) < 0.3, 1, -1).astype(np.int32)
     outs = []
-    for variant in (0, 1, 2, 3, 4, 5):
+    for variant in (0, 1, 2, 3, 4, 5, 8):
         dg = engine.DeviceGrids(L, ng, g0)
         dg.set_option(1, variant)
         r = engine.RngStates(ng, seed, kind=kind)
