@@ -182,6 +182,9 @@ __global__ void __launch_bounds__(256) k_sweep_exact(SweepLaunch p) {
     rg.load(p.rng, p.rng_stride, rep);
     const float shrink = (1.0f - FLT_EPSILON) * (float)N;
     for (int sw = 0; sw < p.nsweeps; ++sw) {
+      // unroll 4: 1.2-1.5x over the compiler's choice on the reference stream
+      // (L=48: 2.45e11 vs 2.04e11 attempts/s at 32768 replicas; L=100: 3.3e10 vs 2.2e10)
+#pragma unroll 4
       for (int a = 0; a < N; ++a) {
         const int s = (int)rg.template site<(L_ > 0 ? L_ * L_ : 0)>(shrink, N);
         const int row = s / L;
