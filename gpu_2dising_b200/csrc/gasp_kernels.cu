@@ -242,6 +242,9 @@ __global__ void __launch_bounds__(128) k_sweep_global(SweepLaunch p) {
   rg.load(p.rng, p.rng_stride, rep);
   const float shrink = (1.0f - FLT_EPSILON) * (float)N;
   for (int sw = 0; sw < p.nsweeps; ++sw) {
+    // unroll 4: L=300, 2048 replicas, 4.3e9 vs 2.4e9 attempts/s (exact stream),
+    // 4.4e9 vs 3.7e9 (MWC64X)
+#pragma unroll 4
     for (int a = 0; a < N; ++a) {
       const int s = (int)rg.template site<0>(shrink, N);
       const int row = s / L;
