@@ -962,13 +962,28 @@ __global__ void k_unpack_grids(const uint32_t *lat, int *g, int L, int ngrids, l
 
 // gridstates.bin payload, N % 32 == 0: output word k is lattice word
 // (rep = k / W, w = k % W): a per-tile transpose.
-__global__ void k_pack_frame32(const uint32_t *lat, uint32_t *out, int W, long long nwords) {
-  const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= nwords) return;
-  const long long rep = k / W;
-  const int w = (int)(k % W);
-  out[k] = lat[(rep >> 5) * W * kTile + (size_t)w * kTile + (rep & 31)];
+// gridstates.bin payload for L*L % 32 == 0: replica r's word w is word w of
+// lane r%32 of tile r/32.  Each 32 x 8 block moves a 32-word x 32-replica
+// square through a padded shared array: the tile's words are read as
+// 128-byte rows, and each replica's 32 words are written as one 128-byte run.
+__global__ void __launch_bounds__(256) k_pack_frame32t(const uint32_t *lat, uint32_t *out, int W,
+                                                        int ngrids, int nchunks) {
+  __shared__ uint32_t sq[32][33];
+  const int tile = (int)(blockIdx.x / (unsigned)nchunks);
+  const int w0 = (int)(blockIdx.x % (unsigned)nchunks) * 32;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
+  const uint32_t *src = lat + (size_t)tile * W * kTile;
+#pragma unroll
+  for (int j = ty; j < 32; j += 8)
+    if (w0 + j < W) sq[j][tx] = src[(size_t)(w0 + j) * kTile + tx];
+  __syncthreads();
+#pragma unroll
+  for (int j = ty; j < 32; j += 8) {  // j: replica of the tile, tx: word of the square
+    const int rep = tile * kTile + j;
+    if (rep < ngrids && w0 + tx < W) out[(size_t)rep * W + w0 + tx] = sq[tx][j];
+  }
 }
+
 
 // General payload: one thread per output byte, bit cursor over all spins.
 __global__ void k_pack_frame8(const uint32_t *lat, uint8_t *out, int L, long long nbits,
@@ -1174,9 +1189,14 @@ int launch_pack_frame(const uint32_t *lat, uint8_t *frame, int L, int ngrids, cu
   const long long nbits = N * ngrids;
   if (nbits == 0) return GASP_OK;
   if (N % 32 == 0) {
-    const long long nwords = nbits / 32;
-    k_pack_frame32<<<(unsigned)((nwords + 255) / 256), 256, 0, s>>>(
-        lat, reinterpret_cast<uint32_t *>(frame), (int)(N / 32), nwords);
+    const int W = (int)(N / 32), nchunks = (W + 31) / 32;
+    const long long blocks = (long long)tiles_for(ngrids) * nchunks;
+    if (blocks > 0x7fffffffLL) {
+      set_error("gridstates frame of %d replicas of L=%d is too large to pack", ngrids, L);
+      return GASP_ERR_UNSUPPORTED;
+    }
+    k_pack_frame32t<<<(unsigned)blocks, 256, 0, s>>>(lat, reinterpret_cast<uint32_t *>(frame), W,
+                                                      ngrids, nchunks);
   } else {
     const long long nbytes = (nbits + 7) / 8;
     k_pack_frame8<<<(unsigned)((nbytes + 255) / 256), 256, 0, s>>>(lat, frame, L, nbits, nbytes);

@@ -215,7 +215,8 @@ def test_committor_on_device_matches_reference_driver(ref_gpu, case, mag_grid):
     assert np.array_equal(dg.download(), dg2.download())
 
 
-@pytest.mark.parametrize("L,ng", [(5, 7), (16, 33), (64, 64), (30, 65)])
+@pytest.mark.parametrize("L,ng", [(5, 7), (16, 33), (64, 64), (30, 65), (48, 70), (32, 1),
+                                  (64, 32768)])
 def test_pack_unpack_frame_and_magnetisation(L, ng):
     g = _grids(L, ng, "random", L + ng)
     dg = engine.DeviceGrids(L, ng, g)
