@@ -856,13 +856,27 @@ int cnn_check_err(gasp_cnn *c, cudaStream_t s) {
 // the host-to-device copies hide behind the convolutions.
 int predict_chunked(gasp_cnn *c, const int8_t *spins, int batch, float *q_out, float *mag_out,
                     cudaStream_t s) {
-  if (!c->copy_stream) {
-    GASP_CUDA(cudaMalloc(&c->d_spins2, (size_t)c->max_batch * c->N));
-    GASP_CUDA(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
-    for (int i = 0; i < 2; ++i) {
-      GASP_CUDA(cudaEventCreateWithFlags(&c->ev_copied[i], cudaEventDisableTiming));
-      GASP_CUDA(cudaEventCreateWithFlags(&c->ev_used[i], cudaEventDisableTiming));
+  if (!c->copy_stream) {  // first chunked call: all four pieces, or none of them
+    int8_t *buf = nullptr;
+    cudaStream_t cs = nullptr;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaError_t e = cudaMalloc(&buf, (size_t)c->max_batch * c->N);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+    for (int i = 0; i < 4 && e == cudaSuccess; ++i)
+      e = cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming);
+    if (e != cudaSuccess) {
+      for (cudaEvent_t x : ev)
+        if (x) cudaEventDestroy(x);
+      if (cs) cudaStreamDestroy(cs);
+      cudaFree(buf);
+      return cuda_fail(e, "gasp_cnn_predict_ex chunk buffers", __FILE__, __LINE__);
     }
+    c->d_spins2 = buf;
+    c->ev_copied[0] = ev[0];
+    c->ev_copied[1] = ev[1];
+    c->ev_used[0] = ev[2];
+    c->ev_used[1] = ev[3];
+    c->copy_stream = cs;
   }
   cudaStream_t cs = c->copy_stream;
   int8_t *buf[2] = {c->d_spins, c->d_spins2};
