@@ -60,6 +60,11 @@ CASES = [  # L, ngrids, method, init, beta, h, nsweeps, ncalls
     (64, 1, 2, "random", 0.54, 0.07, 2, 2),
     (96, 65, 0, "sparse", 0.54, -0.07, 1, 2),
     (96, 1, 1, "random", 0.60, 0.10, 1, 1),
+    # beta = 3: the most costly class can never accept (P below the smallest
+    # uniform), so the kernels compare in float instead of by threshold
+    (64, 40, 2, "random", 3.0, 0.10, 2, 2),
+    (48, 33, 0, "random", 3.0, -0.20, 2, 1),
+    (128, 32, 1, "sparse", 3.0, 0.05, 1, 1),
 ]
 
 
@@ -271,3 +276,11 @@ def test_errors_are_raised_not_hidden():
         dg.sweep(r, 0.5, 0.1, 1)  # fewer RNG states than replicas
     with pytest.raises(GaspError):
         dg.sweep(engine.RngStates(64, 1), 0.5, 0.1, 1, gpu_method=3)
+
+
+def test_float_comparison_switch_is_reported():
+    """At beta = 3 some class can never accept and the set reports the float
+    comparison; at beta = 0.54 the integer thresholds are exact."""
+    dg = engine.DeviceGrids(64, 32)
+    assert dg.thresholds(3.0, 0.10)[1] is True
+    assert dg.thresholds(0.54, 0.07)[1] is False
