@@ -145,19 +145,29 @@ def _check_cv(cv, up, dn):
                       "magnitudes >= 2", UserWarning, stacklevel=3)
 
 
+def _rng_kind(rng):
+    if rng not in ("xorwow", "mwc64x"):
+        raise ValueError(f"rng must be 'xorwow' or 'mwc64x' (got {rng!r})")
+    return rng
+
+
 def run_nucleation_swarm(L, ngrid, tot_nsweeps, beta, h, initial_spin=-1, cv="magnetisation",
                          up_threshold=0.90, dn_threshold=-0.95, mag_output_int=100,
                          grid_output_int=1000, keep_grids=True, max_keep_grids=0,
-                         threadsPerBlock=32, gpu_method=0, seed=None, verbose=False):
+                         threadsPerBlock=32, gpu_method=0, seed=None, verbose=False,
+                         rng="xorwow"):
     """Simulate a swarm of ngrid LxL replicas from a uniform ``initial_spin``
     start; returns float32[tot_nsweeps // mag_output_int], the fraction of
     replicas with cv > up_threshold at each check (src/ising_ext.cu:522-743).
     Default thresholds are those of the reference (computed there from the
-    default initial_spin=-1: up 0.90, dn -0.95)."""
+    default initial_spin=-1: up 0.90, dn -0.95).  rng: "xorwow" (the
+    reference's cuRAND stream, bit-identical trajectories) or "mwc64x" (the
+    production stream: statistically equivalent, faster)."""
     _check_cv(cv, up_threshold, dn_threshold)
     if max_keep_grids < 0:
         raise ValueError("max_keep_grids must be a positive integer")
     _require_device()
+    _rng_kind(rng)
     if os.path.exists("gridstates.bin"):
         os.remove("gridstates.bin")
     _reset_lists()
@@ -168,7 +178,7 @@ def run_nucleation_swarm(L, ngrid, tot_nsweeps, beta, h, initial_spin=-1, cv="ma
     engine.select_gpu_method(L, ngrid, threadsPerBlock)  # evaluated, then ignored (as :678)
     seed = int(time.time()) if seed is None else int(seed)
     dg = engine.DeviceGrids(L, ngrid, host)
-    rng = engine.RngStates(ngrid, seed)
+    rng = engine.RngStates(ngrid, seed, kind=_rng_kind(rng))
     try:
         res, _, _, _ = engine.run_driver(
             dg, rng, beta, h, tot_nsweeps, mag_output_int, grid_output_int, itask=0,
@@ -187,10 +197,12 @@ def run_committor_calc(L, ngrid, tot_nsweeps, beta, h, initial_spin=-1, cv="magn
                        up_threshold=0.90, dn_threshold=-0.93, mag_output_int=100,
                        grid_output_int=1000, keep_grids=True, max_keep_grids=0,
                        threadsPerBlock=32, gpu_method=0, grid_input="gridstates.bin",
-                       grid_array=None, nsms=None, seed=None, compact=False, verbose=False):
+                       grid_array=None, nsms=None, seed=None, compact=False, verbose=False,
+                       rng="xorwow"):
     """Committor pB of each input grid by shooting ngrid/len(grid_array)
     trajectories per input until cv > up_threshold (B) or < dn_threshold (A);
-    returns [(pB, bootstrap error), ...] (src/ising_ext.cu:805-1130)."""
+    returns [(pB, bootstrap error), ...] (src/ising_ext.cu:805-1130).  rng as
+    for run_nucleation_swarm."""
     global gpu_nsms
     if nsms is None:
         nsms = gpu_nsms
@@ -225,6 +237,7 @@ def run_committor_calc(L, ngrid, tot_nsweeps, beta, h, initial_spin=-1, cv="magn
                 raise ValueError("Each grid_array item must have shape LxL")
             arrs.append(a.astype(np.int32))
     _require_device()
+    _rng_kind(rng)
     if os.path.exists("gridstates.bin"):
         os.remove("gridstates.bin")
     _reset_lists()
@@ -246,7 +259,7 @@ def run_committor_calc(L, ngrid, tot_nsweeps, beta, h, initial_spin=-1, cv="magn
     engine.select_gpu_method(L, ngrid, threadsPerBlock)
     seed = int(time.time()) if seed is None else int(seed)
     dg = engine.DeviceGrids(L, ngrid, host)
-    rng = engine.RngStates(ngrid, seed)
+    rng = engine.RngStates(ngrid, seed, kind=_rng_kind(rng))
     try:
         res, fates, _, _ = engine.run_driver(
             dg, rng, beta, h, tot_nsweeps, mag_output_int, grid_output_int, itask=1,

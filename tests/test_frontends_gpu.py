@@ -109,6 +109,25 @@ def test_pygasp_validation(gasp_mod):
                                     grid_array=[np.zeros((8, 8), np.int8)], nsms=4)
     with pytest.raises(ValueError):
         gasp_mod.run_committor_calc(16, 32, 10, 0.5, 0.1, nsms=-1)
+    with pytest.raises(ValueError):
+        gasp_mod.run_nucleation_swarm(16, 32, 10, 0.5, 0.1, rng="philox")
+
+
+def test_pygasp_production_stream(gasp_mod, tmp_path, monkeypatch):
+    """rng="mwc64x" runs both entry points on the production stream: a swarm
+    is reproducible per seed, and the committor of an all-up and an
+    all-down grid is exact."""
+    monkeypatch.chdir(tmp_path)
+    a = gasp_mod.run_nucleation_swarm(32, 64, 200, 0.5, 0.12, seed=5, rng="mwc64x",
+                                      keep_grids=False)
+    b = gasp_mod.run_nucleation_swarm(32, 64, 200, 0.5, 0.12, seed=5, rng="mwc64x",
+                                      keep_grids=False)
+    assert np.array_equal(a, b)
+    grids = [np.ones((16, 16), np.int8), -np.ones((16, 16), np.int8)]
+    out = gasp_mod.run_committor_calc(16, 64, 100, 0.54, 0.07, grid_input="NumPy",
+                                      grid_array=grids, nsms=2, seed=3, rng="mwc64x",
+                                      keep_grids=False)
+    assert [round(float(p), 6) for p, _ in out] == [1.0, 0.0]
 
 
 def test_cli_swarm_matches_reference(ref_gpu, tmp_path):
