@@ -382,7 +382,7 @@ int gasp_grids_download(gasp_grids_t *g, int *host_grids) {
 int gasp_grids_set_option(gasp_grids_t *g, int option, int value) {
   if (!g) return GASP_ERR_INVALID;
   GridsExtra &x = impl(g)->x;
-  if (option == GASP_OPT_SWEEP_VARIANT && value >= 0 && value <= 8) {
+  if (option == GASP_OPT_SWEEP_VARIANT && value >= 0 && value <= 9) {
     x.variant = value;
     return GASP_OK;
   }

@@ -133,6 +133,68 @@ __device__ __forceinline__ void stage_out(const uint32_t *lat_s, const SweepLaun
   }
 }
 
+// Bulk-copy staging (sweep variant 9).  In identity order a tile's W*32 words
+// are contiguous in HBM and in shared memory, so one cp.async.bulk of the
+// whole tile, its completion counted on an mbarrier, replaces the per-lane
+// loads, and one bulk shared->global copy the write-back.  Every wait is
+// bounded: a load that has not completed after kStagePolls polls (and as many
+// again) sets g_stage_timeout, the tile is neither swept nor written back,
+// and the host turns the flag into GASP_ERR_TIMEOUT.
+__device__ int g_stage_timeout;
+constexpr int kStagePolls = 1 << 22;
+
+__device__ __forceinline__ bool stage_wait(uint32_t bar) {
+  for (int i = 0; i < kStagePolls; ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n"
+        " selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(done)
+        : "r"(bar)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+// Returns false (on every lane) when the copy did not complete in time.
+__device__ __forceinline__ bool bulk_stage_in(uint32_t *lat_s, const uint32_t *src, uint32_t bytes,
+                                              uint64_t *bar, int lane) {
+  const uint32_t b = (uint32_t)__cvta_generic_to_shared(bar);
+  if (lane == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(b) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(bytes)
+                 : "memory");
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            (uint32_t)__cvta_generic_to_shared(lat_s)),
+        "l"(src), "r"(bytes), "r"(b)
+        : "memory");
+  }
+  __syncwarp();
+  bool ok = stage_wait(b);
+  if (!ok) {
+    if (lane == 0) atomicOr(&g_stage_timeout, 1);
+    stage_wait(b);  // give the copy in flight a second bounded wait before the CTA moves on
+  }
+  return __all_sync(0xffffffffu, ok);
+}
+
+__device__ __forceinline__ void bulk_stage_out(uint32_t *dst, const uint32_t *lat_s, uint32_t bytes,
+                                               int lane) {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // the sweep's writes, to the copy
+  __syncwarp();
+  if (lane == 0) {
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst),
+                 "r"((uint32_t)__cvta_generic_to_shared(lat_s)), "r"(bytes)
+                 : "memory");
+    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+    asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+  }
+  __syncwarp();
+}
+
 __device__ __forceinline__ uint32_t bit_at(const uint32_t *my, int s) {
   return (my[(s >> 5) * kTile] >> (s & 31)) & 1u;
 }
@@ -652,7 +714,7 @@ __global__ void __launch_bounds__(32) k_sweep_rows_pair(SweepLaunch p) {
 }
 
 template <int L, bool kStatic, bool kFloatCmp, int kRng, bool kMask = false,
-          bool kStoreAlways = false>
+          bool kStoreAlways = false, bool kBulk = false>
 __global__ void __launch_bounds__(32) k_sweep_rows(SweepLaunch p) {
   static_assert(L % 32 == 0, "rows of whole words");
   static_assert(!kMask || (L & (L - 1)) == 0, "the acceptance-mask kernel needs L a power of two");
@@ -707,13 +769,23 @@ __global__ void __launch_bounds__(32) k_sweep_rows(SweepLaunch p) {
   const int slot = tile * kTile + lane;
   const bool live = slot < n_act;
   const int rep = live ? (p.active ? p.active[slot] : slot) : 0;
-  stage_in(lat, p, W, tile, lane, live, rep);
+  constexpr uint32_t kTileBytes = W * kTile * sizeof(uint32_t);
+  bool staged = true;
+  if constexpr (kBulk) {
+    __shared__ __align__(8) uint64_t stage_bar;
+    if (p.active == nullptr)
+      staged = bulk_stage_in(lat, p.lat + (size_t)tile * W * kTile, kTileBytes, &stage_bar, lane);
+    else
+      stage_in(lat, p, W, tile, lane, live, rep);
+  } else {
+    stage_in(lat, p, W, tile, lane, live, rep);
+  }
   __syncwarp();
 
   const char *latb = reinterpret_cast<const char *>(lat);
   const char *thrb = reinterpret_cast<const char *>(thrP);
   const char *paccb = reinterpret_cast<const char *>(paccP);
-  if (live && p.nsweeps > 0) {
+  if (live && staged && p.nsweeps > 0) {
     RngPolicy<kRng> rg;
     rg.load(p.rng, p.rng_stride, rep);
     const float shrink = (1.0f - FLT_EPSILON) * (float)N;
@@ -752,8 +824,16 @@ __global__ void __launch_bounds__(32) k_sweep_rows(SweepLaunch p) {
     rg.store(p.rng, p.rng_stride, rep);
   }
   __syncwarp();
+  if (!staged) return;  // the bulk load timed out: flagged, nothing written back
   epilogue_mag(lat + lane, p, N, W, live, rep);
-  stage_out(lat, p, W, tile, lane, live, rep);
+  if constexpr (kBulk) {
+    if (p.active == nullptr)
+      bulk_stage_out(p.lat + (size_t)tile * W * kTile, lat, kTileBytes, lane);
+    else
+      stage_out(lat, p, W, tile, lane, live, rep);
+  } else {
+    stage_out(lat, p, W, tile, lane, live, rep);
+  }
 }
 
 // Two tiles per warp: each lane sweeps one replica of tile 2b and one of tile
@@ -1082,6 +1162,16 @@ int dispatch_kind(const SweepLaunch &p, cudaStream_t s) {
       default: break;
     }
   }
+  if (p.variant == 9) {  // variant 0 with bulk-copy staging of the tiles (measured slower)
+    switch (p.L) {
+      case 32: return launch_rows(k_sweep_rows<32, true, F, K, false, true, true>, p, 0, s);
+      case 64: return launch_rows(k_sweep_rows<64, true, F, K, false, true, true>, p, 0, s);
+      case 96: return launch_rows(k_sweep_rows<96, false, F, K, false, true, true>, p, dyn96, s);
+      case 128:
+        return launch_rows(k_sweep_rows<128, false, F, K, false, true, true>, p, dyn128, s);
+      default: break;  // other L: the default kernels
+    }
+  }
   if (p.variant == 0) {  // the row kernel writing the centre word back on every attempt
     switch (p.L) {
       case 32: return launch_rows(k_sweep_rows<32, true, F, K, false, true>, p, 0, s);
@@ -1147,6 +1237,23 @@ int launch_sweep_exact(const SweepLaunch &p, cudaStream_t s) {
     q.mag_out = left == 0 ? p.mag_out : nullptr;
     const int rc = p.float_compare ? dispatch_exact<true>(q, s) : dispatch_exact<false>(q, s);
     if (rc) return rc;
+  }
+  if (p.variant == 9) {  // bulk staging: report a timed-out copy (not while a graph is captured)
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    GASP_CUDA(cudaStreamIsCapturing(s, &cs));
+    if (cs == cudaStreamCaptureStatusNone) {
+      int flag = 0;
+      GASP_CUDA(cudaMemcpyFromSymbolAsync(&flag, g_stage_timeout, sizeof(int), 0,
+                                          cudaMemcpyDeviceToHost, s));
+      GASP_CUDA(cudaStreamSynchronize(s));
+      if (flag) {
+        const int zero = 0;
+        GASP_CUDA(cudaMemcpyToSymbolAsync(g_stage_timeout, &zero, sizeof(int), 0,
+                                          cudaMemcpyHostToDevice, s));
+        GASP_CUDA(cudaStreamSynchronize(s));
+        return GASP_ERR_TIMEOUT;
+      }
+    }
   }
   return GASP_OK;
 }

@@ -132,7 +132,13 @@ int gasp_grids_shape(const gasp_grids_t *grids, int *L_out, int *ngrids_out);
  * full adders, per-replica acceptance draws, a ballot flip mask -- replicas
  * of a tile are correlated; about half the throughput of variant 0; 8 the
  * row kernel with two tiles per warp (L = 32, 64, 128; each lane runs the
- * two replicas' attempts interleaved; bit-identical to 0, measured slower).
+ * two replicas' attempts interleaved; bit-identical to 0, measured slower);
+ * 9 variant 0 with each tile staged between HBM and shared memory by one
+ * bulk copy (cp.async.bulk, completion on an mbarrier) instead of per-lane
+ * loads and stores (L = 32, 64, 96, 128 in replica order, i.e. without an
+ * active list; bit-identical to 0, measured slower; each launch reads back
+ * a device flag, so a copy that did not complete within its bounded wait
+ * returns GASP_ERR_TIMEOUT).
  * GASP_OPT_WARPS_PER_CTA: tiles per CTA of the generic kernel (1..8).
  * GASP_OPT_TAIL_REPLICAS: device-side committor shooting (itask 1 with
  * compaction) on the MWC64X stream sweeps with variant 6 once at most this

@@ -178,8 +178,8 @@ def test_cli_committor_reads_gridinput(ref_gpu, tmp_path):
 @pytest.mark.parametrize("beta,h", [(0.45, 0.1), (0.5, 0.0), (1e-9, 0.1)])
 def test_kernel_variants_agree(L, kind, beta, h):
     """The generic (with and without the every-attempt store), row,
-    pairwise-speculative, acceptance-mask and two-tiles-per-warp kernels give
-    identical results for both RNG kinds (96 replicas: the last warp of the
+    pairwise-speculative, acceptance-mask, two-tiles-per-warp and
+    bulk-staged kernels give identical results for both RNG kinds (96 replicas: the last warp of the
     two-tile kernel has one tile).  h = 0 leaves six classes that can
     reject (the most the mask kernel takes); at beta = 1e-9 every P rounds to
     1.0, ten classes can reject and the mask variant falls back to the row
@@ -187,7 +187,7 @@ def test_kernel_variants_agree(L, kind, beta, h):
     ng, seed = 96, 31 + L
     g0 = np.where(np.random.default_rng(seed).random((ng, L, L)) < 0.3, 1, -1).astype(np.int32)
     outs = []
-    for variant in (0, 1, 2, 3, 4, 5, 8):
+    for variant in (0, 1, 2, 3, 4, 5, 8, 9):
         dg = engine.DeviceGrids(L, ng, g0)
         dg.set_option(1, variant)
         r = engine.RngStates(ng, seed, kind=kind)
@@ -197,4 +197,50 @@ def test_kernel_variants_agree(L, kind, beta, h):
     for o in outs[1:]:
         assert np.array_equal(outs[0][0], o[0])
         assert np.array_equal(outs[0][1], o[1])
+    assert not np.array_equal(outs[0][0], g0)
+
+
+@pytest.mark.parametrize("compact", [False, True])
+def test_bulk_staged_committor_matches_default(compact):
+    """Committor shooting through the driver with sweep variant 9: with
+    compaction the active lists take the per-lane staging path of the same
+    kernel, without it every launch stages whole tiles by bulk copies; fates,
+    pB and attempt counts equal variant 0's."""
+    L, k, shots = 64, 3, 96
+    yy, xx = np.mgrid[0:L, 0:L]
+    inputs = np.stack([np.where((yy - L / 2) ** 2 + (xx - L / 2) ** 2 <= r * r, 1, -1)
+                       for r in (6.0, 7.0, 8.0)]).astype(np.int32)
+    outs = []
+    for variant in (0, 9):
+        dg = engine.DeviceGrids(L, k * shots)
+        dg.upload_inputs(inputs)
+        dg.set_option(1, variant)
+        rng = engine.RngStates(k * shots, 5, kind="xorwow")
+        res, fates, _, att = engine.run_driver(dg, rng, 0.54, 0.07, 3000, 10, 3000, itask=1,
+                                               dn_thr=-0.93, up_thr=0.9, ninputs=k,
+                                               compact=compact)
+        outs.append((np.asarray(res).copy(), fates.copy(), att, dg.download()))
+    assert np.array_equal(outs[0][0], outs[1][0])
+    assert np.array_equal(outs[0][1], outs[1][1])
+    assert outs[0][2] == outs[1][2]
+    assert np.array_equal(outs[0][3], outs[1][3])
+
+
+@pytest.mark.parametrize("L,ng", [(64, 40), (96, 33), (128, 1), (32, 65)])
+def test_bulk_staged_sweep_ragged(L, ng):
+    """Sweep variant 9 (tiles staged by one bulk copy each) on replica counts
+    that leave the last tile partly empty: grids, magnetisation and RNG
+    states (of the replicas; the padding of the state rows is never written)
+    equal the default row kernel's."""
+    g0 = np.where(np.random.default_rng(L + ng).random((ng, L, L)) < 0.4, 1, -1).astype(np.int32)
+    outs = []
+    for variant in (0, 9):
+        dg = engine.DeviceGrids(L, ng, g0)
+        dg.set_option(1, variant)
+        r = engine.RngStates(ng, 7 + ng, kind="xorwow")
+        dg.sweep(r, 0.54, 0.07, 4)
+        outs.append((dg.download(), dg.magnetisation(), r.read_states()[:, :ng]))
+    assert np.array_equal(outs[0][0], outs[1][0])
+    assert np.array_equal(outs[0][1], outs[1][1])
+    assert np.array_equal(outs[0][2], outs[1][2])
     assert not np.array_equal(outs[0][0], g0)
