@@ -381,7 +381,7 @@ def run_committor(args):
     t0 = time.perf_counter()
     dg = engine.DeviceGrids(L, n)
     dg.upload_inputs(inputs)
-    if args.committor_tail >= 0:  # 3 = GASP_OPT_TAIL_REPLICAS (MWC64X stream only)
+    if args.committor_tail >= 0:  # 3 = GASP_OPT_TAIL_REPLICAS
         dg.set_option(3, args.committor_tail)
     rng = engine.RngStates(n, SEED, kind=args.rng)
     res, fates, drv_s, attempts = engine.run_driver(
@@ -471,8 +471,8 @@ def run_cluster(args):
 
 
 def run_tail(args):
-    """The end of a committor run: few undecided L=64 replicas on the
-    production stream.  Per replica count, the time of one sweep with the row
+    """The end of a committor run: few undecided L=64 replicas (production
+    stream unless --tail-rng xorwow).  Per replica count, the time of one sweep with the row
     kernel (one lane per replica, variant 0) and with one warp per replica
     (variant 6), CUDA events on the library's stream, 10 sweeps per launch as
     in committor shooting."""
@@ -491,7 +491,7 @@ def run_tail(args):
             for v in (0, 6):
                 dg = engine.DeviceGrids(L, n, -np.ones((n, L, L), np.int32))
                 dg.set_option(nat.OPT_SWEEP_VARIANT, v)
-                rng = engine.RngStates(n, SEED + n, kind="mwc64x")
+                rng = engine.RngStates(n, SEED + n, kind=args.tail_rng)
                 for _ in range(args.warmup):
                     dg.sweep(rng, BETA, H, per_launch)
                 torch.cuda.synchronize()
@@ -513,7 +513,8 @@ def run_tail(args):
             "value": first["variant6"]["ms_per_sweep"], "unit": "ms/sweep", "n_gpus": 1,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,
             "speedup_vs_row_kernel": first["speedup"], "by_replicas": out,
-            "config": {"workload": f"L=64 all-down replicas, beta=0.54, h=0.07, MWC64X stream, "
+            "config": {"workload": f"L=64 all-down replicas, beta=0.54, h=0.07, "
+                                   f"{args.tail_rng} stream, "
                                    f"{per_launch} sweeps per launch; replica counts {counts}"}}
     print(json.dumps(line), flush=True)
 
@@ -604,8 +605,10 @@ def main():
     ap.add_argument("--committor-shots", type=int, default=4096)
     ap.add_argument("--committor-check", type=int, default=10)
     ap.add_argument("--committor-tail", type=int, default=-1,
-                    help="live replicas at which MWC64X shooting switches to one warp per "
+                    help="live replicas at which shooting switches to one warp per "
                          "replica (-1: library default, 0: never)")
+    ap.add_argument("--tail-rng", default="mwc64x", choices=["xorwow", "mwc64x"],
+                    help="stream of the tail workload")
     ap.add_argument("--surrogate-train", type=int, default=20000)
     ap.add_argument("--surrogate-test", type=int, default=2000)
     ap.add_argument("--surrogate-screen", type=int, default=100000)

@@ -54,7 +54,12 @@ struct TableBlock {
 
 // Committor shooting on the MWC64X stream switches to the one-warp-per-replica
 // sweep once at most this many replicas are undecided (GASP_OPT_TAIL_REPLICAS).
-constexpr int kTailReplicasDefault = 4096;
+// Live replicas at which device-side committor shooting hands its last
+// undecided replicas to the one-warp-per-replica kernel, per stream (the
+// XORWOW kernel draws its attempts in order, one warp-wide step per draw,
+// so its throughput crosses the row kernel's at fewer replicas).
+constexpr int kTailReplicasMwc = 4096;
+constexpr int kTailReplicasXorwow = 1024;
 
 struct GridsExtra {
   TableBlock *d_tab = nullptr;
@@ -70,7 +75,7 @@ struct GridsExtra {
   int mask_ok = 0;          // <= 6 classes with P <= 1 (see k_sweep_rows<kMask>)
   int variant = 0;          // GASP_OPT_SWEEP_VARIANT
   int warps_per_cta = 1;    // GASP_OPT_WARPS_PER_CTA
-  int tail_replicas = kTailReplicasDefault;  // GASP_OPT_TAIL_REPLICAS
+  int tail_replicas = -1;   // GASP_OPT_TAIL_REPLICAS (-1: the stream's default)
 };
 
 // Extra state kept beside the public struct (allocated with it).
@@ -984,16 +989,18 @@ int committor_on_device(gasp_grids_t *g, gasp_rng_t *r, int tot, int mag_int, in
   bool done = n0 == 0;
   int checks = 0;
   // Once few replicas are undecided, each gets a warp of its own
-  // (k_sweep_tail, production stream only).  Both kernels are enqueued every
-  // interval and each checks the device count, so the switch happens at the
-  // same interval whatever the host's timing.
-  const bool tail_ok = r->kind == kRngMwc && x.tail_replicas > 0 && !g->global_lattice &&
-                       g->L >= 3 && g->L <= kTailMaxL;
+  // (k_sweep_tail).  Both kernels are enqueued every interval and each checks
+  // the device count, so the switch happens at the same interval whatever the
+  // host's timing.  On the XORWOW stream the tail kernel draws every attempt
+  // in the replica's own order, so the trajectories stay the reference's.
+  const int tail_n = x.tail_replicas >= 0 ? x.tail_replicas
+                     : r->kind == kRngMwc ? kTailReplicasMwc : kTailReplicasXorwow;
+  const bool tail_ok = tail_n > 0 && !g->global_lattice && g->L >= 3 && g->L <= kTailMaxL;
   SweepLaunch q = p;
   if (tail_ok) {
-    p.tail_split = q.tail_split = x.tail_replicas;
+    p.tail_split = q.tail_split = tail_n;
     q.variant = 6;
-    q.n_active = x.tail_replicas < ngrids ? x.tail_replicas : ngrids;
+    q.n_active = tail_n < ngrids ? tail_n : ngrids;
   }
   for (int isweep = 0; isweep < tot && !done; isweep += spc) {
     if (isweep % mag_int == 0) {

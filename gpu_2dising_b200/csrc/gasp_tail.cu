@@ -70,7 +70,7 @@ __device__ __forceinline__ uint32_t bit_of(const uint32_t *words, uint32_t s) {
   return (words[s >> 5] >> (s & 31u)) & 1u;
 }
 
-template <int L_, bool kFloatCmp>
+template <int L_, bool kFloatCmp, int kRng>
 __global__ void __launch_bounds__(128) k_sweep_tail(SweepLaunch p, TailParams tp) {
   const int L = L_ > 0 ? L_ : p.L;
   const int N = L * L;
@@ -99,13 +99,25 @@ __global__ void __launch_bounds__(128) k_sweep_tail(SweepLaunch p, TailParams tp
     marks[w] = marks[W + w] = marks[2 * W + w] = marks[3 * W + w] = 0u;
   }
 
-  // lane j's stream: the replica's state advanced by j * 2^35 draws
-  uint32_t x, c;
-  {
+  // MWC64X: lane j's stream is the replica's state advanced by j * 2^35 draws.
+  // XORWOW: every lane holds the replica's one state and steps it in
+  // lockstep, so the attempts are drawn in the replica's own order (site,
+  // acceptance, site, ...) exactly as the row kernels draw them.
+  uint32_t x = 0u, c = 0u;
+  curandStateXORWOW st;
+  if constexpr (kRng == kRngMwc) {
     const uint64_t X = (uint64_t)p.rng[rep] * kMwcA + p.rng[p.rng_stride + rep];
     const uint64_t Xj = mulmod_m(X, tp.mul[lane]);
     x = (uint32_t)(Xj / kMwcA);
     c = (uint32_t)(Xj % kMwcA);
+  } else {
+    st.d = p.rng[rep];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) st.v[k] = p.rng[(k + 1) * p.rng_stride + rep];
+    st.boxmuller_flag = 0;
+    st.boxmuller_flag_double = 0;
+    st.boxmuller_extra = 0.f;
+    st.boxmuller_extra_double = 0.0;
   }
   uint32_t ndraw = 0;
   auto next = [&]() -> uint32_t {
@@ -116,28 +128,57 @@ __global__ void __launch_bounds__(128) k_sweep_tail(SweepLaunch p, TailParams tp
     ++ndraw;
     return r;
   };
-  // site of a draw: its top bits scaled to [0, N) (as the row kernels)
+  // site of a draw: MWC64X, its top bits scaled to [0, N); XORWOW, the
+  // reference's float arithmetic (src/mc_gpu.cu:311,317), as the row kernels
+  const float shrink = (1.0f - FLT_EPSILON) * (float)N;
   auto site_of = [&](uint32_t r) -> uint32_t {
-    if constexpr (L_ > 0 && ((L_ * L_) & (L_ * L_ - 1)) == 0)
+    if constexpr (kRng == kRngXorwow)
+      return (uint32_t)__float2int_rd(shrink * _curand_uniform(r));
+    else if constexpr (L_ > 0 && ((L_ * L_) & (L_ * L_ - 1)) == 0)
       return r >> (32 - __builtin_ctz((unsigned)(L_ * L_)));
     else
       return __umulhi(r, (uint32_t)N);
   };
-  // Every lane holds its next attempt ready (drawn one assignment ahead), so
-  // a refill is a register move and the draws stay off the round's chain.
-  uint32_t ns = site_of(next());
-  uint32_t nu = next();
+  // XORWOW refill: the warp draws the next `nnew` attempts in order (warp-
+  // uniform loop); the lane whose attempt is the q-th of them keeps its pair.
+  auto draw_in_order = [&](int nnew, int q, uint32_t &s_out, uint32_t &u_out) {
+    uint32_t a = 0u, b = 0u;
+    for (int j = 0; j < nnew; ++j) {
+      const uint32_t r0 = curand(&st);
+      const uint32_t r1 = curand(&st);
+      if (j == q) {
+        a = r0;
+        b = r1;
+      }
+    }
+    if (q >= 0 && q < nnew) {
+      s_out = site_of(a);
+      u_out = b;
+    }
+  };
+  // MWC64X: every lane holds its next attempt ready (drawn one assignment
+  // ahead), so a refill is a register move and the draws stay off the
+  // round's chain.
+  uint32_t ns = 0u, nu = 0u;
+  if constexpr (kRng == kRngMwc) {
+    ns = site_of(next());
+    nu = next();
+  }
   __syncwarp();
 
   const int Q = p.nsweeps * N;  // attempts of this launch (< 2^30)
   int drawn = Q < 32 ? Q : 32;
   bool valid = lane < drawn;
   uint32_t s = 0u, u = 0u;
-  if (valid) {
-    s = ns;
-    u = nu;
-    ns = site_of(next());
-    nu = next();
+  if constexpr (kRng == kRngMwc) {
+    if (valid) {
+      s = ns;
+      u = nu;
+      ns = site_of(next());
+      nu = next();
+    }
+  } else {
+    draw_in_order(drawn, lane, s, u);
   }
   int head = 0, pend = drawn, done = 0, rnd = 0;
   bool pvalid = false;  // this lane's mark of the previous round, to clear
@@ -197,27 +238,35 @@ __global__ void __launch_bounds__(128) k_sweep_tail(SweepLaunch p, TailParams tp
     const int room = 32 - pend, left = Q - drawn;
     const int nnew = room < left ? room : left;
     const int pos2 = (lane - head) & 31;
-    if (pos2 >= pend) {
-      valid = pos2 - pend < nnew;
-      if (valid) {
+    if (pos2 >= pend) valid = pos2 - pend < nnew;
+    if constexpr (kRng == kRngMwc) {
+      if (pos2 >= pend && valid) {
         s = ns;
         u = nu;
         ns = site_of(next());
         nu = next();
       }
+    } else {
+      draw_in_order(nnew, pos2 - pend, s, u);  // lanes still pending keep theirs (q < 0)
     }
     pend += nnew;
     drawn += nnew;
   }
 
-  // the replica's stream continues past the longest lane segment used
-  const uint32_t most = __reduce_max_sync(kFull, ndraw);
-  const int jstar = __ffs(__ballot_sync(kFull, ndraw == most)) - 1;
-  if (lane == jstar) {
-    const uint64_t Xe = (uint64_t)x * kMwcA + c;
-    const uint64_t Xb = mulmod_m(Xe, tp.inv[lane]);
-    p.rng[rep] = (uint32_t)(Xb / kMwcA);
-    p.rng[p.rng_stride + rep] = (uint32_t)(Xb % kMwcA);
+  if constexpr (kRng == kRngMwc) {
+    // the replica's stream continues past the longest lane segment used
+    const uint32_t most = __reduce_max_sync(kFull, ndraw);
+    const int jstar = __ffs(__ballot_sync(kFull, ndraw == most)) - 1;
+    if (lane == jstar) {
+      const uint64_t Xe = (uint64_t)x * kMwcA + c;
+      const uint64_t Xb = mulmod_m(Xe, tp.inv[lane]);
+      p.rng[rep] = (uint32_t)(Xb / kMwcA);
+      p.rng[p.rng_stride + rep] = (uint32_t)(Xb % kMwcA);
+    }
+  } else if (lane == 0) {  // 2 draws per attempt consumed, as by the row kernels
+    p.rng[rep] = st.d;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) p.rng[(k + 1) * p.rng_stride + rep] = st.v[k];
   }
   __syncwarp();
   int pc = 0;
@@ -230,12 +279,12 @@ __global__ void __launch_bounds__(128) k_sweep_tail(SweepLaunch p, TailParams tp
   if (lane == 0 && p.mag_out != nullptr) p.mag_out[rep] = (float)(2 * pc - N) / (float)N;
 }
 
-template <int L_, bool F>
+template <int L_, bool F, int K>
 int launch_tail_kernel(const SweepLaunch &p, cudaStream_t s) {
   const int W = words_per_replica(p.L);
   const int nwarps = kTailWordsPerW * W <= 4096 ? 4 : 1;
   const size_t smem = (size_t)(kTailHeaderWords + nwarps * kTailWordsPerW * W) * sizeof(uint32_t);
-  auto kern = k_sweep_tail<L_, F>;
+  auto kern = k_sweep_tail<L_, F, K>;
   if (smem > 48 * 1024)
     GASP_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int blocks = (p.n_active + nwarps - 1) / nwarps;
@@ -246,16 +295,24 @@ int launch_tail_kernel(const SweepLaunch &p, cudaStream_t s) {
 
 }  // namespace
 
+template <int K>
+int launch_tail_kind(const SweepLaunch &p, cudaStream_t s) {
+  if (p.L == 64)
+    return p.float_compare ? launch_tail_kernel<64, true, K>(p, s)
+                           : launch_tail_kernel<64, false, K>(p, s);
+  return p.float_compare ? launch_tail_kernel<0, true, K>(p, s)
+                         : launch_tail_kernel<0, false, K>(p, s);
+}
+
 int launch_sweep_tail(const SweepLaunch &p, cudaStream_t s) {
-  if (p.rng_kind != kRngMwc || p.lattice_in_global || p.L < 3 || p.L > kTailMaxL) {
-    set_error("the one-warp-per-replica sweep needs the MWC64X stream and 3 <= L <= %d "
-              "(shared-memory lattices)", kTailMaxL);
+  if (p.lattice_in_global || p.L < 3 || p.L > kTailMaxL) {
+    set_error("the one-warp-per-replica sweep needs 3 <= L <= %d (shared-memory lattices)",
+              kTailMaxL);
     return GASP_ERR_UNSUPPORTED;
   }
   if (p.n_active <= 0 || p.nsweeps <= 0) return GASP_OK;
-  if (p.L == 64)
-    return p.float_compare ? launch_tail_kernel<64, true>(p, s) : launch_tail_kernel<64, false>(p, s);
-  return p.float_compare ? launch_tail_kernel<0, true>(p, s) : launch_tail_kernel<0, false>(p, s);
+  return p.rng_kind == kRngMwc ? launch_tail_kind<kRngMwc>(p, s)
+                               : launch_tail_kind<kRngXorwow>(p, s);
 }
 
 }  // namespace gasp

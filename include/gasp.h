@@ -120,12 +120,14 @@ int gasp_grids_shape(const gasp_grids_t *grids, int *L_out, int *ngrids_out);
  * decided by a per-draw mask of accepted neighbourhoods (falls back to 2 when
  * more than six classes can reject; L = 32, 64, 128 only), 5 the generic
  * kernel writing the centre word back on every attempt, 6 one warp per
- * replica (MWC64X stream only, 3 <= L <= 512; GASP_ERR_UNSUPPORTED otherwise):
- * the warp applies up to 32 queued attempts of its replica per step, all
- * those that touch no site or neighbour of another, in the order drawn --
- * the same dynamics as the other variants with a different assignment of
- * draws, and ~5x less time per sweep of a single replica, at a quarter of
- * the throughput per SM when many replicas are live; 7 the multispin
+ * replica (3 <= L <= 512; GASP_ERR_UNSUPPORTED otherwise): the warp applies
+ * up to 32 queued attempts of its replica per step, all those that touch no
+ * site or neighbour of another, in the order drawn -- on the XORWOW stream
+ * the attempts are drawn in the replica's own order, so the result is
+ * bit-identical to variant 0; on MWC64X each lane draws from its own
+ * substream, the same dynamics as the other variants with a different
+ * assignment of draws, ~5x less time per sweep of a single replica, at a
+ * quarter of the throughput per SM when many replicas are live; 7 the multispin
  * shared-site sweep (MWC64X stream only, integer thresholds, no active
  * list; GASP_ERR_UNSUPPORTED otherwise): the 32 replicas of a tile share each
  * attempt's site, held as one word per site, neighbour counts by bitwise
@@ -141,9 +143,10 @@ int gasp_grids_shape(const gasp_grids_t *grids, int *L_out, int *ngrids_out);
  * returns GASP_ERR_TIMEOUT).
  * GASP_OPT_WARPS_PER_CTA: tiles per CTA of the generic kernel (1..8).
  * GASP_OPT_TAIL_REPLICAS: device-side committor shooting (itask 1 with
- * compaction) on the MWC64X stream sweeps with variant 6 once at most this
- * many replicas are undecided (default 4096; 0: never).  No effect on the
- * XORWOW stream, whose trajectories stay bit-identical to the reference's. */
+ * compaction) sweeps with variant 6 once at most this many replicas are
+ * undecided (default 4096 on the MWC64X stream, 1024 on XORWOW; 0: never).
+ * On the XORWOW stream the trajectories stay bit-identical to the
+ * reference's either way. */
 enum { GASP_OPT_SWEEP_VARIANT = 1, GASP_OPT_WARPS_PER_CTA = 2, GASP_OPT_TAIL_REPLICAS = 3 };
 int gasp_grids_set_option(gasp_grids_t *grids, int option, int value);
 

@@ -2,8 +2,10 @@
 the row and generic kernels against the serial one-stream sweep, and the
 one-warp-per-replica kernel (variant 6) against its serial statement -- which
 applies attempts one at a time, so equality also shows that the kernel's
-parallel rounds change nothing.  Then committor shooting that switches to
-variant 6 for its last undecided replicas against shooting that never does."""
+parallel rounds change nothing.  On the reference (XORWOW) stream variant 6
+draws in the replica's own order and equals the row kernel bit for bit.  Then
+committor shooting that switches to variant 6 for its last undecided
+replicas against shooting that never does."""
 import numpy as np
 import pytest
 
@@ -73,13 +75,53 @@ def test_warp_per_replica_kernel_matches_serial_oracle(L, nsweeps, n):
         assert mag[r] == oracle.magnetisation_gpu(L, g.reshape(1, L, L))[0]
 
 
-def test_warp_per_replica_kernel_needs_the_production_stream():
-    dg = engine.DeviceGrids(64, 32)
-    dg.set_option(nat.OPT_SWEEP_VARIANT, 6)
-    rng = engine.RngStates(32, 1, kind="xorwow")
-    with pytest.raises(nat.GaspError) as e:
-        dg.sweep(rng, BETA, H, 1)
-    assert e.value.status == nat.GASP_ERR_UNSUPPORTED
+@pytest.mark.parametrize("L,nsweeps,n,beta", [(64, 2, 37, BETA), (48, 2, 37, BETA),
+                                              (20, 3, 37, BETA), (128, 1, 37, BETA),
+                                              (5, 4, 37, BETA), (3, 5, 3, BETA),
+                                              (64, 1, 1, BETA), (64, 2, 33, 3.0)])
+def test_warp_per_replica_kernel_on_reference_stream_equals_row_kernel(L, nsweeps, n, beta):
+    """On the XORWOW stream variant 6 draws each replica's attempts in the
+    replica's own order, so its grids, magnetisation and RNG states equal the
+    row kernel's (and so the reference kernels'), the float-comparison path
+    (beta = 3) included."""
+    g0 = _start(L, n, 300 + L)
+    outs = []
+    for variant in (0, 6):
+        dg = engine.DeviceGrids(L, n, g0)
+        dg.set_option(nat.OPT_SWEEP_VARIANT, variant)
+        rng = engine.RngStates(n, 17 + L, kind="xorwow")
+        dg.sweep(rng, beta, H, nsweeps)
+        dg.sweep(rng, beta, H, 1)
+        outs.append((dg.download(), dg.magnetisation(), rng.read_states()[:, :n]))
+    assert np.array_equal(outs[0][0], outs[1][0])
+    assert np.array_equal(outs[0][1], outs[1][1])
+    assert np.array_equal(outs[0][2], outs[1][2])
+    assert not np.array_equal(outs[0][0], g0)
+
+
+@pytest.mark.parametrize("tail", [1 << 30, 700])
+def test_committor_tail_on_reference_stream_changes_nothing(tail):
+    """Committor shooting on the XORWOW stream: fates, pB, attempt counts and
+    final grids are the same whether the last undecided replicas (or all of
+    them from the start) sweep with one warp each or stay on the row kernel."""
+    yy, xx = np.mgrid[0:64, 0:64]
+    inputs = np.stack([np.where((yy - 32) ** 2 + (xx - 32) ** 2 <= r * r, 1, -1)
+                       for r in (6.0, 7.0, 8.0)]).astype(np.int32)
+    outs = []
+    for t in (0, tail):
+        dg = engine.DeviceGrids(64, 3 * 256)
+        dg.upload_inputs(inputs)
+        dg.set_option(nat.OPT_TAIL_REPLICAS, t)
+        rng = engine.RngStates(3 * 256, 29, kind="xorwow")
+        res, fates, _, att = engine.run_driver(dg, rng, BETA, H, 20000, 10, 20000, itask=1,
+                                               dn_thr=-0.93, up_thr=0.9, ninputs=3,
+                                               compact=True)
+        assert np.count_nonzero(fates == -1) == 0
+        outs.append((np.asarray(res).copy(), fates.copy(), att, dg.download()))
+    assert np.array_equal(outs[0][0], outs[1][0])
+    assert np.array_equal(outs[0][1], outs[1][1])
+    assert outs[0][2] == outs[1][2]
+    assert np.array_equal(outs[0][3], outs[1][3])
 
 
 def _droplets(L, radii):
