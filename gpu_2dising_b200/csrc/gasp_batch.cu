@@ -490,7 +490,10 @@ int gasp_batch_autotune(gasp_batch_t *b, int nsweeps, int *choice_out) {
     if ((rc = prepare_tables(gr, b->groups[g].beta, b->groups[g].h))) break;
     const int L = b->groups[g].L;
     const bool rows = (L == 32 || L == 64 || L == 96 || L == 128);
-    // candidates: (variant, warps_per_cta)
+    // candidates: (variant, warps_per_cta).  One warp per replica (variant 6)
+    // is not one: timed alone it halves a small group's sweep (L=128, 512
+    // replicas, XORWOW), but it spends ~20x the issue slots per attempt, and
+    // in the concurrent graph that slows the other groups by more than it saves.
     std::vector<std::pair<int, int>> cand;
     if (rows) cand = {{0, 1}, {2, 1}};
     else cand = {{0, 1}, {0, 2}, {0, 4}};
