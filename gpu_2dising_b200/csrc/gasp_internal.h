@@ -118,7 +118,7 @@ int launch_rng_init(uint32_t *rng, int ngrids, int stride, unsigned long long se
 int launch_build_thresholds(const float *d_pacc20, uint32_t *d_thr10, int *d_flags, cudaStream_t s);
 int launch_sweep_exact(const SweepLaunch &p, cudaStream_t s);
 int launch_sweep_trace_cpu(const SweepLaunch &p, cudaStream_t s);
-// One warp per replica, MWC64X stream only (gasp_tail.cu); p.n_active is the
+// One warp per replica, either stream (gasp_tail.cu); p.n_active is the
 // launch shape (an upper bound of *p.n_active_dev when that is set).
 int launch_sweep_tail(const SweepLaunch &p, cudaStream_t s);
 // Multispin shared-site sweep, MWC64X stream, no active list (gasp_shared.cu).

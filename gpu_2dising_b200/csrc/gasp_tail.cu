@@ -1,5 +1,5 @@
 // gasp_tail.cu -- one warp per replica: the latency-bound end of a committor
-// run on the production (MWC64X) stream.
+// run, on the production (MWC64X) stream and on the reference (XORWOW) one.
 //
 // Near the end of a shooting run only a few trajectories are undecided.  The
 // row kernels give each replica one lane, and a lane's attempts form one
@@ -25,10 +25,13 @@
 //     drawn: the dynamics is random-site Metropolis with i.i.d. uniform sites
 //     and acceptance draws, the same Markov chain as the row kernels.
 //
-// At L=64 about 22 attempts are applied per round.  Lane j draws from the
-// replica's MWC64X stream skipped ahead by j * 2^35 (a one-off 64-bit modular
-// multiply per lane and launch); after the launch the replica's state is set
-// past the longest lane segment used, so later launches never reuse a draw.
+// At L=64 about 22 attempts are applied per round.  On the XORWOW stream the
+// whole warp steps the replica's one state and hands the refilled lanes their
+// draws in order, so the attempts are the row kernel's, bit for bit.  On
+// MWC64X lane j draws from the replica's stream skipped ahead by j * 2^35
+// (a one-off 64-bit modular multiply per lane and launch); after the launch
+// the replica's state is set past the longest lane segment used, so later
+// launches never reuse a draw.
 // Per warp, shared memory holds the lattice (W words) and two sets of marks
 // (occupancy + duplicates, W words each) used in alternate rounds, so a
 // round's marks are cleared during the next round without a third warp
