@@ -7,10 +7,22 @@ One step = one check interval: 100 sweeps of every replica (32768 * 4096 *
 100 attempted flips) plus the fused magnetisation of the resulting state.
 
   python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+  python bench.py --workload {committor,batched,surrogate,cnn,rate,cluster,tail}
 
 Prints one JSON line on rank 0.  Multi-GPU: replicas are independent, so each
 rank runs its own 32768 replicas (weak scaling, no data-path collective); the
-timing is the max over ranks.
+timing is the max over ranks.  `--gpus N` without a launcher starts the N
+ranks itself (torch.distributed.run on this host); `--dry-run` runs the same
+rank plumbing with a host stand-in for the sweep (gloo, no GPU).
+
+The default line (N = 1) also carries
+  * cpu_baseline: the reference's own mc_driver_cpu on every host core, on
+    the CPU configuration of the same system (L=64, 1248 replicas, 5000
+    sweeps, checks every 100);
+  * secondary: the committor (64 droplet grids x 4096 shots, both streams,
+    pB compared), the uneven batched launch against plain per-group launches,
+    and the surrogate-screened committor against shooting alone -- each with
+    its own clock record, run in a child process after the timed region.
 """
 from __future__ import annotations
 
@@ -43,7 +55,10 @@ CONFIG = {
     "rng": "cuRAND XORWOW per replica (reference stream)",
     "l2": "flushed between timed steps (256 MiB device write)",
 }
-CPU_SAMPLE = {"replicas_per_process": 32, "sweeps": 400}
+# The CPU configuration of the same system (the reference's mc_driver_cpu):
+# L=64, 1248 replicas, 5000 sweeps, magnetisation checked every 100 sweeps.
+CPU_CONFIG = {"L": 64, "replicas": 1248, "sweeps": 5000, "mag_output_int": 100}
+CPU_MARK_INT = 50  # output-callback interval of the timing harness (step boundaries)
 
 
 def load_peaks():
@@ -107,60 +122,176 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_reference_sample(nproc=None, replicas=None, sweeps=None):
+def clocked(fn, *a, **kw):
+    """fn(*a, **kw) -> dict, with the clock record of the GPU while it ran."""
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+        out = fn(*a, **kw)
+    out["clocks"] = clk.summary()
+    return out
+
+
+def _cpu_cores():
+    return sorted(os.sched_getaffinity(0))
+
+
+def cpu_reference_run(replicas, sweeps, cores=None, seed=SEED):
     """The reference's own CPU driver (oracle/_ref/ref_cpu_bench: mc_cpu.c +
-    mt19937ar.c compiled unmodified) on every host core, one process per core
-    (its MT19937 state is a process global).  Returns attempts/s, cores, sample."""
+    mt19937ar.c compiled unmodified) on every host core: one process per core
+    (its MT19937 state is a process global), each pinned to its core and
+    given a contiguous, balanced share of the replicas and its own seed.
+    Returns None when the harness is not built, else a dict with the attempts
+    made, the wall time and, per process, the callback timestamps (every
+    CPU_MARK_INT sweeps) that cut the run into steps."""
     exe = os.path.join(REPO, "oracle", "_ref", "ref_cpu_bench")
     if not os.path.exists(exe):
         return None
-    nproc = nproc or len(os.sched_getaffinity(0))
-    replicas = replicas or CPU_SAMPLE["replicas_per_process"]
-    sweeps = sweeps or CPU_SAMPLE["sweeps"]
+    cores = cores or _cpu_cores()
+    nproc = max(1, min(len(cores), replicas))
+    procs = []
     t0 = time.perf_counter()
-    procs = [subprocess.Popen([exe, str(L), str(replicas), str(sweeps), str(MAG_INT), str(BETA),
-                               str(H), str(SEED + i)], stdout=subprocess.DEVNULL,
-                              stderr=subprocess.PIPE, text=True) for i in range(nproc)]
-    attempts = 0.0
+    for i in range(nproc):
+        _, count = shards.shard_range(replicas, nproc, i)
+        core = cores[i % len(cores)]
+        procs.append(subprocess.Popen(
+            [exe, str(CPU_CONFIG["L"]), str(count), str(sweeps), str(CPU_CONFIG["mag_output_int"]),
+             str(BETA), str(H), str(seed + i), str(CPU_MARK_INT)],
+            stdout=subprocess.DEVNULL, stderr=subprocess.PIPE, text=True,
+            preexec_fn=(lambda c=core: os.sched_setaffinity(0, {c}))))
+    attempts, marks = 0.0, []
     for p in procs:
         _, err = p.communicate()
-        a, _w = err.split()[-2:]
+        if p.returncode != 0:
+            raise RuntimeError(f"ref_cpu_bench failed ({p.returncode}): {err[-300:]}")
+        lines = err.strip().splitlines()
+        a, _w = lines[-2].split()
         attempts += float(a)
+        f = lines[-1].split()[1:]
+        marks.append((float(f[0]), {int(f[i]): float(f[i + 1]) for i in range(1, len(f), 2)}))
     wall = time.perf_counter() - t0
-    sample = (f"{nproc} processes x {replicas} replicas x {sweeps} sweeps of L={L} "
-              f"(beta={BETA}, h={H}, all-down), mc_driver_cpu unmodified")
-    return attempts / wall, nproc, sample, wall
+    return {"attempts": attempts, "wall_s": wall, "cores": nproc, "marks": marks,
+            "replicas": replicas, "sweeps": sweeps}
 
 
-def run_reference(args, rank):
+def cpu_steps(run, steps):
+    """Step times of one CPU run cut into `steps` equal sweep ranges: a step
+    ends when every process has passed its last sweep (boundaries rounded to
+    the callback interval)."""
+    sweeps = run["sweeps"]
+    bounds = [0] + [int(round(k * sweeps / steps / CPU_MARK_INT)) * CPU_MARK_INT
+                    for k in range(1, steps)] + [None]
+
+    def at(b):
+        ts = []
+        for t_start, m in run["marks"]:
+            if b == 0:
+                ts.append(t_start)
+            elif b is None or b not in m:
+                ts.append(max(m.values()))  # the end of that process's run
+            else:
+                ts.append(m[b])
+        return max(ts)
+
+    times = [at(bounds[k + 1]) - at(bounds[k]) for k in range(steps)]
+    return [max(t, 0.0) for t in times]
+
+
+def cpu_config_baseline():
+    """cpu_baseline of the JSON line: the CPU configuration run once in full."""
+    run = cpu_reference_run(CPU_CONFIG["replicas"], CPU_CONFIG["sweeps"])
+    if run is None:
+        return None
+    return {"value": run["attempts"] / run["wall_s"], "unit": UNIT, "cores": run["cores"],
+            "kind": "reference", "wall_s": run["wall_s"],
+            "sample": (f"the CPU configuration: L=64, {run['replicas']} replicas, "
+                       f"{run['sweeps']} sweeps, checks every {CPU_CONFIG['mag_output_int']}, "
+                       f"beta={BETA}, h={H}, all-down; {run['cores']} processes (one per core, "
+                       "pinned), mc_driver_cpu unmodified")}
+
+
+def run_reference(args, rank, world):
+    """The reference arm: the reference's own CPU path (mc_driver_cpu compiled
+    unmodified) on all host cores.  The K timed steps are the CPU
+    configuration (1248 replicas x 5000 sweeps) run once in full and cut into
+    K equal sweep ranges; the W warm-up steps are short runs before it.  The
+    line also reports the reference's GPU sweep kernels, compiled unmodified
+    for sm_100a, timed on this GPU on the headline workload."""
     if rank != 0:
         return
-    res = [cpu_reference_sample() for _ in range(args.warmup)]
-    t_total, a_total = 0.0, 0.0
-    last = None
-    for _ in range(args.steps):
-        last = cpu_reference_sample()
-        if last is None:
+    for _ in range(args.warmup):
+        if cpu_reference_run(len(_cpu_cores()), 100) is None:
             break
-        rate, nproc, sample, wall = last
-        t_total += wall
-        a_total += rate * wall
-    if last is None:
+    run = cpu_reference_run(CPU_CONFIG["replicas"], CPU_CONFIG["sweeps"])
+    if run is None:
         print(json.dumps({"impl": "reference",
                           "unavailable": "oracle/_ref/ref_cpu_bench not built (make -C oracle ref)"}))
         return
-    del res
-    value = a_total / t_total
+    step_s = cpu_steps(run, args.steps)
+    value = run["attempts"] / run["wall_s"]
+    sample = (f"the CPU configuration (L=64, {run['replicas']} replicas, {run['sweeps']} "
+              f"sweeps, checks every {CPU_CONFIG['mag_output_int']}) cut into {args.steps} "
+              f"steps; {run['cores']} processes, one per core, mc_driver_cpu unmodified")
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_total / args.steps,
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * run["wall_s"] / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "i32",
-        "data": "synthetic", "config": CONFIG, "impl": "reference",
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": last[1], "kind": "reference",
-                         "sample": last[2]},
+        "data": "synthetic (all-down L=64 lattices, seeded MT19937 per process)",
+        "config": {"workload": f"plain reversal on the CPU: L=64, beta=0.54, h=0.07, all-down, "
+                               f"{run['replicas']} replicas, {run['sweeps']} sweeps, "
+                               f"magnetisation checked every {CPU_CONFIG['mag_output_int']}",
+                   **CPU_CONFIG},
+        "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": run["cores"], "kind": "reference",
+                         "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "step_ms": [round(1e3 * t, 3) for t in step_s],
+        "wall_s": run["wall_s"],
     }
+    if not args.no_reference_gpu and _gpu_visible():
+        line["reference_gpu_kernels"] = reference_gpu_kernels()
     print(json.dumps(line), flush=True)
+
+
+def _gpu_visible():
+    try:
+        r = subprocess.run(["nvidia-smi", "-L"], capture_output=True, text=True, timeout=30)
+        return r.returncode == 0 and "GPU" in r.stdout
+    except (OSError, subprocess.TimeoutExpired):
+        return False
+
+
+def reference_gpu_kernels(calls=5):
+    """The reference's own GPU sweep kernels (src/mc_gpu.cu mc_sweep_gpu_bitmap32,
+    _bitrep, mc_sweep_gpu; compiled unmodified for sm_100a into
+    oracle/_ref/libref_gpu.so) on the headline workload: L=64, 32768 all-down
+    replicas, beta=0.54, h=0.07, 100 sweeps per launch, tpb 32 -- the
+    reference driver's launch shape.  Device time per launch from CUDA events."""
+    import ctypes as C
+    path = os.path.join(REPO, "oracle", "_ref", "libref_gpu.so")
+    if not os.path.exists(path):
+        return {"unavailable": "oracle/_ref/libref_gpu.so not built"}
+    try:
+        lib = C.CDLL(path)
+    except OSError as e:
+        return {"unavailable": f"libref_gpu.so did not load: {e}"}
+    lib.refgpu_time_kernels.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_ulonglong,
+                                        C.c_double, C.c_double, C.c_int, C.c_int,
+                                        C.POINTER(C.c_double)]
+    out = {}
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+        for method in (2, 1, 0):
+            ms = C.c_double(0.0)
+            rc = lib.refgpu_time_kernels(L, R, 32, method, 2024, BETA, H, SWEEPS_PER_STEP, calls,
+                                         C.byref(ms))
+            if rc != 0:
+                out[f"gpu_method_{method}"] = {"error": f"rc {rc}"}
+                continue
+            out[f"gpu_method_{method}"] = {
+                "ms_per_launch": ms.value,
+                "attempts_per_s": L * L * R * SWEEPS_PER_STEP / (ms.value / 1e3)}
+    return {"what": "reference GPU sweep kernels, unmodified, sm_100a, this GPU",
+            "workload": f"L=64, {R} all-down replicas, beta=0.54, h=0.07, {SWEEPS_PER_STEP} "
+                        "sweeps per launch, tpb 32", "calls": calls, "methods": out,
+            "clocks": clk.summary()}
 
 
 def read_profile_traffic():
@@ -215,17 +346,72 @@ def run_e2e(args, rank, world, dist, torch, engine):
                      "packed dumps every 1000 sweeps)"}
 
 
+def _init_dist(world, local_rank, backend):
+    if world <= 1:
+        return None
+    import datetime
+    import torch
+    import torch.distributed as dist
+    kw = {"timeout": datetime.timedelta(seconds=120)}
+    if backend == "nccl":
+        kw["device_id"] = torch.device("cuda", local_rank)
+    dist.init_process_group(backend, **kw)
+    return dist
+
+
+def run_dry(args, rank, world, local_rank):
+    """The rank plumbing of the default line without a GPU: each rank times a
+    host stand-in step (a numpy bit-count over a seeded lattice stack), the
+    step time is the max over ranks, rank 0 prints the line."""
+    dist = _init_dist(world, local_rank, "gloo")
+    rs = np.random.default_rng(shards.rank_seed(SEED, rank))
+    lat = rs.integers(0, 2 ** 32, size=(64, 128), dtype=np.uint64)
+    if dist is not None:
+        dist.barrier()
+    t0 = time.perf_counter()
+    pc = 0
+    for _ in range(args.steps):
+        pc += int(np.unpackbits(lat.view(np.uint8)).sum())
+    t = shards.max_over_ranks(time.perf_counter() - t0, dist)
+    n = shards.sum_over_ranks(args.steps * lat.size, dist)
+    if rank == 0:
+        line = {"metric": "dry run: host stand-in words/s", "value": n / max(t, 1e-9),
+                "unit": "words/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dry_run": True, "backend": "gloo" if dist is not None else None,
+                "world_size": dist.get_world_size() if dist is not None else 1,
+                "config": {"workload": "dry run: host stand-in step, no GPU"}}
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def run_secondary_child(args):
+    """The secondary figures, measured in a child process after the timed
+    region (its own CUDA context: a failure there cannot take the headline
+    line with it)."""
+    cmd = [sys.executable, os.path.abspath(__file__), "--workload", "secondary",
+           "--rng", "xorwow"]
+    if args.secondary_quick:
+        cmd.append("--secondary-quick")
+    try:
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=args.secondary_timeout)
+    except subprocess.TimeoutExpired:
+        return {"error": f"secondary measurements exceeded {args.secondary_timeout} s"}
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    if r.returncode != 0 or not lines:
+        return {"error": f"rc {r.returncode}: {r.stderr.strip()[-400:]}"}
+    return json.loads(lines[-1])
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     from gpu_2dising_b200 import engine
 
     torch.cuda.set_device(local_rank)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local_rank))
+    dist = _init_dist(world, local_rank, "nccl")
     engine.init_device(local_rank)
     stream = torch.cuda.Stream()
     engine.set_stream(stream.cuda_stream)
@@ -260,6 +446,10 @@ def run_ours(args, rank, world, local_rank):
     value = attempts_step * args.steps * world / (t_max / 1e3)
     mag = dg.magnetisation()
     assert np.all(np.abs(mag) <= 1.0)
+    dg.close()
+    rng.close()
+    del flush
+    torch.cuda.empty_cache()
 
     # End to end through the public driver (gasp_mc_driver_gpu): host int32
     # grids in, RNG seeding, K check intervals with the per-check
@@ -267,18 +457,13 @@ def run_ours(args, rank, world, local_rank):
     e2e = None
     if not args.no_e2e:
         e2e = run_e2e(args, rank, world, dist, torch, engine)
+    line = None
     if rank == 0:
         sm_max_mhz, peak_kind = load_peaks()
         peak = 148 * 128 * sm_max_mhz * 1e6 / 1e12       # T lane-ops/s
         launch_s = t_max / 1e3 / args.steps
         achieved = OPS_PER_ATTEMPT * attempts_step / launch_s / 1e12
         traffic = read_profile_traffic()
-        cpu = None
-        if world == 1 and not args.no_cpu_baseline:
-            c = cpu_reference_sample()
-            if c is not None:
-                cpu = {"value": c[0], "unit": UNIT, "cores": c[1], "kind": "reference",
-                       "sample": c[2]}
         if args.rng != "xorwow":
             CONFIG["rng"] = "MWC64X production stream (statistically equivalent, not bit-exact)"
             CONFIG["workload"] = CONFIG["workload"].replace("gpu_method 2 exact", "production RNG")
@@ -293,15 +478,23 @@ def run_ours(args, rank, world, local_rank):
                          "ops_per_attempt": OPS_PER_ATTEMPT,
                          "peak_basis": f"148 SMs x 128 lanes x {sm_max_mhz:.0f} MHz "
                                        f"({peak_kind} sm_max_mhz)"},
-            "cpu_baseline": cpu,
+            "cpu_baseline": None,
             "e2e": e2e,
             "gpu_launches": args.steps,
             "clocks": clk.summary(),
         }
-        print(json.dumps(line), flush=True)
+        if dist is not None:
+            line["nccl_world"] = dist.get_world_size()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+    if rank == 0:
+        # after the timed region and after the other ranks are done
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_config_baseline()
+        if world == 1 and not args.no_secondary:
+            line["secondary"] = run_secondary_child(args)
+        print(json.dumps(line), flush=True)
 
 
 BATCH_GROUPS_L = (32, 48, 64, 96, 128)
@@ -316,9 +509,9 @@ def batched_groups(seed=2024):
             for L, R_ in zip(BATCH_GROUPS_L, BATCH_GROUPS_R)]
 
 
-def run_batched(args):
-    """One JSON line for the uneven batched launch vs one plain launch per
-    group, both counting only attempts of not-yet-nucleated replicas."""
+def batched_measure(args):
+    """The uneven batched launch vs one plain launch per group, both counting
+    only attempts of not-yet-nucleated replicas."""
     import ctypes as C
     from gpu_2dising_b200 import _native as nat, engine
     engine.init_device(0)
@@ -339,7 +532,7 @@ def run_batched(args):
         res[name] = {"attempts": att.value, "seconds": el.value, "value": att.value / el.value,
                      "nucleated": counts.reshape(-1, len(groups))[-1].tolist()}
     nat.lib().gasp_batch_free(h)
-    line = {
+    return {
         "metric": "spin-flip attempts/s, uneven batched launch vs plain per-group launches",
         "value": res["graph"]["value"], "unit": UNIT, "n_gpus": 1,
         "speedup_vs_plain": res["graph"]["value"] / res["plain"]["value"],
@@ -351,7 +544,10 @@ def run_batched(args):
                    "sweeps": tot, "check_int": chk, "rng": args.rng,
                    "autotune": choice.reshape(-1, 2).tolist()},
     }
-    print(json.dumps(line), flush=True)
+
+
+def run_batched(args):
+    print(json.dumps(clocked(batched_measure, args)), flush=True)
 
 
 def committor_inputs(n=64, L_=L, seed=7):
@@ -370,11 +566,12 @@ def committor_inputs(n=64, L_=L, seed=7):
     return np.stack(out), np.array(radii)
 
 
-def run_committor(args):
+def committor_measure(args, rng_kind=None):
     """Committor shooting of 64 seeded droplet grids, 4096 replicas each,
     until every replica reaches A (m < -0.93) or B (m > 0.9), cap 20000 sweeps."""
     from gpu_2dising_b200 import analysis, engine
     engine.init_device(0)
+    rng_kind = rng_kind or args.rng
     ngrid_in, shots = args.committor_inputs, args.committor_shots
     inputs, radii = committor_inputs(ngrid_in)
     n = ngrid_in * shots
@@ -383,30 +580,51 @@ def run_committor(args):
     dg.upload_inputs(inputs)
     if args.committor_tail >= 0:  # 3 = GASP_OPT_TAIL_REPLICAS
         dg.set_option(3, args.committor_tail)
-    rng = engine.RngStates(n, SEED, kind=args.rng)
+    rng = engine.RngStates(n, SEED, kind=rng_kind)
     res, fates, drv_s, attempts = engine.run_driver(
         dg, rng, BETA, H, 20000, args.committor_check, 20000, itask=1, dn_thr=-0.93,
         up_thr=0.90, ninputs=ngrid_in, compact=True)
     wall = time.perf_counter() - t0
+    dg.close()
+    rng.close()
     errs = [analysis.committor_errbar(fates[i * shots:(i + 1) * shots]) for i in range(ngrid_in)]
-    line = {
+    resolved = [int(np.count_nonzero(fates[i * shots:(i + 1) * shots] >= 0))
+                for i in range(ngrid_in)]
+    return {
         "metric": "committor evaluations/s (shooting)", "value": ngrid_in / wall,
         "unit": "grids/s", "n_gpus": 1, "attempts_per_s": attempts / drv_s,
         "wall_s": wall, "driver_s": drv_s, "attempts": attempts,
         "unresolved": int(np.count_nonzero(fates == -1)),
         "pB": [round(float(x), 5) for x in res], "pB_err": [round(e, 5) for e in errs],
-        "radii": [round(float(r), 3) for r in radii],
+        "resolved": resolved, "radii": [round(float(r), 3) for r in radii],
         "config": {"workload": f"{ngrid_in} droplet grids L=64 (r~U[4,12], 2% flips), "
                                f"{shots} shots each, beta=0.54, h=0.07, dn=-0.93, up=0.9, "
                                "cap 20000 sweeps, compaction on",
-                   "check_int": args.committor_check, "rng": args.rng,
+                   "check_int": args.committor_check, "rng": rng_kind,
                    "tail_replicas": (args.committor_tail if args.committor_tail >= 0
                                      else "default")},
     }
-    print(json.dumps(line), flush=True)
 
 
-def run_cnn(args):
+def compare_pb(a, b):
+    """Per-grid pB of two independent shooting runs: z-scores of the
+    differences under binomial errors."""
+    pa, pb_ = np.asarray(a["pB"], np.float64), np.asarray(b["pB"], np.float64)
+    na, nb = np.asarray(a["resolved"], np.float64), np.asarray(b["resolved"], np.float64)
+    var = pa * (1 - pa) / np.maximum(na, 1) + pb_ * (1 - pb_) / np.maximum(nb, 1)
+    diff = pa - pb_
+    z = np.where(var > 0, diff / np.sqrt(np.where(var > 0, var, 1.0)), 0.0)
+    return {"grids": int(pa.size), "max_abs_z": float(np.max(np.abs(z))),
+            "n_abs_z_above_3": int(np.count_nonzero(np.abs(z) > 3)),
+            "mean_abs_diff": float(np.mean(np.abs(diff))),
+            "chi2_per_grid": float(np.mean(z ** 2))}
+
+
+def run_committor(args):
+    print(json.dumps(clocked(committor_measure, args)), flush=True)
+
+
+def cnn_measure(args):
     """Surrogate CNN inference throughput: predict() on int8 L=64 grids from
     host memory (batches of 1024), timed on the host around synchronised
     calls, plus one timed Adam step on a 1024-grid batch."""
@@ -438,10 +656,14 @@ def run_cnn(args):
             "config": {"workload": f"predict on {n} int8 L=64 grids (host memory, batches of "
                                    "1024); 4x conv3x3(32) tcgen05, pool, 32->1"}}
     net.close()
-    print(json.dumps(line), flush=True)
+    return line
 
 
-def run_cluster(args):
+def run_cnn(args):
+    print(json.dumps(clocked(cnn_measure, args)), flush=True)
+
+
+def cluster_measure(args):
     """Largest-cluster collective variable on the device: gasp_largest_cluster
     over 32768 L=64 grids, near the site-percolation threshold (p = 0.593,
     the largest and most tangled clusters) and sparse (2 % of sites up, like a
@@ -467,10 +689,14 @@ def run_cluster(args):
             "cases": out,
             "config": {"workload": f"gasp_largest_cluster(spin=+1) on {R} L=64 grids, "
                                    "including the device->host copy of the sizes"}}
-    print(json.dumps(line), flush=True)
+    return line
 
 
-def run_tail(args):
+def run_cluster(args):
+    print(json.dumps(clocked(cluster_measure, args)), flush=True)
+
+
+def tail_measure(args):
     """The end of a committor run: few undecided L=64 replicas (production
     stream unless --tail-rng xorwow).  Per replica count, the time of one sweep with the row
     kernel (one lane per replica, variant 0) and with one warp per replica
@@ -516,10 +742,14 @@ def run_tail(args):
             "config": {"workload": f"L=64 all-down replicas, beta=0.54, h=0.07, "
                                    f"{args.tail_rng} stream, "
                                    f"{per_launch} sweeps per launch; replica counts {counts}"}}
-    print(json.dumps(line), flush=True)
+    return line
 
 
-def run_rate(args):
+def run_tail(args):
+    print(json.dumps(clocked(tail_measure, args)), flush=True)
+
+
+def rate_measure(args):
     """The full production swarm of the headline workload (L=64, 32768
     replicas, beta=0.54, h=0.07, 50 000 sweeps, checks every 100, dumps every
     1000 not written): nucleated-fraction curve fitted to 1 - exp(-k (t - t0))
@@ -556,10 +786,14 @@ def run_rate(args):
                                            "P2000)"},
             "config": {"workload": f"L=64, {R} replicas, beta=0.54, h=0.07, all-down, {tot} "
                                    "sweeps, magnetisation checked every 100 sweeps, up 0.9"}}
-    print(json.dumps(line), flush=True)
+    return line
 
 
-def run_surrogate(args):
+def run_rate(args):
+    print(json.dumps(clocked(rate_measure, args)), flush=True)
+
+
+def surrogate_measure(args):
     """The learned committor surrogate: snapshots from a swarm at beta=0.54,
     h=0.07, shooting labels, GPU training, held-out MAE against 1024-shot
     labels, and screening throughput vs shooting alone."""
@@ -578,10 +812,73 @@ def run_surrogate(args):
                                    f"{res['n_screen']} screened; CNN 4x conv3x3(32)+ReLU, "
                                    "avg-pool, 32->1 sigmoid, batch 1024; fallback "
                                    "|pred-0.5|<0.1 shot with 64 trajectories"}}
-    print(json.dumps(line), flush=True)
+    return line
 
 
-def main():
+def run_surrogate(args):
+    print(json.dumps(clocked(surrogate_measure, args)), flush=True)
+
+
+def secondary_measure(args):
+    """The figures of the metric's second half and of the other north-star
+    configurations, each with its own clock record: committor shooting of
+    the 64 droplet grids on both streams (pB compared), the uneven batch
+    against plain per-group launches, and surrogate screening against
+    shooting alone."""
+    from gpu_2dising_b200 import engine
+    engine.init_device(0)
+    out = {}
+    if args.secondary_quick:  # a short form for development runs
+        args.committor_inputs, args.committor_shots = 16, 1024
+        args.batched_sweeps = 200
+        args.surrogate_train, args.surrogate_test, args.surrogate_screen = 2048, 512, 8192
+        args.surrogate_epochs = 4
+    ex = clocked(committor_measure, args, "xorwow")
+    pr = clocked(committor_measure, args, "mwc64x")
+    keep = ("value", "unit", "attempts_per_s", "wall_s", "unresolved", "clocks")
+    out["committor"] = {
+        "metric": "committor evaluations/s (shooting)", "unit": "grids/s",
+        "workload": ex["config"]["workload"],
+        "exact_stream": {k: ex[k] for k in keep},
+        "production_stream": {k: pr[k] for k in keep},
+        "pB_exact_vs_production": compare_pb(ex, pr),
+        "pB_exact": ex["pB"], "pB_production": pr["pB"]}
+    bt = clocked(batched_measure, args)
+    out["batched"] = {"metric": bt["metric"], "value": bt["value"], "unit": bt["unit"],
+                      "speedup_vs_plain": bt["speedup_vs_plain"],
+                      "plain": bt["plain"], "graph": bt["graph"],
+                      "autotune": bt["config"]["autotune"], "workload": bt["config"]["workload"],
+                      "clocks": bt["clocks"]}
+    su = clocked(surrogate_measure, args)
+    keys = ("value", "unit", "speedup_vs_shooting", "screen_grids_per_s", "shoot_grids_per_s",
+            "cnn_only_grids_per_s", "mae_surrogate", "mae_screened", "mae_shooting_baseline",
+            "fallback_fraction", "test_mid_0.1_0.9", "mae_shooting_by_shots", "n_train",
+            "n_test", "n_screen", "times_s", "clocks")
+    out["surrogate"] = {"metric": su["metric"], **{k: su[k] for k in keys if k in su},
+                        "equal_mae": su.get("by_cap", {}).get("equal_mae"),
+                        "workload": su["config"]["workload"]}
+    out["quick"] = bool(args.secondary_quick)
+    return out
+
+
+def run_secondary(args):
+    print(json.dumps(secondary_measure(args)), flush=True)
+
+
+def spawn_ranks(n, argv):
+    """Runs this script on n ranks of this host (torch.distributed.run), each
+    rank seeing WORLD_SIZE; returns the launcher's exit status."""
+    import socket
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+           f"--nproc-per-node={n}", "--master-addr", "127.0.0.1", f"--master-port={port}",
+           os.path.abspath(__file__), *argv]
+    return subprocess.call(cmd)
+
+
+def main(argv=None):
     global SWEEPS_PER_STEP
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -594,7 +891,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--workload", default="swarm",
                     choices=["swarm", "batched", "committor", "surrogate", "cnn", "rate",
-                             "cluster", "tail"],
+                             "cluster", "tail", "secondary"],
                     help="swarm: the headline single-group swarm; batched: uneven groups; "
                          "committor: seeded droplet shooting")
     ap.add_argument("--cnn-grids", type=int, default=100000)
@@ -618,15 +915,37 @@ def main():
                     help="xorwow: the reference stream (bit-exact); mwc64x: production stream")
     ap.add_argument("--variant", type=int, default=0,
                     help="sweep kernel variant (0 fastest for L, 1 generic) for comparisons")
-    args = ap.parse_args()
+    ap.add_argument("--no-secondary", action="store_true",
+                    help="default line without the secondary block")
+    ap.add_argument("--secondary-quick", action="store_true",
+                    help="secondary block at reduced sizes (development runs)")
+    ap.add_argument("--secondary-timeout", type=int, default=900)
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="reference arm without timing the reference's GPU kernels")
+    ap.add_argument("--cpu-replicas", type=int, default=CPU_CONFIG["replicas"],
+                    help="CPU runs: replicas (default: the CPU configuration's 1248)")
+    ap.add_argument("--cpu-sweeps", type=int, default=CPU_CONFIG["sweeps"],
+                    help="CPU runs: sweeps (default: the CPU configuration's 5000)")
+    ap.add_argument("--dry-run", action="store_true",
+                    help="rank plumbing with a host stand-in step (no GPU, gloo)")
+    argv = sys.argv[1:] if argv is None else list(argv)
+    args = ap.parse_args(argv)
     args.warmup = max(args.warmup, 3)
+    CPU_CONFIG["replicas"], CPU_CONFIG["sweeps"] = args.cpu_replicas, args.cpu_sweeps
     SWEEPS_PER_STEP = args.sweeps_per_step
     CONFIG["sweeps_per_step"] = SWEEPS_PER_STEP
+    if "WORLD_SIZE" not in os.environ and args.gpus > 1 and args.impl == "ours" \
+            and args.workload == "swarm":
+        return spawn_ranks(args.gpus, argv)
     rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
+    world = int(os.environ.get("WORLD_SIZE", str(args.gpus if args.impl == "reference" else 1)))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
-        run_reference(args, rank)
+        run_reference(args, rank, world)
+    elif args.dry_run:
+        run_dry(args, rank, world, local_rank)
+    elif args.workload == "secondary":
+        run_secondary(args)
     elif args.workload == "batched":
         if rank == 0:
             run_batched(args)
@@ -652,4 +971,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    sys.exit(main() or 0)

@@ -12,7 +12,10 @@ import subprocess
 
 PKG_DIR = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(PKG_DIR)
-REFERENCE_SRC = os.environ.get("GASP_REFERENCE_SRC", "/root/reference")
+# The reference checkout (read only): GASP_REFERENCE_SRC, else a "reference"
+# directory beside the repository.
+REFERENCE_SRC = os.path.abspath(
+    os.environ.get("GASP_REFERENCE_SRC", os.path.join(REPO, os.pardir, "reference")))
 
 
 def _make(directory, *targets):

@@ -72,7 +72,6 @@ struct GridsExtra {
   float *d_lclus = nullptr; // largest-cluster sizes [ngrids]
   int *d_cwork = nullptr;   // largest-cluster global work area (large L only)
   size_t cwork_bytes = 0;
-  int mask_ok = 0;          // <= 6 classes with P <= 1 (see k_sweep_rows<kMask>)
   int variant = 0;          // GASP_OPT_SWEEP_VARIANT
   int warps_per_cta = 1;    // GASP_OPT_WARPS_PER_CTA
   int tail_replicas = -1;   // GASP_OPT_TAIL_REPLICAS (-1: the stream's default)
@@ -124,11 +123,6 @@ int ensure_tables(gasp_grids_t *g, double beta, double h) {
   GASP_CUDA(cudaMemcpyAsync(flags, x.d_tab->flags, sizeof flags, cudaMemcpyDeviceToHost, s));
   GASP_CUDA(cudaStreamSynchronize(s));
   x.float_cmp = flags[0] != 0;
-  // A class with P > 1 accepts every draw (u <= 1 < P); the others need a
-  // comparison.  The acceptance-mask row kernel has room for six of those.
-  int cmp_classes = 0;
-  for (int c = 0; c < 10; ++c) cmp_classes += !(hb.pacc[2 * c] > 1.0f);
-  x.mask_ok = cmp_classes <= 6;
   x.beta = beta;
   x.h = h;
   return GASP_OK;
@@ -387,7 +381,10 @@ int gasp_grids_download(gasp_grids_t *g, int *host_grids) {
 int gasp_grids_set_option(gasp_grids_t *g, int option, int value) {
   if (!g) return GASP_ERR_INVALID;
   GridsExtra &x = impl(g)->x;
-  if (option == GASP_OPT_SWEEP_VARIANT && value >= 0 && value <= 9) {
+  // Variants 3, 4 and 8 (pairwise speculation, acceptance mask, two tiles
+  // per warp) were measured slower than variant 0 and have been retired.
+  if (option == GASP_OPT_SWEEP_VARIANT && value >= 0 && value <= 9 && value != 3 &&
+      value != 4 && value != 8) {
     x.variant = value;
     return GASP_OK;
   }
@@ -596,7 +593,6 @@ SweepLaunch base_launch(gasp_grids_t *g) {
   p.pacc_cpu = x.d_tab->pacc_cpu;
   p.float_compare = x.float_cmp;
   p.variant = x.variant;
-  p.mask_ok = x.mask_ok;
   p.lattice_in_global = g->global_lattice;
   p.warps_per_cta = x.warps_per_cta;
   return p;

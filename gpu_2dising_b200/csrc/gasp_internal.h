@@ -82,11 +82,10 @@ struct SweepLaunch {
   float *mag_out;         // optional: magnetisation after the batch [ngrids]
   int float_compare;      // exact mode: compare in float (thresholds unusable)
   int warps_per_cta;      // launch shape (0: default)
-  int variant;            // 0: fastest kernel for L; 1: generic; 2: row kernel, no pairing
+  int variant;            // GASP_OPT_SWEEP_VARIANT (0: fastest kernel for L)
   int rng_kind;           // RngKind of p.rng
   const int *n_active_dev;// optional device count overriding n_active (graph replays)
   int lattice_in_global;  // L beyond shared memory: sweep the lattice in place in HBM
-  int mask_ok;            // at most 6 classes can reject (the acceptance-mask row kernel applies)
   int tail_split;         // > 0: with n live replicas, the one-warp-per-replica kernel runs
                           // only when n <= tail_split and the other kernels only when
                           // n > tail_split (both are enqueued; the choice is made on the

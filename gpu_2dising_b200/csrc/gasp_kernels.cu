@@ -432,300 +432,14 @@ __device__ __forceinline__ void row_attempt(uint32_t &s, Rng &rg, const char *la
   }
 }
 
-// row_attempt split in two for k_sweep_rows2: the probe (loads, pattern,
-// acceptance, the draws) returns the byte offset of the site's word and its new
-// value; the caller stores it.  Same arithmetic and draw order.
-template <int L, bool kFloatCmp, bool kLookahead, typename Rng>
-__device__ __forceinline__ void row_probe(uint32_t &s, Rng &rg, const char *latb, const char *thrb,
-                                          const char *paccb, uint32_t lane4, float shrink,
-                                          uint32_t &off_out, uint32_t &word_out) {
-  constexpr int N = L * L;
-  constexpr int R = L / 32;
-  constexpr bool kPow2 = (L & (L - 1)) == 0;
-  constexpr uint32_t kMask = (uint32_t)(4 * N - 1) & ~127u;  // word part of a byte offset
-  const uint32_t b = s & 31u;
-  uint32_t offc, offu, offd;
-  if constexpr (kPow2) {
-    offc = ((s << 2) & kMask) | lane4;
-    offu = ((offc - 128u * R) & kMask) | lane4;
-    offd = ((offc + 128u * R) & kMask) | lane4;
-  } else {  // rows of R words, R not a power of two: wrap by compare (4N bytes per tile)
-    offc = ((s << 2) & ~127u) | lane4;
-    offu = offc >= 128u * R ? offc - 128u * R : offc + (4u * N - 128u * R);
-    offd = offc + 128u * R < 4u * N ? offc + 128u * R : offc - (4u * N - 128u * R);
-  }
-  const uint32_t wu = *reinterpret_cast<const uint32_t *>(latb + offu);
-  const uint32_t wd = *reinterpret_cast<const uint32_t *>(latb + offd);
-  uint32_t wc, lo, hi;
-  if constexpr (R == 1) {
-    wc = *reinterpret_cast<const uint32_t *>(latb + offc);
-    lo = hi = wc;
-  } else if constexpr (R == 2) {
-    wc = *reinterpret_cast<const uint32_t *>(latb + offc);
-    const uint32_t wx = *reinterpret_cast<const uint32_t *>(latb + (offc ^ 128u));
-    if constexpr (Rng::kKind == kRngXorwow) {
-      // The row is the circular 64 bits (wx:wc) seen from the site's word: for
-      // b >= 3 the bits b-1..b+1 sit in (wx:wc) >> (b-3) (b = 31 reaches wx
-      // bit 0); for b < 3 the left neighbour wraps to the top of wx, so the
-      // pair is read as (wc:wx), whose shift by b+29 lands on the same bits.
-      // One compare instead of two: 4.23e11 vs 4.11e11 attempts/s.
-      const bool wrap = b < 3u;
-      lo = wrap ? wx : wc;
-      hi = wrap ? wc : wx;
-    } else {  // with the MWC64X stream the two-compare form schedules better (4.96e11 vs 4.89e11)
-      lo = (b == 0u) ? wx : wc;
-      hi = (b == 31u) ? wx : wc;
-    }
-  } else {
-    // word of the site within its row
-    const uint32_t wi = kPow2 ? (offc >> 7) & (uint32_t)(R - 1) : (s >> 5) % (uint32_t)R;
-    const uint32_t offl = (b == 0u) ? (wi == 0u ? offc + 128u * (R - 1) : offc - 128u) : offc;
-    const uint32_t offr =
-        (b == 31u) ? (wi == (uint32_t)(R - 1) ? offc - 128u * (R - 1) : offc + 128u) : offc;
-    lo = *reinterpret_cast<const uint32_t *>(latb + offl);
-    hi = *reinterpret_cast<const uint32_t *>(latb + offr);
-    wc = (b == 0u) ? hi : lo;
-  }
-  const uint32_t t = __funnelshift_r(lo, hi, b + 29u);  // bits 2,3,4: left, centre, right
-  const uint32_t u = __funnelshift_r(wu, wu, b + 27u);  // bit 5: up
-  const uint32_t d = __funnelshift_r(wd, wd, b + 26u);  // bit 6: down
-  const uint32_t p4 = (t & 0x1Cu) | (u & 0x20u) | (d & 0x40u);
-  const uint32_t x2 = rg.next();
-  const uint32_t sc = s;
-  if constexpr (kLookahead) s = rg.template site<N>(shrink, N);
-  bool acc;
-  if constexpr (kFloatCmp) {
-    acc = _curand_uniform(x2) < *reinterpret_cast<const float *>(paccb + p4);
-  } else {
-    acc = x2 <= *reinterpret_cast<const uint32_t *>(thrb + p4);
-  }
-  off_out = offc;
-  word_out = acc ? wc ^ (1u << (sc & 31u)) : wc;  // written back unchanged when rejected
-}
-
-
-// row_attempt with the threshold lookup taken off the dependency chain.  For
-// the raw acceptance draw x2, the accepted classes are those whose threshold
-// is >= x2; with the classes sorted by threshold that is a suffix of the
-// order, so one count r = #{i < 6 : x2 <= S_i} over the six smallest
-// thresholds S (every other class has P > 1 and accepts everything) selects
-// a 32-bit mask pm[r] of accepted 5-spin patterns.  r and pm[r] depend only
-// on the draw, so they are computed while the lattice loads are in flight;
-// the attempt's own chain ends in a shift of that mask by the pattern.
-// Bit-identical to the table lookup: the same "x2 <= thr[class]" decisions.
-template <int L, bool kLookahead, typename Rng>
-__device__ __forceinline__ void row_attempt_mask(uint32_t &s, Rng &rg, const char *latb,
-                                                 const uint32_t (&S)[6], const uint32_t *pm,
-                                                 uint32_t lane4, float shrink) {
-  constexpr int N = L * L;
-  constexpr int R = L / 32;
-  constexpr uint32_t kMask = (uint32_t)(4 * N - 1) & ~127u;
-  const uint32_t b = s & 31u;
-  const uint32_t offc = ((s << 2) & kMask) | lane4;
-  const uint32_t offu = ((offc - 128u * R) & kMask) | lane4;
-  const uint32_t offd = ((offc + 128u * R) & kMask) | lane4;
-  const uint32_t wu = *reinterpret_cast<const uint32_t *>(latb + offu);
-  const uint32_t wd = *reinterpret_cast<const uint32_t *>(latb + offd);
-  uint32_t wc, lo, hi;
-  if constexpr (R == 1) {
-    wc = *reinterpret_cast<const uint32_t *>(latb + offc);
-    lo = hi = wc;
-  } else if constexpr (R == 2) {
-    wc = *reinterpret_cast<const uint32_t *>(latb + offc);
-    const uint32_t wx = *reinterpret_cast<const uint32_t *>(latb + (offc ^ 128u));
-    lo = (b == 0u) ? wx : wc;
-    hi = (b == 31u) ? wx : wc;
-  } else {
-    const uint32_t wi = (offc >> 7) & (uint32_t)(R - 1);
-    const uint32_t offl = (b == 0u) ? (wi == 0u ? offc + 128u * (R - 1) : offc - 128u) : offc;
-    const uint32_t offr =
-        (b == 31u) ? (wi == (uint32_t)(R - 1) ? offc - 128u * (R - 1) : offc + 128u) : offc;
-    lo = *reinterpret_cast<const uint32_t *>(latb + offl);
-    hi = *reinterpret_cast<const uint32_t *>(latb + offr);
-    wc = (b == 0u) ? hi : lo;
-  }
-  const uint32_t x2 = rg.next();
-  const uint32_t r = (uint32_t)(x2 <= S[0]) + (uint32_t)(x2 <= S[1]) + (uint32_t)(x2 <= S[2]) +
-                     (uint32_t)(x2 <= S[3]) + (uint32_t)(x2 <= S[4]) + (uint32_t)(x2 <= S[5]);
-  const uint32_t m = pm[r];
-  const uint32_t sc = s;
-  if constexpr (kLookahead) s = rg.template site<N>(shrink, N);
-  const uint32_t t = __funnelshift_r(lo, hi, b + 31u);  // bits 0,1,2: left, centre, right
-  const uint32_t u = __funnelshift_r(wu, wu, b + 29u);  // bit 3: up
-  const uint32_t d = __funnelshift_r(wd, wd, b + 28u);  // bit 4: down
-  const uint32_t pat = (t & 7u) | (u & 8u) | (d & 16u);
-  if ((m >> pat) & 1u)
-    *reinterpret_cast<uint32_t *>(const_cast<char *>(latb) + offc) = wc ^ (1u << (sc & 31u));
-}
-
-// The shared-memory words one attempt reads, and its 5-spin pattern.
-struct Probe {
-  uint32_t offc;  // byte offset of the centre word
-  uint32_t wc;    // centre word as loaded
-  uint32_t p4;    // pattern * 4 (left, centre, right, up, down at bits 2..6)
-  uint32_t bit;   // 1 << (site & 31)
-};
-
-template <int L>
-__device__ __forceinline__ Probe row_probe(uint32_t s, const char *latb, uint32_t lane4) {
-  constexpr int N = L * L;
-  constexpr int R = L / 32;
-  constexpr uint32_t kMask = (uint32_t)(4 * N - 1) & ~127u;
-  Probe q;
-  const uint32_t b = s & 31u;
-  q.bit = 1u << b;
-  q.offc = ((s << 2) & kMask) | lane4;
-  const uint32_t offu = ((q.offc - 128u * R) & kMask) | lane4;
-  const uint32_t offd = ((q.offc + 128u * R) & kMask) | lane4;
-  const uint32_t wu = *reinterpret_cast<const uint32_t *>(latb + offu);
-  const uint32_t wd = *reinterpret_cast<const uint32_t *>(latb + offd);
-  uint32_t lo, hi;
-  if constexpr (R == 1) {
-    q.wc = *reinterpret_cast<const uint32_t *>(latb + q.offc);
-    lo = hi = q.wc;
-  } else if constexpr (R == 2) {
-    q.wc = *reinterpret_cast<const uint32_t *>(latb + q.offc);
-    const uint32_t wx = *reinterpret_cast<const uint32_t *>(latb + (q.offc ^ 128u));
-    lo = (b == 0u) ? wx : q.wc;
-    hi = (b == 31u) ? wx : q.wc;
-  } else {
-    const uint32_t wi = (q.offc >> 7) & (uint32_t)(R - 1);
-    const uint32_t offl =
-        (b == 0u) ? (wi == 0u ? q.offc + 128u * (R - 1) : q.offc - 128u) : q.offc;
-    const uint32_t offr =
-        (b == 31u) ? (wi == (uint32_t)(R - 1) ? q.offc - 128u * (R - 1) : q.offc + 128u) : q.offc;
-    lo = *reinterpret_cast<const uint32_t *>(latb + offl);
-    hi = *reinterpret_cast<const uint32_t *>(latb + offr);
-    q.wc = (b == 0u) ? hi : lo;
-  }
-  const uint32_t t = __funnelshift_r(lo, hi, b + 29u);
-  const uint32_t u = __funnelshift_r(wu, wu, b + 27u);
-  const uint32_t d = __funnelshift_r(wd, wd, b + 26u);
-  q.p4 = (t & 0x1Cu) | (u & 0x20u) | (d & 0x40u);
-  return q;
-}
-
-template <bool kFloatCmp>
-__device__ __forceinline__ bool row_accept(uint32_t x2, uint32_t p4, const char *thrb,
-                                           const char *paccb) {
-  if constexpr (kFloatCmp) return _curand_uniform(x2) < *reinterpret_cast<const float *>(paccb + p4);
-  else return x2 <= *reinterpret_cast<const uint32_t *>(thrb + p4);
-}
-
-// Could site sa be one of the five sites attempt sb reads (sb, its left,
-// right, up, down neighbours, rows and columns periodic)?  Conservative: also
-// true for the two diagonal offsets L-1 and N-L+1.
-template <int L>
-__device__ __forceinline__ bool row_collide(uint32_t sa, uint32_t sb) {
-  constexpr uint32_t N = (uint32_t)(L * L);
-  const uint32_t e = (sa - sb + 1u) & (N - 1u);  // (sa - sb) + 1 mod N
-  return (e <= 2u) | ((e - (uint32_t)L) <= 1u) | ((e - (N - (uint32_t)L + 1u)) <= 1u);
-}
-
-// Two consecutive attempts (a, b) of every lane.  Unless some lane's attempt
-// a touches a site attempt b reads, both are evaluated on the lattice as it
-// was before the pair and their flips applied in order (b's store forwards a's
-// flip when both flip the same word); otherwise the warp runs them in order.
-// Either way each replica sees exactly the sequential result.
-template <int L, bool kFloatCmp>
-__device__ __forceinline__ void row_pair(uint32_t sa, uint32_t x2a, uint32_t sb, uint32_t x2b,
-                                         const char *latb, const char *thrb, const char *paccb,
-                                         uint32_t lane4) {
-  char *latw = const_cast<char *>(latb);
-  const bool coll = row_collide<L>(sa, sb);
-  const Probe A = row_probe<L>(sa, latb, lane4);
-  if (!__any_sync(__activemask(), coll)) {
-    const Probe B = row_probe<L>(sb, latb, lane4);
-    const bool acc_a = row_accept<kFloatCmp>(x2a, A.p4, thrb, paccb);
-    const bool acc_b = row_accept<kFloatCmp>(x2b, B.p4, thrb, paccb);
-    const uint32_t fa = acc_a ? A.bit : 0u;
-    if (acc_a) *reinterpret_cast<uint32_t *>(latw + A.offc) = A.wc ^ A.bit;
-    const uint32_t wcb = B.wc ^ ((B.offc == A.offc) ? fa : 0u);
-    if (acc_b) *reinterpret_cast<uint32_t *>(latw + B.offc) = wcb ^ B.bit;
-  } else {
-    if (row_accept<kFloatCmp>(x2a, A.p4, thrb, paccb))
-      *reinterpret_cast<uint32_t *>(latw + A.offc) = A.wc ^ A.bit;
-    const Probe B = row_probe<L>(sb, latb, lane4);
-    if (row_accept<kFloatCmp>(x2b, B.p4, thrb, paccb))
-      *reinterpret_cast<uint32_t *>(latw + B.offc) = B.wc ^ B.bit;
-  }
-}
-
-// k_sweep_rows with pairwise speculation (see row_pair).  The four draws of
-// the next pair are made during the current pair, in the reference's order.
-template <int L, bool kStatic, bool kFloatCmp, int kRng>
-__global__ void __launch_bounds__(32) k_sweep_rows_pair(SweepLaunch p) {
-  static_assert(L % 32 == 0 && (L & (L - 1)) == 0, "L must be a power of two >= 32");
-  constexpr int N = L * L;
-  constexpr int W = N / 32;
-  __shared__ __align__(16) uint32_t thrP[32];
-  __shared__ __align__(16) float paccP[32];
-  extern __shared__ __align__(16) uint32_t dyn[];
-  uint32_t *lat = LatticeStore<W * kTile, kStatic>::get(dyn);
-
-  const int lane = threadIdx.x;
-  {
-    const int c = (lane >> 1) & 1;
-    const int cls = 5 * c + __popc(lane & 0x1D);
-    thrP[lane] = p.thr[cls];
-    paccP[lane] = p.pacc_f[2 * cls];
-  }
-  const int n_act = live_count(p);
-  const int tile = blockIdx.x;
-  if (tile * kTile >= n_act) return;  // whole CTA (one warp) idle this batch
-  const int slot = tile * kTile + lane;
-  const bool live = slot < n_act;
-  const int rep = live ? (p.active ? p.active[slot] : slot) : 0;
-  stage_in(lat, p, W, tile, lane, live, rep);
-  __syncwarp();
-
-  const char *latb = reinterpret_cast<const char *>(lat);
-  const char *thrb = reinterpret_cast<const char *>(thrP);
-  const char *paccb = reinterpret_cast<const char *>(paccP);
-  if (live && p.nsweeps > 0) {
-    RngPolicy<kRng> rg;
-    rg.load(p.rng, p.rng_stride, rep);
-    const float shrink = (1.0f - FLT_EPSILON) * (float)N;
-    const uint32_t lane4 = (uint32_t)lane << 2;
-    // N is even, so a batch is a whole number of pairs.
-    uint32_t sa = rg.template site<N>(shrink, N);
-    uint32_t x2a = rg.next();
-    uint32_t sb = rg.template site<N>(shrink, N);
-    uint32_t x2b = rg.next();
-    const int pairs = (N / 2) * p.nsweeps;
-#pragma unroll 2
-    for (int k = 0; k < pairs - 1; ++k) {
-      const uint32_t na = rg.template site<N>(shrink, N);
-      const uint32_t nxa = rg.next();
-      const uint32_t nb = rg.template site<N>(shrink, N);
-      const uint32_t nxb = rg.next();
-      row_pair<L, kFloatCmp>(sa, x2a, sb, x2b, latb, thrb, paccb, lane4);
-      sa = na;
-      x2a = nxa;
-      sb = nb;
-      x2b = nxb;
-    }
-    row_pair<L, kFloatCmp>(sa, x2a, sb, x2b, latb, thrb, paccb, lane4);
-    rg.store(p.rng, p.rng_stride, rep);
-  }
-  __syncwarp();
-  epilogue_mag(lat + lane, p, N, W, live, rep);
-  stage_out(lat, p, W, tile, lane, live, rep);
-}
-
-template <int L, bool kStatic, bool kFloatCmp, int kRng, bool kMask = false,
-          bool kStoreAlways = false, bool kBulk = false>
+template <int L, bool kStatic, bool kFloatCmp, int kRng, bool kStoreAlways = false,
+          bool kBulk = false>
 __global__ void __launch_bounds__(32) k_sweep_rows(SweepLaunch p) {
   static_assert(L % 32 == 0, "rows of whole words");
-  static_assert(!kMask || (L & (L - 1)) == 0, "the acceptance-mask kernel needs L a power of two");
-  static_assert(!(kMask && kFloatCmp), "the acceptance mask needs integer thresholds");
   constexpr int N = L * L;
   constexpr int W = N / 32;
   __shared__ __align__(16) uint32_t thrP[32];   // threshold by 5-spin pattern
   __shared__ __align__(16) float paccP[32];     // float table by pattern
-  __shared__ uint32_t sortS[16];                // kMask: thresholds in ascending order
-  __shared__ int sortC[16];                     // kMask: their classes
-  __shared__ uint32_t pmS[8];                   // kMask: accepted-pattern masks by count
   extern __shared__ __align__(16) uint32_t dyn[];
   uint32_t *lat = LatticeStore<W * kTile, kStatic>::get(dyn);
 
@@ -736,32 +450,6 @@ __global__ void __launch_bounds__(32) k_sweep_rows(SweepLaunch p) {
     const int cls = 5 * c + __popc(lane & 0x1D);
     thrP[lane] = p.thr[cls];
     paccP[lane] = p.pacc_f[2 * cls];
-  }
-  uint32_t S[6];
-  if constexpr (kMask) {
-    if (lane < 10) {  // rank of class `lane` by (threshold, class)
-      const uint32_t v = p.thr[lane];
-      int rank = 0;
-      for (int j = 0; j < 10; ++j) {
-        const uint32_t w = p.thr[j];
-        rank += (w < v || (w == v && j < lane)) ? 1 : 0;
-      }
-      sortS[rank] = v;
-      sortC[rank] = lane;
-    }
-    __syncwarp();
-    if (lane < 7) {  // count r accepts the classes of ranks 6-r .. 9
-      uint32_t m = 0;
-      for (int q = 0; q < 32; ++q) {
-        const int cls = 5 * ((q >> 1) & 1) + __popc(q & 0x1D);
-        for (int j = 6 - lane; j < 10; ++j)
-          if (sortC[j] == cls) m |= 1u << q;
-      }
-      pmS[lane] = m;
-    }
-    __syncwarp();
-#pragma unroll
-    for (int i = 0; i < 6; ++i) S[i] = sortS[i];
   }
   const int n_act = live_count(p);
   const int tile = blockIdx.x;
@@ -794,12 +482,7 @@ __global__ void __launch_bounds__(32) k_sweep_rows(SweepLaunch p) {
     // x1(a+1), ... as in the reference.  The host keeps N*nsweeps < 2^31.
     uint32_t s = rg.template site<N>(shrink, N);
     const int total = N * p.nsweeps;
-    if constexpr (kMask) {
-#pragma unroll 5
-      for (int a = 0; a < total - 1; ++a)
-        row_attempt_mask<L, true>(s, rg, latb, S, pmS, lane4, shrink);
-      row_attempt_mask<L, false>(s, rg, latb, S, pmS, lane4, shrink);
-    } else if constexpr (L == 64 && kRng == kRngXorwow) {
+    if constexpr (L == 64 && kRng == kRngXorwow) {
       // unroll measured at L=64 on the reference stream: 8 -> 4.40e11, 5 -> 4.23e11,
       // 16 -> 4.36e11, 10 -> 4.28e11 attempts/s (the MWC64X stream is fastest at 5)
 #pragma unroll 8
@@ -833,85 +516,6 @@ __global__ void __launch_bounds__(32) k_sweep_rows(SweepLaunch p) {
       stage_out(lat, p, W, tile, lane, live, rep);
   } else {
     stage_out(lat, p, W, tile, lane, live, rep);
-  }
-}
-
-// Two tiles per warp: each lane sweeps one replica of tile 2b and one of tile
-// 2b+1, the two attempts of a step probed before either is stored, so the
-// two replicas' dependency chains overlap in one thread (instruction-level
-// parallelism in place of a second warp on the scheduler).  Per replica the
-// attempts and draws are exactly those of k_sweep_rows.  Lanes without a
-// replica in the second tile sweep a zeroed scratch copy and store nothing
-// back.
-template <int L, bool kStatic, bool kFloatCmp, int kRng>
-__global__ void __launch_bounds__(32) k_sweep_rows2(SweepLaunch p) {
-  static_assert(L % 32 == 0, "rows of whole words");
-  constexpr int N = L * L;
-  constexpr int W = N / 32;
-  __shared__ __align__(16) uint32_t thrP[32];
-  __shared__ __align__(16) float paccP[32];
-  extern __shared__ __align__(16) uint32_t dyn[];
-  uint32_t *lat = LatticeStore<2 * W * kTile, kStatic>::get(dyn);
-
-  const int lane = threadIdx.x;
-  {
-    const int c = (lane >> 1) & 1;
-    const int cls = 5 * c + __popc(lane & 0x1D);
-    thrP[lane] = p.thr[cls];
-    paccP[lane] = p.pacc_f[2 * cls];
-  }
-  const int n_act = live_count(p);
-  const int tileA = 2 * blockIdx.x, tileB = tileA + 1;
-  if (tileA * kTile >= n_act) return;  // whole CTA idle this batch
-  const int slotA = tileA * kTile + lane, slotB = tileB * kTile + lane;
-  const bool liveA = slotA < n_act, liveB = slotB < n_act;
-  const int repA = liveA ? (p.active ? p.active[slotA] : slotA) : 0;
-  const int repB = liveB ? (p.active ? p.active[slotB] : slotB) : 0;
-  uint32_t *latA = lat, *latB = lat + W * kTile;
-  const bool tileB_live = tileB * kTile < n_act;
-  stage_in(latA, p, W, tileA, lane, liveA, repA);
-  if (tileB_live) {
-    stage_in(latB, p, W, tileB, lane, liveB, repB);
-  } else {
-    for (int w = 0; w < W; ++w) latB[w * kTile + lane] = 0u;
-  }
-  __syncwarp();
-
-  char *latbA = reinterpret_cast<char *>(latA);
-  char *latbB = reinterpret_cast<char *>(latB);
-  const char *thrb = reinterpret_cast<const char *>(thrP);
-  const char *paccb = reinterpret_cast<const char *>(paccP);
-  if (liveA && p.nsweeps > 0) {
-    RngPolicy<kRng> ra, rb;
-    ra.load(p.rng, p.rng_stride, repA);
-    if (liveB) rb.load(p.rng, p.rng_stride, repB);
-    else rb.load(p.rng, p.rng_stride, repA);  // a stand-in stream; nothing of B is kept
-    const float shrink = (1.0f - FLT_EPSILON) * (float)N;
-    const uint32_t lane4 = (uint32_t)lane << 2;
-    uint32_t sa = ra.template site<N>(shrink, N);
-    uint32_t sb = rb.template site<N>(shrink, N);
-    const int total = N * p.nsweeps;
-    uint32_t oa, wa, ob, wb;
-#pragma unroll 2
-    for (int a = 0; a < total - 1; ++a) {
-      row_probe<L, kFloatCmp, true>(sa, ra, latbA, thrb, paccb, lane4, shrink, oa, wa);
-      row_probe<L, kFloatCmp, true>(sb, rb, latbB, thrb, paccb, lane4, shrink, ob, wb);
-      *reinterpret_cast<uint32_t *>(latbA + oa) = wa;
-      *reinterpret_cast<uint32_t *>(latbB + ob) = wb;
-    }
-    row_probe<L, kFloatCmp, false>(sa, ra, latbA, thrb, paccb, lane4, shrink, oa, wa);
-    row_probe<L, kFloatCmp, false>(sb, rb, latbB, thrb, paccb, lane4, shrink, ob, wb);
-    *reinterpret_cast<uint32_t *>(latbA + oa) = wa;
-    *reinterpret_cast<uint32_t *>(latbB + ob) = wb;
-    ra.store(p.rng, p.rng_stride, repA);
-    if (liveB) rb.store(p.rng, p.rng_stride, repB);
-  }
-  __syncwarp();
-  epilogue_mag(latA + lane, p, N, W, liveA, repA);
-  stage_out(latA, p, W, tileA, lane, liveA, repA);
-  if (tileB_live) {
-    epilogue_mag(latB + lane, p, N, W, liveB, repB);
-    stage_out(latB, p, W, tileB, lane, liveB, repB);
   }
 }
 
@@ -1109,18 +713,6 @@ int launch_rows(Kern kern, const SweepLaunch &p, size_t dyn_smem, cudaStream_t s
   return GASP_OK;
 }
 
-// k_sweep_rows2: one warp per CTA and two tiles per warp.
-template <typename Kern>
-int launch_rows2(Kern kern, const SweepLaunch &p, size_t dyn_smem, cudaStream_t s) {
-  const int tiles = tiles_for(p.n_active);
-  if (tiles == 0) return GASP_OK;
-  if (dyn_smem > 0)
-    GASP_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_smem));
-  kern<<<(tiles + 1) / 2, 32, dyn_smem, s>>>(p);
-  GASP_CUDA(cudaGetLastError());
-  return GASP_OK;
-}
-
 template <bool F, int K>
 int dispatch_kind(const SweepLaunch &p, cudaStream_t s) {
   if (p.lattice_in_global) {
@@ -1129,16 +721,6 @@ int dispatch_kind(const SweepLaunch &p, cudaStream_t s) {
     GASP_CUDA(cudaGetLastError());
     return GASP_OK;
   }
-  if (p.variant == 8) {  // two tiles per warp
-    switch (p.L) {
-      case 32: return launch_rows2(k_sweep_rows2<32, true, F, K>, p, 0, s);
-      case 64: return launch_rows2(k_sweep_rows2<64, false, F, K>, p,
-                                   2 * (size_t)words_per_replica(64) * kTile * 4, s);
-      case 128: return launch_rows2(k_sweep_rows2<128, false, F, K>, p,
-                                    2 * (size_t)words_per_replica(128) * kTile * 4, s);
-      default: break;  // other L: the default kernels
-    }
-  }
   if (p.variant == 6) return launch_sweep_tail(p, s);    // one warp per replica (MWC64X)
   if (p.variant == 7) return launch_sweep_shared(p, s);  // shared site per tile (MWC64X)
   if (p.variant == 1) {  // the generic kernel, kept selectable for comparisons
@@ -1146,38 +728,22 @@ int dispatch_kind(const SweepLaunch &p, cudaStream_t s) {
   }
   const size_t dyn128 = (size_t)words_per_replica(128) * kTile * sizeof(uint32_t);
   const size_t dyn96 = (size_t)words_per_replica(96) * kTile * sizeof(uint32_t);
-  if (p.variant == 3) {  // row kernel with pairwise speculation (measured slower)
-    switch (p.L) {
-      case 32: return launch_rows(k_sweep_rows_pair<32, true, F, K>, p, 0, s);
-      case 64: return launch_rows(k_sweep_rows_pair<64, true, F, K>, p, 0, s);
-      case 128: return launch_rows(k_sweep_rows_pair<128, false, F, K>, p, dyn128, s);
-      default: break;
-    }
-  }
-  if (p.variant == 4 && p.mask_ok && !F) {  // row kernel with the acceptance mask
-    switch (p.L) {
-      case 32: return launch_rows(k_sweep_rows<32, true, false, K, true>, p, 0, s);
-      case 64: return launch_rows(k_sweep_rows<64, true, false, K, true>, p, 0, s);
-      case 128: return launch_rows(k_sweep_rows<128, false, false, K, true>, p, dyn128, s);
-      default: break;
-    }
-  }
   if (p.variant == 9) {  // variant 0 with bulk-copy staging of the tiles (measured slower)
     switch (p.L) {
-      case 32: return launch_rows(k_sweep_rows<32, true, F, K, false, true, true>, p, 0, s);
-      case 64: return launch_rows(k_sweep_rows<64, true, F, K, false, true, true>, p, 0, s);
-      case 96: return launch_rows(k_sweep_rows<96, false, F, K, false, true, true>, p, dyn96, s);
+      case 32: return launch_rows(k_sweep_rows<32, true, F, K, true, true>, p, 0, s);
+      case 64: return launch_rows(k_sweep_rows<64, true, F, K, true, true>, p, 0, s);
+      case 96: return launch_rows(k_sweep_rows<96, false, F, K, true, true>, p, dyn96, s);
       case 128:
-        return launch_rows(k_sweep_rows<128, false, F, K, false, true, true>, p, dyn128, s);
+        return launch_rows(k_sweep_rows<128, false, F, K, true, true>, p, dyn128, s);
       default: break;  // other L: the default kernels
     }
   }
   if (p.variant == 0) {  // the row kernel writing the centre word back on every attempt
     switch (p.L) {
-      case 32: return launch_rows(k_sweep_rows<32, true, F, K, false, true>, p, 0, s);
-      case 64: return launch_rows(k_sweep_rows<64, true, F, K, false, true>, p, 0, s);
-      case 96: return launch_rows(k_sweep_rows<96, false, F, K, false, true>, p, dyn96, s);
-      case 128: return launch_rows(k_sweep_rows<128, false, F, K, false, true>, p, dyn128, s);
+      case 32: return launch_rows(k_sweep_rows<32, true, F, K, true>, p, 0, s);
+      case 64: return launch_rows(k_sweep_rows<64, true, F, K, true>, p, 0, s);
+      case 96: return launch_rows(k_sweep_rows<96, false, F, K, true>, p, dyn96, s);
+      case 128: return launch_rows(k_sweep_rows<128, false, F, K, true>, p, dyn128, s);
       default: break;
     }
   }

@@ -67,8 +67,10 @@ extern "C" int gasp_grids_upload_inputs_noalloc(gasp_grids_t *g, const int *inpu
   cudaStream_t s = gasp::current_stream();
   GASP_CUDA(cudaMemcpyAsync(stage, inputs, (size_t)need * sizeof(int), cudaMemcpyHostToDevice, s));
   rc = gasp::launch_pack_grids(stage, g->d_lat, g->L, g->ngrids, s, g->ngrids / ninputs);
+  // The stage is free for the next call once this returns: wait for the copy
+  // on the error path too, then report the first error.
+  const cudaError_t se = cudaStreamSynchronize(s);
   if (rc) return rc;
-  // The stage is free for the next call once this returns.
-  GASP_CUDA(cudaStreamSynchronize(s));
+  if (se != cudaSuccess) return gasp::cuda_fail(se, "cudaStreamSynchronize", __FILE__, __LINE__);
   return GASP_OK;
 }

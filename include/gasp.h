@@ -99,8 +99,11 @@ int gasp_grids_upload_inputs(gasp_grids_t *grids, const int *inputs, int ninputs
  * - ninputs * L * L above GASP_NOALLOC_MAX_INPUT_INTS -> GASP_ERR_INVALID
  *   with a message naming the limit; nothing is copied.
  * - Nothing has to start at zero: each call overwrites the staged inputs.
- * - The first call on each device looks up the array's device address; make
- *   that first call before any stream capture.
+ * - The first call on each device looks up the array's device address and
+ *   keeps it for the life of the process; make that first call before any
+ *   stream capture.  After cudaDeviceReset the kept address is stale: a
+ *   process that resets a device must not call this function again.
+ * - Like the other gasp_grids_* calls, it leaves grids->device current.
  * - There is one array per device: calls that overlap in time (two host
  *   threads, or a call while another is still running) race on it.  Calls
  *   that follow one another are safe, as each waits for its copy and pack
@@ -115,10 +118,7 @@ int gasp_grids_shape(const gasp_grids_t *grids, int *L_out, int *ngrids_out);
  * stream's draws to attempts differently: same dynamics, other trajectories).  GASP_OPT_SWEEP_VARIANT: 0 the fastest kernel for L (default: for
  * L = 32, 64, 96, 128 the row kernel writing the centre word back on every
  * attempt, no divergent branch), 1 the generic kernel, 2 the row kernel with a
- * store only on acceptance, 3 the row kernel with pairwise
- * speculation of consecutive attempts, 4 the row kernel with the acceptance
- * decided by a per-draw mask of accepted neighbourhoods (falls back to 2 when
- * more than six classes can reject; L = 32, 64, 128 only), 5 the generic
+ * store only on acceptance, 5 the generic
  * kernel writing the centre word back on every attempt, 6 one warp per
  * replica (3 <= L <= 512; GASP_ERR_UNSUPPORTED otherwise): the warp applies
  * up to 32 queued attempts of its replica per step, all those that touch no
@@ -132,15 +132,14 @@ int gasp_grids_shape(const gasp_grids_t *grids, int *L_out, int *ngrids_out);
  * list; GASP_ERR_UNSUPPORTED otherwise): the 32 replicas of a tile share each
  * attempt's site, held as one word per site, neighbour counts by bitwise
  * full adders, per-replica acceptance draws, a ballot flip mask -- replicas
- * of a tile are correlated; about half the throughput of variant 0; 8 the
- * row kernel with two tiles per warp (L = 32, 64, 128; each lane runs the
- * two replicas' attempts interleaved; bit-identical to 0, measured slower);
+ * of a tile are correlated; about half the throughput of variant 0;
  * 9 variant 0 with each tile staged between HBM and shared memory by one
  * bulk copy (cp.async.bulk, completion on an mbarrier) instead of per-lane
  * loads and stores (L = 32, 64, 96, 128 in replica order, i.e. without an
  * active list; bit-identical to 0, measured slower; each launch reads back
  * a device flag, so a copy that did not complete within its bounded wait
- * returns GASP_ERR_TIMEOUT).
+ * returns GASP_ERR_TIMEOUT).  Values 3, 4 and 8 (retired kernels that were
+ * measured slower) and values outside 0..9 return GASP_ERR_INVALID.
  * GASP_OPT_WARPS_PER_CTA: tiles per CTA of the generic kernel (1..8).
  * GASP_OPT_TAIL_REPLICAS: device-side committor shooting (itask 1 with
  * compaction) sweeps with variant 6 once at most this many replicas are

@@ -5,8 +5,14 @@
  * core (the reference's MT19937 state is a process global) for its CPU
  * baseline and its `--impl reference` arm.
  *
- * usage: ref_cpu_bench L ngrids nsweeps mag_output_int beta h seed
- * prints one line to stderr: "<attempts> <wall_seconds>"
+ * usage: ref_cpu_bench L ngrids nsweeps mag_output_int beta h seed [grid_output_int]
+ * prints two lines to stderr:
+ *   "<attempts> <wall_seconds>"  attempts actually made (the driver stops
+ *                                early once every replica has nucleated)
+ *   "T <t0> <isweep> <t> ..."    CLOCK_MONOTONIC seconds at the start and at
+ *                                each output callback (every grid_output_int
+ *                                sweeps, before that batch is swept), so a
+ *                                caller can cut one run into steps
  */
 #include <stdio.h>
 #include <stdlib.h>
@@ -16,20 +22,41 @@
 #include "mc_cpu.h"
 #include "grid.h"
 
-static int null_outfunc(int L, int ngrids, int *grid_data, int isweep, float *m,
+#define MAX_MARKS 4096
+static int n_marks = 0;
+static int mark_sweep[MAX_MARKS];
+static double mark_time[MAX_MARKS];
+
+static double now_s(void) {
+  struct timespec t;
+  clock_gettime(CLOCK_MONOTONIC, &t);
+  return (double)t.tv_sec + 1e-9 * (double)t.tv_nsec;
+}
+
+/* Output callback: writes nothing, records when each batch starts. */
+static int mark_outfunc(int L, int ngrids, int *grid_data, int isweep, float *m,
                         float *lc, char *cv, double dn, double up, char *fn) {
-  (void)L; (void)ngrids; (void)grid_data; (void)isweep; (void)m; (void)lc;
+  (void)L; (void)ngrids; (void)grid_data; (void)m; (void)lc;
   (void)cv; (void)dn; (void)up; (void)fn;
+  if (n_marks < MAX_MARKS) {
+    mark_sweep[n_marks] = isweep;
+    mark_time[n_marks] = now_s();
+    n_marks++;
+  }
   return 0;
 }
 
 int main(int argc, char **argv) {
-  if (argc != 8) {
-    fprintf(stderr, "usage: ref_cpu_bench L ngrids nsweeps mag_output_int beta h seed\n");
+  if (argc != 8 && argc != 9) {
+    fprintf(stderr,
+            "usage: ref_cpu_bench L ngrids nsweeps mag_output_int beta h seed [grid_output_int]\n");
     return 2;
   }
   int L = atoi(argv[1]), ngrids = atoi(argv[2]), nsweeps = atoi(argv[3]);
   int mag = atoi(argv[4]);
+  int gint = argc == 9 ? atoi(argv[8]) : mag;
+  if (L < 1 || ngrids < 1 || nsweeps < 1 || mag < 1 || gint < 1) return 2;
+  const int spc = mag < gint ? mag : gint;  /* sweeps per batch, src/mc_cpu.c:140 */
   double beta = atof(argv[5]), h = atof(argv[6]);
   unsigned long seed = strtoul(argv[7], NULL, 10);
 
@@ -39,19 +66,25 @@ int main(int argc, char **argv) {
   preComputeProbs_cpu(beta, h);
 
   mc_grids_t g; g.L = L; g.ngrids = ngrids; g.ising_grids = grids;
-  mc_sampler_t s; s.tot_nsweeps = nsweeps; s.mag_output_int = mag; s.grid_output_int = mag;
+  mc_sampler_t s; s.tot_nsweeps = nsweeps; s.mag_output_int = mag; s.grid_output_int = gint;
   mc_function_t c; memset(&c, 0, sizeof c);
   c.itask = 0; c.dn_thr = -0.90; c.up_thr = 0.90; c.ninputs = 1; c.initial_spin = -1;
   c.cv = (char *)"magnetisation"; c.result = result; c.filename = (char *)"/dev/null";
 
   if (!freopen("/dev/null", "w", stdout)) return 3;
-  struct timespec t0, t1;
-  clock_gettime(CLOCK_MONOTONIC, &t0);
-  mc_driver_cpu(g, beta, h, NULL, s, c, null_outfunc);
-  clock_gettime(CLOCK_MONOTONIC, &t1);
-  double wall = (double)(t1.tv_sec - t0.tv_sec) + 1e-9 * (double)(t1.tv_nsec - t0.tv_nsec);
-  double attempts = (double)L * L * (double)ngrids * (double)nsweeps;
-  fprintf(stderr, "%.0f %.6f\n", attempts, wall);
+  const double t0 = now_s();
+  mc_driver_cpu(g, beta, h, NULL, s, c, mark_outfunc);
+  const double t1 = now_s();
+  /* The callback runs before each batch (isweep % grid_output_int == 0) and
+   * the driver breaks at a check before the callback, so the sweeps made are
+   * the last callback's isweep plus one batch, capped at nsweeps. */
+  long long done = n_marks ? (long long)mark_sweep[n_marks - 1] + spc : 0;
+  if (done > nsweeps) done = nsweeps;
+  const double attempts = (double)L * L * (double)ngrids * (double)done;
+  fprintf(stderr, "%.0f %.6f\n", attempts, t1 - t0);
+  fprintf(stderr, "T %.6f", t0);
+  for (int i = 0; i < n_marks; ++i) fprintf(stderr, " %d %.6f", mark_sweep[i], mark_time[i]);
+  fprintf(stderr, " %lld %.6f\n", done, t1);
   free(grids);
   free(result);
   return 0;

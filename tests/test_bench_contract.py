@@ -17,14 +17,18 @@ REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 def test_reference_arm_prints_contract_line():
     if ref_lib_path("ref_cpu_bench") is None:
         pytest.skip("oracle/_ref/ref_cpu_bench not built")
-    r = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--steps", "1",
-                        "--warmup", "1"], cwd=REPO, capture_output=True, text=True, timeout=600)
+    r = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--steps", "2",
+                        "--warmup", "1", "--cpu-replicas", "48", "--cpu-sweeps", "300",
+                        "--no-reference-gpu"],
+                       cwd=REPO, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
     line = json.loads(r.stdout.strip().splitlines()[-1])
     assert line["impl"] == "reference"
     assert line["metric"] == "spin-flip attempts/s" and line["unit"] == "attempts/s"
     assert line["value"] > 0 and line["higher_is_better"] is True
-    assert line["warmup"] >= 3 and line["steps"] == 1
+    assert line["warmup"] >= 3 and line["steps"] == 2 and len(line["step_ms"]) == 2
+    assert line["n_gpus"] == 1
+    assert line["config"]["replicas"] == 48 and line["config"]["sweeps"] == 300
     cpu = line["cpu_baseline"]
     assert cpu["kind"] == "reference" and cpu["cores"] >= 1 and cpu["value"] == line["value"]
     assert "mc_driver_cpu" in cpu["sample"]
@@ -39,3 +43,33 @@ def test_bench_lists_its_workloads():
     assert r.returncode == 0
     for w in ("swarm", "batched", "committor", "surrogate", "cnn", "rate", "cluster", "tail"):
         assert w in r.stdout
+
+
+def test_cpu_harness_counts_attempts_and_marks_steps():
+    """The timing harness reports the attempts the unmodified driver made and
+    a timestamp at every output callback, from which bench.py cuts steps."""
+    if ref_lib_path("ref_cpu_bench") is None:
+        pytest.skip("oracle/_ref/ref_cpu_bench not built")
+    sys.path.insert(0, REPO)
+    import bench
+    run = bench.cpu_reference_run(3, 200, cores=[0])
+    assert run["cores"] == 1 and run["attempts"] == 64 * 64 * 3 * 200
+    (t0, marks), = run["marks"]
+    assert sorted(marks) == list(range(0, 201, bench.CPU_MARK_INT))
+    steps = bench.cpu_steps(run, 4)
+    assert len(steps) == 4 and all(t >= 0 for t in steps)
+    assert abs(sum(steps) - (marks[200] - t0)) < 1e-6
+
+
+def test_gpus_flag_starts_the_ranks_itself():
+    """bench.py --gpus 2 without a launcher starts two ranks (gloo in the dry
+    run) and rank 0 alone prints one line with n_gpus 2."""
+    r = subprocess.run([sys.executable, "bench.py", "--gpus", "2", "--dry-run", "--steps", "3",
+                        "--warmup", "3"], cwd=REPO, capture_output=True, text=True, timeout=600,
+                       env={**os.environ, "OMP_NUM_THREADS": "1"})
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    line = json.loads(lines[0])
+    assert line["n_gpus"] == 2 and line["world_size"] == 2 and line["backend"] == "gloo"
+    assert line["steps"] == 3 and line["value"] > 0

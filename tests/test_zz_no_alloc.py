@@ -73,3 +73,31 @@ def test_noalloc_rejects_inputs_above_the_stage():
     g2 = engine.DeviceGrids(L, 10)
     with pytest.raises(GaspError):
         check(_upload(lib().gasp_grids_upload_inputs_noalloc, g2, _inputs(rs, 3, L)))
+
+
+def _free_device_bytes():
+    """Free device memory as the driver reports it (cuMemGetInfo on the
+    context this thread already uses)."""
+    import ctypes as C
+    cu = C.CDLL("libcuda.so.1")
+    free, total = C.c_size_t(), C.c_size_t()
+    assert cu.cuMemGetInfo_v2(C.byref(free), C.byref(total)) == 0
+    return free.value
+
+
+def test_noalloc_takes_no_device_memory():
+    """The property the entry point exists for: repeated calls leave the
+    device's free memory unchanged, on a set that has no int32 buffer of its
+    own (the allocating form would stage there or in a new buffer).  The
+    set's download then allocates its 64 MiB int32 buffer, which the same
+    measurement sees, so the check is able to see an allocation."""
+    L, nin, per = 64, 64, 64  # 4096 replicas; their int32 image is 64 MiB
+    rs = np.random.default_rng(5)
+    g = engine.DeviceGrids(L, nin * per)
+    check(_upload(lib().gasp_grids_upload_inputs_noalloc, g, _inputs(rs, nin, L)))  # warm
+    before = _free_device_bytes()
+    for _ in range(3):
+        check(_upload(lib().gasp_grids_upload_inputs_noalloc, g, _inputs(rs, nin, L)))
+    assert _free_device_bytes() == before
+    g.download()  # allocates the set's int32 image
+    assert _free_device_bytes() <= before - nin * per * L * L * 4
