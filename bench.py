@@ -157,19 +157,24 @@ def cpu_reference_run(replicas, sweeps, cores=None, seed=SEED):
              str(BETA), str(H), str(seed + i), str(CPU_MARK_INT)],
             stdout=subprocess.DEVNULL, stderr=subprocess.PIPE, text=True,
             preexec_fn=(lambda c=core: os.sched_setaffinity(0, {c}))))
-    attempts, marks = 0.0, []
+    attempts, marks, cpu, walls = 0.0, [], [], []
     for p in procs:
         _, err = p.communicate()
         if p.returncode != 0:
             raise RuntimeError(f"ref_cpu_bench failed ({p.returncode}): {err[-300:]}")
         lines = err.strip().splitlines()
-        a, _w = lines[-2].split()
+        a, w = lines[-3].split()
         attempts += float(a)
-        f = lines[-1].split()[1:]
+        walls.append(float(w))
+        f = lines[-2].split()[1:]
         marks.append((float(f[0]), {int(f[i]): float(f[i + 1]) for i in range(1, len(f), 2)}))
+        cpu.append(float(lines[-1].split()[1]))
     wall = time.perf_counter() - t0
     return {"attempts": attempts, "wall_s": wall, "cores": nproc, "marks": marks,
-            "replicas": replicas, "sweeps": sweeps}
+            "replicas": replicas, "sweeps": sweeps,
+            # CPU time / wall time of the processes: below 1 when a core was shared
+            "cpu_share": sum(cpu) / max(sum(walls), 1e-9),
+            "loadavg_after": os.getloadavg()[0]}
 
 
 def cpu_steps(run, steps):
@@ -201,7 +206,7 @@ def cpu_config_baseline():
     if run is None:
         return None
     return {"value": run["attempts"] / run["wall_s"], "unit": UNIT, "cores": run["cores"],
-            "kind": "reference", "wall_s": run["wall_s"],
+            "kind": "reference", "wall_s": run["wall_s"], "cpu_share": run["cpu_share"],
             "sample": (f"the CPU configuration: L=64, {run['replicas']} replicas, "
                        f"{run['sweeps']} sweeps, checks every {CPU_CONFIG['mag_output_int']}, "
                        f"beta={BETA}, h={H}, all-down; {run['cores']} processes (one per core, "
@@ -244,7 +249,7 @@ def run_reference(args, rank, world):
                          "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "step_ms": [round(1e3 * t, 3) for t in step_s],
-        "wall_s": run["wall_s"],
+        "wall_s": run["wall_s"], "cpu_share": run["cpu_share"],
     }
     if not args.no_reference_gpu and _gpu_visible():
         line["reference_gpu_kernels"] = reference_gpu_kernels()
@@ -407,6 +412,11 @@ def run_secondary_child(args):
 
 
 def run_ours(args, rank, world, local_rank):
+    # The CPU baseline runs first, before this process starts CUDA and torch's
+    # thread pools, so that nothing of ours shares the host cores with it.
+    cpu_first = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu_first = cpu_config_baseline()
     import torch
     from gpu_2dising_b200 import engine
 
@@ -490,8 +500,7 @@ def run_ours(args, rank, world, local_rank):
         dist.destroy_process_group()
     if rank == 0:
         # after the timed region and after the other ranks are done
-        if world == 1 and not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_config_baseline()
+        line["cpu_baseline"] = cpu_first
         if world == 1 and not args.no_secondary:
             line["secondary"] = run_secondary_child(args)
         print(json.dumps(line), flush=True)

@@ -11,8 +11,8 @@
 // shared memory in the no-swizzle interleaved layout (8-row x 16-byte core
 // matrices); one thread issues K/16 tcgen05.mma (kind::f16, M=128, N=32), a
 // tcgen05.commit arrives on an mbarrier, and every warp reads its 32 rows of D
-// with tcgen05.ld.  Weight gradients are FP32 reductions over pixels on the
-// CUDA cores.
+// with tcgen05.ld.  Weight gradients are tcgen05 GEMMs too, reducing over the
+// batch's pixels with both operands MN-major (k_conv_dw_win, k_conv_dw1_tc).
 //
 // Activations: BF16, [image][pixel][32 channels] (pixel = row*L + col).
 #include <cuda_bf16.h>
@@ -503,66 +503,8 @@ size_t conv_smem(int mode) {
   return (size_t)kTileM * K * 2 + (size_t)kC * K * 2 + 64 + (size_t)kTileM * 33 * 4;
 }
 
-// FP32 weight gradient of one layer: dW[co][k] += sum_p dZ[p][co] * X[p, k]
-// with X[p, tap*Cin + ci] = input[nbr(p, tap)][ci]; db[co] += sum_p dZ[p][co].
-// Thread t accumulates co = t/8 and k = (t%8) + 8j.  CTAs stride over 32-pixel
-// chunks of the whole batch, then add their partial sums atomically.
-template <int CIN>
-__global__ void __launch_bounds__(256) k_conv_dw(int L, int B, const __nv_bfloat16 *dz,
-                                                 const __nv_bfloat16 *xin, const int8_t *spins,
-                                                 float *dW, float *db) {
-  constexpr int K = 9 * CIN;
-  constexpr int KPT = (K + 7) / 8;  // k values per thread
-  constexpr int P = 32;             // pixels per chunk (static shared memory < 48 KB)
-  __shared__ float s_dz[P][kC + 1];
-  __shared__ float s_x[P][K + 1];
-  const int N = L * L;
-  const int tid = threadIdx.x;
-  const int co = tid >> 3, k0 = tid & 7;
-  float acc[KPT];
-#pragma unroll
-  for (int j = 0; j < KPT; ++j) acc[j] = 0.f;
-  float accb = 0.f;
-  const long long nchunks = (long long)B * N / P;
-  for (long long ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
-    const long long pix0 = ch * P;
-    const int img = (int)(pix0 / N);
-    const int p0 = (int)(pix0 % N);
-    for (int i = tid; i < P * kC; i += blockDim.x) {
-      const int r = i / kC, c = i % kC;
-      s_dz[r][c] = __bfloat162float(dz[((size_t)img * N + p0 + r) * kC + c]);
-    }
-    for (int i = tid; i < P * K; i += blockDim.x) {
-      const int r = i / K, k = i % K;
-      const int tap = k / CIN, ci = k % CIN;
-      const int q = nbr(p0 + r, tap, L);
-      float v;
-      if constexpr (CIN == 1) v = (float)spins[(size_t)img * N + q];
-      else v = __bfloat162float(xin[((size_t)img * N + q) * kC + ci]);
-      s_x[r][k] = v;
-    }
-    __syncthreads();
-#pragma unroll 4
-    for (int r = 0; r < P; ++r) {
-      const float g = s_dz[r][co];
-#pragma unroll
-      for (int j = 0; j < KPT; ++j) {
-        const int k = k0 + 8 * j;
-        if (k < K) acc[j] += g * s_x[r][k];
-      }
-      if (k0 == 0) accb += g;
-    }
-    __syncthreads();
-  }
-#pragma unroll
-  for (int j = 0; j < KPT; ++j) {
-    const int k = k0 + 8 * j;
-    if (k < K) atomicAdd(&dW[co * K + k], acc[j]);
-  }
-  if (k0 == 0) atomicAdd(&db[co], accb);
-}
-
-// FP32 weight gradient of a 32->32 layer, register-tiled: dW[co][k] +=
+// FP32 weight gradient of a 32->32 layer for L other than 32, 64, 128 (the
+// tcgen05 kernel k_conv_dw_win takes those), register-tiled: dW[co][k] +=
 // sum_p dZ[p][co] * X[p, k] (k = tap*32 + ci, X the layer input at the tap's
 // neighbour).  A block takes chunks of 32 pixels; thread t accumulates the 4
 // output channels 4*(t/32).. and the 9 k values (t%32) + 32*j, so each pixel
@@ -641,6 +583,292 @@ __global__ void __launch_bounds__(256) k_conv_dw32(int L, int B, const __nv_bflo
   }
 }
 
+// ---------------------------------------------------------------------------
+// Weight gradients on tcgen05.  dW[co][k] = sum_p dZ[p][co] * X[p][k] is a GEMM
+// whose reduction runs over every pixel of the batch: D[m][n] = sum_k A[m][k]
+// B[n][k] with k = pixel, n = co (N = 32) and m = the layer-input value a tap
+// reads.  Both operands are MN-major in shared memory (no swizzle): a core
+// matrix is 8 pixels (K) x 8 values (MN) = 8 rows of 16 bytes, 8-pixel groups
+// 128 B apart (LBO), 8-value groups SBO apart.  dZ is staged [co chunk][pixel]
+// [16 B] (SBO 2 KB).  FP32 accumulation in TMEM over all of a CTA's tiles;
+// each CTA adds its partial sums to dW and db (one atomicAdd per value).
+// ---------------------------------------------------------------------------
+// Instruction descriptor: D F32, A/B BF16, both MN-major, N=32, M=128.
+constexpr uint32_t kIdescMN = kIdesc | (1u << 15) | (1u << 16);
+
+__device__ __forceinline__ void umma_bf16_mn(uint32_t tmem_d, uint64_t da, uint64_t db,
+                                             uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+      "l"(da), "l"(db), "r"(kIdescMN), "r"(accumulate));
+}
+
+struct DwArgs {
+  int L;
+  const __nv_bfloat16 *x;   // layer input activations [B][N][32] (32->32 layers)
+  const int8_t *spins;      // layer 1: the input grids [B][N]
+  const __nv_bfloat16 *dz;  // this layer's output gradient (after the ReLU mask) [B][N][32]
+  float *dW, *db;           // gradients, added to
+  int *err;                 // set on a timed-out wait
+  int ntiles;               // images * (L*L / 128)
+};
+
+// 32->32 layers, L = LT in {32, 64, 128}.  The A operand is the input window
+// of k_conv_win: the tile's rows and one row above and below (W = 128 + 2L
+// pixels), staged as copies rotated by dx = -1, 0, +1 within each image row,
+// [copy][channel chunk][pixel][16 B]; read with pixels along K and channels
+// along M, copy v's four channel chunks are M rows 32v..32v+31 (SBO = W*16,
+// the chunk stride; copies follow one another at 4*W*16).  A fourth copy holds
+// ones, so M rows 96..127 accumulate sum_p dZ[p][co] = db.  A tap's row offset
+// dy is a start offset of (dy+1)*L pixels along K, and each dy has its own
+// accumulator (TMEM columns 32*(dy+1)): per 128-pixel tile 3 x 8 MMAs of
+// M=128, N=32, K=16 (the ones rows repeated for dy = 0, +1 are not used).
+// The next tile's window and dZ rows are loaded into registers while the
+// current tile's MMAs run.
+template <int LT>
+__global__ void __launch_bounds__(128) k_conv_dw_win(DwArgs a) {
+  static_assert(LT == 32 || LT == 64 || LT == 128, "whole image rows per tile");
+  constexpr int L = LT, N = L * L;
+  constexpr int W = kTileM + 2 * L;             // window pixels
+  constexpr uint32_t lbo = (uint32_t)W * 16;    // bytes between channel chunks
+  constexpr uint32_t vstride = 4u * lbo;        // bytes between rotated copies
+  constexpr int tiles_per_img = N / kTileM;
+  extern __shared__ __align__(1024) unsigned char smem[];
+  unsigned char *sA = smem;                      // [4][4][W][16 B]; copy 3 = ones
+  unsigned char *sB = smem + 4 * vstride;        // dZ: [4][128][16 B]
+  uint64_t *mbar = reinterpret_cast<uint64_t *>(sB + 4 * kTileM * 16);
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(mbar + 1);
+  const int tid = threadIdx.x, warp = tid >> 5;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(tslot)),
+                 "r"(128)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    mbar_init(smem_u32(mbar), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  {
+    const uint4 ones = make_uint4(0x3F803F80u, 0x3F803F80u, 0x3F803F80u, 0x3F803F80u);
+    for (int i = tid; i < 4 * W; i += blockDim.x)
+      *reinterpret_cast<uint4 *>(sA + 3 * vstride + (uint32_t)i * 16) = ones;
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t taddr = *tslot;
+
+  constexpr int kPerW = W * 4 / 128;  // 16-byte window chunks per thread
+  uint4 v4[kPerW];
+  uint4 g4[4];
+  auto load_tile = [&](int t) {
+    const int timg = t / tiles_per_img;
+    const int y0 = ((t % tiles_per_img) * kTileM) / L;  // first output row of the tile
+    const __nv_bfloat16 *xs = a.x + (size_t)timg * N * kC;
+#pragma unroll
+    for (int j = 0; j < kPerW; ++j) {
+      const int c = (tid & 31) >> 3, w = j * 32 + (tid >> 5) * 8 + (tid & 7);
+      int row = y0 - 1 + w / L;
+      row = row < 0 ? row + L : (row >= L ? row - L : row);
+      v4[j] = *reinterpret_cast<const uint4 *>(xs + ((size_t)row * L + (w % L)) * kC + 8 * c);
+    }
+    const uint4 *gz = reinterpret_cast<const uint4 *>(
+        a.dz + ((size_t)timg * N + (size_t)(t % tiles_per_img) * kTileM + tid) * kC);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) g4[c] = gz[c];
+  };
+  if ((int)blockIdx.x < a.ntiles) load_tile(blockIdx.x);
+
+  uint32_t phase = 0;
+  bool first = true, ok = true;
+  for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
+    if (!first) {  // the previous tile's MMAs still read the shared operands
+      bool waited = true;
+      if (tid == 0) waited = mbar_wait(smem_u32(mbar), phase);
+      ok = __syncthreads_and(waited ? 1 : 0) != 0;
+      phase ^= 1u;
+      if (!ok) break;
+    }
+#pragma unroll
+    for (int j = 0; j < kPerW; ++j) {
+      const int c = (tid & 31) >> 3, w = j * 32 + (tid >> 5) * 8 + (tid & 7);
+      const int col = w % L, rbase = w - col;
+#pragma unroll
+      for (int v = 0; v < 3; ++v) {  // copy v holds, at column col', input column col' + v - 1
+        const int cd = (col - (v - 1) + L) % L;
+        *reinterpret_cast<uint4 *>(sA + v * vstride + c * lbo + (uint32_t)(rbase + cd) * 16) =
+            v4[j];
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+      *reinterpret_cast<uint4 *>(sB + c * (kTileM * 16) + tid * 16) = g4[c];
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (tid == 0) {
+      const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
+#pragma unroll
+      for (int dy = 0; dy < 3; ++dy) {
+#pragma unroll
+        for (int s = 0; s < kTileM / 16; ++s)
+          umma_bf16_mn(taddr + (uint32_t)(dy * 32),
+                       umma_desc(a0 + (uint32_t)(dy * L + 16 * s) * 16, 128, lbo),
+                       umma_desc(b0 + (uint32_t)s * 256, 128, kTileM * 16),
+                       (first && s == 0) ? 0u : 1u);
+      }
+      umma_commit(smem_u32(mbar));
+    }
+    first = false;
+    const int nt = tile + (int)gridDim.x;
+    if (nt < a.ntiles) load_tile(nt);
+  }
+  if (!first && ok) {  // the last tile's MMAs, then this CTA's sums
+    bool waited = true;
+    if (tid == 0) waited = mbar_wait(smem_u32(mbar), phase);
+    ok = __syncthreads_and(waited ? 1 : 0) != 0;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (ok) {
+      const int lane = tid & 31;
+#pragma unroll 1
+      for (int dy = 0; dy < 3; ++dy) {
+        float acc[32];
+        tmem_ld32(taddr + ((uint32_t)(warp * 32) << 16) + (uint32_t)(dy * 32), acc);
+        if (warp < 3) {  // copy v = warp: tap (dy, dx = v - 1), ci = lane
+          const int k = (dy * 3 + warp) * kC + lane;
+#pragma unroll
+          for (int co = 0; co < kC; ++co) atomicAdd(&a.dW[co * 9 * kC + k], acc[co]);
+        } else if (dy == 0 && lane == 0) {  // a row of ones: sum_p dZ[p][co]
+#pragma unroll
+          for (int co = 0; co < kC; ++co) atomicAdd(&a.db[co], acc[co]);
+        }
+      }
+    }
+  }
+  if (!ok && tid == 0 && a.err) atomicExch(a.err, 1);
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(128)
+                 : "memory");
+  }
+}
+
+constexpr size_t dw_win_smem(int L) {
+  return 4 * 4 * ((size_t)kTileM + 2 * (size_t)L) * 16 + 4 * (size_t)kTileM * 16 + 64;
+}
+
+// Layer 1 (one input channel, 9 taps): A rows are the taps, staged per pixel
+// as two 16-byte MN groups (taps 0-7; tap 8 and seven zeros), then a group of
+// ones (rows 16..23: db) and thirteen zero groups to fill M = 128 (SBO 2 KB:
+// [group][pixel][16 B]).  One accumulator; 8 MMAs per 128-pixel tile.
+__global__ void __launch_bounds__(128) k_conv_dw1_tc(DwArgs a) {
+  constexpr int kGroups = 16;
+  constexpr uint32_t sbo = kTileM * 16;  // 2 KB
+  extern __shared__ __align__(1024) unsigned char smem[];
+  unsigned char *sA = smem;                           // [16][128][16 B]
+  unsigned char *sB = smem + kGroups * sbo;           // dZ: [4][128][16 B]
+  uint64_t *mbar = reinterpret_cast<uint64_t *>(sB + 4 * sbo);
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(mbar + 1);
+  const int L = a.L, N = L * L;
+  const int tiles_per_img = N / kTileM;
+  const int tid = threadIdx.x, warp = tid >> 5;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(tslot)),
+                 "r"(32)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    mbar_init(smem_u32(mbar), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  {
+    const uint4 ones = make_uint4(0x3F803F80u, 0x3F803F80u, 0x3F803F80u, 0x3F803F80u);
+    const uint4 zero = make_uint4(0u, 0u, 0u, 0u);
+    for (int i = tid; i < (kGroups - 2) * kTileM; i += blockDim.x)
+      *reinterpret_cast<uint4 *>(sA + 2 * sbo + (uint32_t)i * 16) = i < kTileM ? ones : zero;
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t taddr = *tslot;
+
+  uint32_t phase = 0;
+  bool first = true, ok = true;
+  for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
+    const int img = tile / tiles_per_img;
+    const int p = (tile % tiles_per_img) * kTileM + tid;
+    const int8_t *sp = a.spins + (size_t)img * N;
+    __align__(16) __nv_bfloat16 v[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) v[k] = __float2bfloat16_rn(k < 9 ? (float)sp[nbr(p, k, L)] : 0.0f);
+    const uint4 *gz = reinterpret_cast<const uint4 *>(a.dz + ((size_t)img * N + p) * kC);
+    uint4 g4[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) g4[c] = gz[c];
+    if (!first) {
+      bool waited = true;
+      if (tid == 0) waited = mbar_wait(smem_u32(mbar), phase);
+      ok = __syncthreads_and(waited ? 1 : 0) != 0;
+      phase ^= 1u;
+      if (!ok) break;
+    }
+    *reinterpret_cast<uint4 *>(sA + tid * 16) = *reinterpret_cast<const uint4 *>(&v[0]);
+    *reinterpret_cast<uint4 *>(sA + sbo + tid * 16) = *reinterpret_cast<const uint4 *>(&v[8]);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) *reinterpret_cast<uint4 *>(sB + c * sbo + tid * 16) = g4[c];
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (tid == 0) {
+      const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
+#pragma unroll
+      for (int s = 0; s < kTileM / 16; ++s)
+        umma_bf16_mn(taddr, umma_desc(a0 + (uint32_t)s * 256, 128, sbo),
+                     umma_desc(b0 + (uint32_t)s * 256, 128, sbo), (first && s == 0) ? 0u : 1u);
+      umma_commit(smem_u32(mbar));
+    }
+    first = false;
+  }
+  if (!first && ok) {
+    bool waited = true;
+    if (tid == 0) waited = mbar_wait(smem_u32(mbar), phase);
+    ok = __syncthreads_and(waited ? 1 : 0) != 0;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (ok && warp == 0) {  // rows 0..8: taps; row 16: ones
+      const int lane = tid & 31;
+      float acc[32];
+      tmem_ld32(taddr, acc);
+      if (lane < 9) {
+#pragma unroll
+        for (int co = 0; co < kC; ++co) atomicAdd(&a.dW[co * 9 + lane], acc[co]);
+      } else if (lane == 16) {
+#pragma unroll
+        for (int co = 0; co < kC; ++co) atomicAdd(&a.db[co], acc[co]);
+      }
+    }
+  }
+  if (!ok && tid == 0 && a.err) atomicExch(a.err, 1);
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(32)
+                 : "memory");
+  }
+}
+
+constexpr size_t kDw1Smem = 16 * (size_t)kTileM * 16 + 4 * (size_t)kTileM * 16 + 64;
+
 // Head: mean pool -> linear -> sigmoid -> cross-entropy; one warp per image,
 // lane = channel.  Writes q, adds the mean loss, the head's gradients and
 // dmean[b][c] = dL/d(pooled mean).
@@ -690,14 +918,21 @@ __global__ void k_head(int B, int N, const float *pool, const float *params, con
 }
 
 // dZ4 = dmean / N on every pixel where the layer-4 activation is positive.
+// One thread per 8 channels of a pixel (16-byte loads and stores).
 __global__ void k_dz4(int B, int N, const float *dmean, const __nv_bfloat16 *a4,
                       __nv_bfloat16 *dz4) {
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= (long long)B * N * kC) return;
-  const int c = (int)(i % kC);
-  const long long b = i / ((long long)N * kC);
-  const float g = __bfloat162float(a4[i]) > 0.0f ? dmean[b * kC + c] / (float)N : 0.0f;
-  dz4[i] = __float2bfloat16_rn(g);
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;  // 8-channel chunk
+  if (i >= (long long)B * N * (kC / 8)) return;
+  const int c0 = (int)(i % (kC / 8)) * 8;
+  const long long b = i / ((long long)N * (kC / 8));
+  const uint4 av = reinterpret_cast<const uint4 *>(a4)[i];
+  const __nv_bfloat16 *ah = reinterpret_cast<const __nv_bfloat16 *>(&av);
+  const float *dm = dmean + b * kC + c0;
+  __align__(16) __nv_bfloat16 o[8];
+#pragma unroll
+  for (int e = 0; e < 8; ++e)
+    o[e] = __float2bfloat16_rn(__bfloat162float(ah[e]) > 0.0f ? dm[e] / (float)N : 0.0f);
+  reinterpret_cast<uint4 *>(dz4)[i] = *reinterpret_cast<const uint4 *>(o);
 }
 
 // BF16 copies of the weights: W1 [32][16] (taps padded), W2..4 [32][288]
@@ -781,6 +1016,28 @@ int launch_persistent(Kern kern, size_t smem_max, size_t smem, const ConvArgs &b
   const int by_regs = fa.numRegs > 0 ? 65536 / (fa.numRegs * 128) : 16;
   if (per_sm > by_regs) per_sm = by_regs;
   if (per_sm > 16) per_sm = 16;  // 2048 threads per SM; also all TMEM (16 x 32 columns)
+  if (per_sm < 1) per_sm = 1;
+  const int grid = b.ntiles < nsm * per_sm ? b.ntiles : nsm * per_sm;
+  kern<<<grid, 128, smem, s>>>(b);
+  GASP_CUDA(cudaGetLastError());
+  return GASP_OK;
+}
+
+// Persistent launch of a weight-gradient kernel: all CTAs resident, at most
+// 512 / tmem_cols per SM (TMEM), bounded by shared memory and registers.
+template <typename Kern>
+int launch_dw(Kern kern, size_t smem, int tmem_cols, const DwArgs &b, cudaStream_t s) {
+  GASP_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int dev = 0, nsm = 0, smem_sm = 0;
+  GASP_CUDA(cudaGetDevice(&dev));
+  GASP_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  GASP_CUDA(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+  int per_sm = smem_sm / (int)(smem + 1024);
+  cudaFuncAttributes fa;
+  GASP_CUDA(cudaFuncGetAttributes(&fa, kern));
+  const int by_regs = fa.numRegs > 0 ? 65536 / (fa.numRegs * 128) : 16;
+  if (per_sm > by_regs) per_sm = by_regs;
+  if (per_sm > 512 / tmem_cols) per_sm = 512 / tmem_cols;
   if (per_sm < 1) per_sm = 1;
   const int grid = b.ntiles < nsm * per_sm ? b.ntiles : nsm * per_sm;
   kern<<<grid, 128, smem, s>>>(b);
@@ -927,7 +1184,7 @@ int cnn_backward(gasp_cnn *c, int batch, cudaStream_t s) {
   k_head<<<(B + 7) / 8, 256, 0, s>>>(B, N, c->d_pool, c->d_params, c->d_labels, c->d_q, c->d_loss,
                                      c->d_grad, c->d_dmean);
   GASP_CUDA(cudaGetLastError());
-  const long long tot = (long long)B * N * kC;
+  const long long tot = (long long)B * N * (kC / 8);
   k_dz4<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(B, N, c->d_dmean, c->d_act[3], c->d_dz[0]);
   GASP_CUDA(cudaGetLastError());
   int cur = 0;
@@ -935,10 +1192,28 @@ int cnn_backward(gasp_cnn *c, int batch, cudaStream_t s) {
   GASP_CUDA(cudaGetDevice(&dev));
   GASP_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
   const int dw_grid = nsm * 3;  // k_conv_dw32: 3 resident blocks per SM (registers)
+  DwArgs d;
+  memset(&d, 0, sizeof d);
+  d.L = c->L;
+  d.err = c->d_err;
+  d.ntiles = B * (N / kTileM);
   for (int l = 3; l >= 1; --l) {  // layers 4, 3, 2 (0-based l)
     float *gW = c->d_grad + kOffW2 + (l - 1) * (9216 + 32);
-    k_conv_dw32<<<dw_grid, 256, 0, s>>>(c->L, B, c->d_dz[cur], c->d_act[l - 1], gW, gW + 9216);
-    GASP_CUDA(cudaGetLastError());
+    d.x = c->d_act[l - 1];
+    d.dz = c->d_dz[cur];
+    d.dW = gW;
+    d.db = gW + 9216;
+    switch (c->L) {
+      case 32: rc = launch_dw(k_conv_dw_win<32>, dw_win_smem(32), 128, d, s); break;
+      case 64: rc = launch_dw(k_conv_dw_win<64>, dw_win_smem(64), 128, d, s); break;
+      case 128: rc = launch_dw(k_conv_dw_win<128>, dw_win_smem(128), 128, d, s); break;
+      default:
+        k_conv_dw32<<<dw_grid, 256, 0, s>>>(c->L, B, c->d_dz[cur], c->d_act[l - 1], gW,
+                                            gW + 9216);
+        GASP_CUDA(cudaGetLastError());
+        rc = GASP_OK;
+    }
+    if (rc) return rc;
     ConvArgs a;
     memset(&a, 0, sizeof a);
     a.L = c->L;
@@ -950,10 +1225,12 @@ int cnn_backward(gasp_cnn *c, int batch, cudaStream_t s) {
     if ((rc = launch_conv<kBwd>(a, B, s))) return rc;
     cur ^= 1;
   }
-  k_conv_dw<1><<<dw_grid, 256, 0, s>>>(c->L, B, c->d_dz[cur], nullptr, c->d_spins,
-                                       c->d_grad + kOffW1, c->d_grad + kOffB1);
-  GASP_CUDA(cudaGetLastError());
-  return GASP_OK;
+  d.x = nullptr;
+  d.spins = c->d_spins;
+  d.dz = c->d_dz[cur];
+  d.dW = c->d_grad + kOffW1;
+  d.db = c->d_grad + kOffB1;
+  return launch_dw(k_conv_dw1_tc, kDw1Smem, 32, d, s);
 }
 
 }  // namespace

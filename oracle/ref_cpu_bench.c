@@ -13,6 +13,8 @@
  *                                each output callback (every grid_output_int
  *                                sweeps, before that batch is swept), so a
  *                                caller can cut one run into steps
+ *   "C <cpu_seconds>"            CPU time the process used in the driver (below
+ *                                the wall time when the core was shared)
  */
 #include <stdio.h>
 #include <stdlib.h>
@@ -26,6 +28,12 @@
 static int n_marks = 0;
 static int mark_sweep[MAX_MARKS];
 static double mark_time[MAX_MARKS];
+
+static double cpu_s(void) {
+  struct timespec t;
+  clock_gettime(CLOCK_PROCESS_CPUTIME_ID, &t);
+  return (double)t.tv_sec + 1e-9 * (double)t.tv_nsec;
+}
 
 static double now_s(void) {
   struct timespec t;
@@ -72,9 +80,11 @@ int main(int argc, char **argv) {
   c.cv = (char *)"magnetisation"; c.result = result; c.filename = (char *)"/dev/null";
 
   if (!freopen("/dev/null", "w", stdout)) return 3;
+  const double c0 = cpu_s();
   const double t0 = now_s();
   mc_driver_cpu(g, beta, h, NULL, s, c, mark_outfunc);
   const double t1 = now_s();
+  const double c1 = cpu_s();
   /* The callback runs before each batch (isweep % grid_output_int == 0) and
    * the driver breaks at a check before the callback, so the sweeps made are
    * the last callback's isweep plus one batch, capped at nsweeps. */
@@ -85,6 +95,7 @@ int main(int argc, char **argv) {
   fprintf(stderr, "T %.6f", t0);
   for (int i = 0; i < n_marks; ++i) fprintf(stderr, " %d %.6f", mark_sweep[i], mark_time[i]);
   fprintf(stderr, " %lld %.6f\n", done, t1);
+  fprintf(stderr, "C %.6f\n", c1 - c0);
   free(grids);
   free(result);
   return 0;
