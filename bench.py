@@ -531,9 +531,12 @@ def batched_measure(args):
     nat.check(nat.lib().gasp_batch_create(arr, len(groups), SEED, kind, C.byref(h)))
     choice = np.zeros(2 * len(groups), np.int32)
     nat.check(nat.lib().gasp_batch_autotune(h, 2, choice))
+    t_sep, t_one = C.c_float(), C.c_float()
+    layout = nat.lib().gasp_batch_layout(h, C.byref(t_sep), C.byref(t_one))
     tot, chk, up = args.batched_sweeps, 50, 0.9
     res = {}
-    for name, mode in (("plain", nat.BATCH_PLAIN), ("graph", nat.BATCH_GRAPH)):
+    for name, mode in (("plain", nat.BATCH_PLAIN), ("graph", nat.BATCH_GRAPH),
+                       ("one_launch", nat.BATCH_MULTI)):
         counts = np.zeros((tot // chk) * len(groups), np.int32)
         att, el = C.c_longlong(), C.c_double()
         nat.check(nat.lib().gasp_batch_swarm(h, tot, chk, up, mode, counts, C.byref(att),
@@ -545,7 +548,11 @@ def batched_measure(args):
         "metric": "spin-flip attempts/s, uneven batched launch vs plain per-group launches",
         "value": res["graph"]["value"], "unit": UNIT, "n_gpus": 1,
         "speedup_vs_plain": res["graph"]["value"] / res["plain"]["value"],
-        "plain": res["plain"], "graph": res["graph"],
+        "one_launch_speedup_vs_plain": res["one_launch"]["value"] / res["plain"]["value"],
+        "plain": res["plain"], "graph": res["graph"], "one_launch": res["one_launch"],
+        "layout": {"chosen": ["one kernel per group", "one persistent launch"][layout],
+                   "autotune_ms_3_intervals": {"per_group_kernels": t_sep.value,
+                                               "one_launch": t_one.value}},
         "config": {"workload": "5 groups L=32/48/64/96/128, replicas 16384/8192/4096/2048/512, "
                                "all-down, nucleated replicas (m > 0.9 at a check) finished",
                    "groups": [{"L": L, "replicas": n, "beta": b, "h": hh}
@@ -855,7 +862,9 @@ def secondary_measure(args):
     bt = clocked(batched_measure, args)
     out["batched"] = {"metric": bt["metric"], "value": bt["value"], "unit": bt["unit"],
                       "speedup_vs_plain": bt["speedup_vs_plain"],
-                      "plain": bt["plain"], "graph": bt["graph"],
+                      "one_launch_speedup_vs_plain": bt["one_launch_speedup_vs_plain"],
+                      "layout": bt["layout"],
+                      "plain": bt["plain"], "graph": bt["graph"], "one_launch": bt["one_launch"],
                       "autotune": bt["config"]["autotune"], "workload": bt["config"]["workload"],
                       "clocks": bt["clocks"]}
     su = clocked(surrogate_measure, args)

@@ -31,6 +31,7 @@ OPT_TAIL_REPLICAS = 3
 
 BATCH_PLAIN = 0
 BATCH_GRAPH = 1
+BATCH_MULTI = 2
 
 RNG_XORWOW = 0
 RNG_MWC64X = 1
@@ -55,6 +56,7 @@ EXPORTED = (
     "gasp_read_frame", "gasp_write_input_grid", "gasp_checkpoint_save", "gasp_checkpoint_info",
     "gasp_checkpoint_load",
     "gasp_batch_create", "gasp_batch_free", "gasp_batch_swarm", "gasp_batch_autotune",
+    "gasp_batch_layout",
     "gasp_cnn_param_count", "gasp_cnn_create", "gasp_cnn_free", "gasp_cnn_set_params",
     "gasp_cnn_get_params", "gasp_cnn_predict", "gasp_cnn_predict_ex", "gasp_cnn_gradients",
     "gasp_cnn_train_step",
@@ -182,6 +184,7 @@ def _bind(lib):
         "gasp_batch_swarm": (I, [P, I, I, C.c_double, I, _i32p, C.POINTER(C.c_longlong),
                                  C.POINTER(C.c_double)]),
         "gasp_batch_autotune": (I, [P, I, _i32p]),
+        "gasp_batch_layout": (I, [P, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
         "gasp_cnn_param_count": (I, []),
         "gasp_cnn_create": (I, [I, I, C.POINTER(P)]),
         "gasp_cnn_free": (I, [P]),

@@ -383,7 +383,7 @@ int gasp_grids_set_option(gasp_grids_t *g, int option, int value) {
   GridsExtra &x = impl(g)->x;
   // Variants 3, 4 and 8 (pairwise speculation, acceptance mask, two tiles
   // per warp) were measured slower than variant 0 and have been retired.
-  if (option == GASP_OPT_SWEEP_VARIANT && value >= 0 && value <= 9 && value != 3 &&
+  if (option == GASP_OPT_SWEEP_VARIANT && value >= 0 && value <= 10 && value != 3 &&
       value != 4 && value != 8) {
     x.variant = value;
     return GASP_OK;
@@ -471,6 +471,28 @@ const TailParams &gasp::mwc_lane_params() {
   return t;
 }
 
+namespace gasp {
+// Seeds the states of r in place (the same streams gasp_init_rand_mode gives
+// for this seed) on the current stream, and waits for them.
+int rng_reseed(gasp_rng_t *r, unsigned long long seed) {
+  cudaStream_t s = current_stream();
+  int rc = GASP_OK;
+  if (r->kind == kRngMwc) {
+    std::vector<uint32_t> host;
+    mwc_seed_states(seed, r->ngrids, r->stride, host);
+    const cudaError_t e = cudaMemcpyAsync(r->d_state, host.data(), host.size() * sizeof(uint32_t),
+                                          cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return cuda_fail(e, "gasp_init_rand upload", __FILE__, __LINE__);
+  } else {
+    rc = launch_rng_init(r->d_state, r->ngrids, r->stride, seed, s);
+    if (rc) return rc;
+  }
+  const cudaError_t e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_fail(e, "gasp_init_rand", __FILE__, __LINE__);
+  return GASP_OK;
+}
+}  // namespace gasp
+
 extern "C" {
 
 int gasp_init_rand_mode(int ngrids, int threads_per_block, unsigned long long seed, int kind,
@@ -494,21 +516,7 @@ int gasp_init_rand_mode(int ngrids, int threads_per_block, unsigned long long se
     delete r;
     return cuda_fail(e, "gasp_init_rand allocation", __FILE__, __LINE__);
   }
-  cudaStream_t s = current_stream();
-  int rc = GASP_OK;
-  std::vector<uint32_t> host;
-  if (r->kind == kRngMwc) {
-    mwc_seed_states(seed, ngrids, r->stride, host);
-    e = cudaMemcpyAsync(r->d_state, host.data(), host.size() * sizeof(uint32_t),
-                        cudaMemcpyHostToDevice, s);
-    if (e != cudaSuccess) rc = cuda_fail(e, "gasp_init_rand upload", __FILE__, __LINE__);
-  } else {
-    rc = launch_rng_init(r->d_state, ngrids, r->stride, seed, s);
-  }
-  if (rc == GASP_OK) {
-    e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) rc = cuda_fail(e, "gasp_init_rand", __FILE__, __LINE__);
-  }
+  const int rc = rng_reseed(r, seed);
   if (rc) {
     cudaFree(r->d_state);
     delete r;

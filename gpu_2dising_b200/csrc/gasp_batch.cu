@@ -10,6 +10,7 @@
 // GASP_BATCH_PLAIN: one launch per group per interval over all of its
 // replicas, groups one after another, checks on the host (the comparison
 // path: what running each group with the single-group driver amounts to).
+#include <algorithm>
 #include <chrono>
 #include <cstdio>
 #include <cstring>
@@ -241,6 +242,14 @@ struct gasp_batch {
   cudaGraphExec_t exec = nullptr;
   int graph_check_int = -1;
   double graph_up = 0.0;
+  int graph_layout = -1;
+  // Sweep layout of the graph: 0 one kernel per group (concurrent branches),
+  // 1 all groups in one persistent launch (k_sweep_multi).  Set by the autotuner.
+  int layout = 0;
+  SweepLaunch *d_multi = nullptr;  // [ngroups] sweep parameters, largest L first
+  int *d_tile_begin = nullptr;     // [ngroups + 1]
+  int multi_tiles = 0, multi_max_L = 0;
+  float layout_ms[2] = {-1.f, -1.f};  // autotuner's timing of the two layouts
 };
 
 namespace {
@@ -258,6 +267,8 @@ int batch_release(gasp_batch *b) {
   for (auto *a : b->d_active) cudaFree(a);
   cudaFree(b->d_small);
   cudaFree(b->d_counts);
+  cudaFree(b->d_multi);
+  cudaFree(b->d_tile_begin);
   for (auto s : b->streams) cudaStreamDestroy(s);
   if (b->origin) cudaStreamDestroy(b->origin);
   for (auto e : b->events) cudaEventDestroy(e);
@@ -272,11 +283,11 @@ int batch_reset(gasp_batch *b, cudaStream_t s) {
     gasp_grids_t *gr = b->grids[g];
     const size_t words = (size_t)gr->ntiles * gr->W * kTile;
     GASP_CUDA(cudaMemsetAsync(gr->d_lat, 0, words * sizeof(uint32_t), s));
-    gasp_free_rand(b->rngs[g]);
-    b->rngs[g] = nullptr;
+    // re-seeded in place: a captured graph keeps pointing at these states
     gasp_set_stream(s);
-    const int rc = gasp_init_rand_mode(gr->ngrids, 32, b->seed + 1000003ull * (unsigned)g,
-                                       b->rng_kind, &b->rngs[g]);
+    const unsigned long long seed = b->seed + 1000003ull * (unsigned)g;
+    const int rc = b->rngs[g] ? rng_reseed(b->rngs[g], seed)
+                              : gasp_init_rand_mode(gr->ngrids, 32, seed, b->rng_kind, &b->rngs[g]);
     if (rc) return rc;
     k_iota<<<(gr->ngrids + 255) / 256, 256, 0, s>>>(b->d_active[g], gr->ngrids);
     GASP_CUDA(cudaGetLastError());
@@ -299,16 +310,68 @@ SweepLaunch group_launch(gasp_batch *b, int g, int nsweeps) {
   return p;
 }
 
+// Can every group run in one persistent launch?  (integer thresholds and
+// lattices in shared memory; the tables must be prepared)
+bool multi_possible(gasp_batch *b) {
+  for (int g = 0; g < b->ngroups; ++g) {
+    const SweepLaunch p = launch_for(b->grids[g], b->rngs[g]);
+    if (p.float_compare || p.lattice_in_global) return false;
+  }
+  return true;
+}
+
+// Uploads the groups' sweep parameters for k_sweep_multi, largest L first
+// (longest chains start first).  Synchronous; not while capturing.
+int batch_prepare_multi(gasp_batch *b, int check_int, cudaStream_t s) {
+  std::vector<int> order((size_t)b->ngroups);
+  for (int g = 0; g < b->ngroups; ++g) order[(size_t)g] = g;
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int x, int y) { return b->groups[x].L > b->groups[y].L; });
+  std::vector<SweepLaunch> ps;
+  std::vector<int> begin(1, 0);
+  int max_L = 0;
+  for (int g : order) {
+    ps.push_back(group_launch(b, g, check_int));
+    begin.push_back(begin.back() + tiles_for(b->groups[g].ngrids));
+    if (b->groups[g].L > max_L) max_L = b->groups[g].L;
+  }
+  if (!b->d_multi) {
+    GASP_CUDA(cudaMalloc(&b->d_multi, (size_t)b->ngroups * sizeof(SweepLaunch)));
+    GASP_CUDA(cudaMalloc(&b->d_tile_begin, (size_t)(b->ngroups + 1) * sizeof(int)));
+  }
+  GASP_CUDA(cudaMemcpyAsync(b->d_multi, ps.data(), ps.size() * sizeof(SweepLaunch),
+                            cudaMemcpyHostToDevice, s));
+  GASP_CUDA(cudaMemcpyAsync(b->d_tile_begin, begin.data(), begin.size() * sizeof(int),
+                            cudaMemcpyHostToDevice, s));
+  GASP_CUDA(cudaStreamSynchronize(s));
+  b->multi_tiles = begin.back();
+  b->multi_max_L = max_L;
+  return GASP_OK;
+}
+
 // One interval of all groups, issued on the per-group streams (captured into
-// the graph by the caller).
-int batch_issue_interval(gasp_batch *b, cudaStream_t origin, int check_int, double up) {
+// the graph by the caller).  layout 1: the sweeps of all groups are one
+// k_sweep_multi launch on the origin stream (batch_prepare_multi first), the
+// checks still one branch per group.
+int batch_issue_interval(gasp_batch *b, cudaStream_t origin, int check_int, double up,
+                         int layout) {
+  if (layout == 1) {
+    const int rc = launch_sweep_multi(b->d_multi, b->d_tile_begin, b->ngroups, b->multi_tiles,
+                                      b->multi_max_L, b->rng_kind == GASP_RNG_MWC64X ? kRngMwc
+                                                                                     : kRngXorwow,
+                                      origin);
+    if (rc) return rc;
+  }
   GASP_CUDA(cudaEventRecord(b->events[0], origin));
   for (int g = 0; g < b->ngroups; ++g) {
     cudaStream_t sg = b->streams[g];
     GASP_CUDA(cudaStreamWaitEvent(sg, b->events[0], 0));
-    const SweepLaunch p = group_launch(b, g, check_int);
-    int rc = launch_sweep_exact(p, sg);
-    if (rc) return rc;
+    int rc = GASP_OK;
+    if (layout != 1) {
+      const SweepLaunch p = group_launch(b, g, check_int);
+      rc = launch_sweep_exact(p, sg);
+      if (rc) return rc;
+    }
     rc = launch_check_compact(b->grids[g]->d_mag, b->d_active[g], b->d_small + 2 * g,
                               b->groups[g].ngrids, up, b->d_counts + (size_t)g * b->max_intervals,
                               b->d_small + 2 * g + 1, b->max_intervals, sg);
@@ -317,6 +380,36 @@ int batch_issue_interval(gasp_batch *b, cudaStream_t origin, int check_int, doub
     GASP_CUDA(cudaStreamWaitEvent(origin, b->events[1 + g], 0));
   }
   return GASP_OK;
+}
+
+// The interval graph for (check_int, up, layout), captured once and cached.
+// Leaves the batch reset (an uncaptured warm-up interval sets the kernels'
+// launch attributes first).  The tables must be prepared.
+int batch_build_graph(gasp_batch *b, cudaStream_t s, int check_int, double up, int layout) {
+  if (b->exec && b->graph_check_int == check_int && b->graph_up == up &&
+      b->graph_layout == layout)
+    return GASP_OK;
+  if (b->exec) {
+    cudaGraphExecDestroy(b->exec);
+    b->exec = nullptr;
+  }
+  int rc;
+  if (layout == 1 && (rc = batch_prepare_multi(b, check_int, s))) return rc;
+  if ((rc = batch_issue_interval(b, s, check_int, up, layout))) return rc;
+  GASP_CUDA(cudaStreamSynchronize(s));
+  cudaGraph_t graph;
+  GASP_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
+  rc = batch_issue_interval(b, s, check_int, up, layout);
+  cudaError_t e = cudaStreamEndCapture(s, &graph);
+  if (rc) return rc;
+  if (e != cudaSuccess) return cuda_fail(e, "graph capture", __FILE__, __LINE__);
+  e = cudaGraphInstantiate(&b->exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) return cuda_fail(e, "graph instantiate", __FILE__, __LINE__);
+  b->graph_check_int = check_int;
+  b->graph_up = up;
+  b->graph_layout = layout;
+  return batch_reset(b, s);  // restart from a clean state after the warm-up interval
 }
 
 }  // namespace
@@ -376,7 +469,8 @@ int gasp_batch_free(gasp_batch_t *b) { return batch_release(b); }
 
 int gasp_batch_swarm(gasp_batch_t *b, int tot_nsweeps, int check_int, double up_thr, int mode,
                      int *counts_out, long long *attempts_out, double *elapsed_out) {
-  if (!b || tot_nsweeps < 0 || check_int <= 0 || (mode != GASP_BATCH_PLAIN && mode != GASP_BATCH_GRAPH))
+  if (!b || tot_nsweeps < 0 || check_int <= 0 ||
+      (mode != GASP_BATCH_PLAIN && mode != GASP_BATCH_GRAPH && mode != GASP_BATCH_MULTI))
     return GASP_ERR_INVALID;
   const int nint = tot_nsweeps / check_int;
   int rc;
@@ -402,29 +496,14 @@ int gasp_batch_swarm(gasp_batch_t *b, int tot_nsweeps, int check_int, double up_
   std::vector<int> counts((size_t)b->ngroups * nint, 0);
   long long attempts = 0;
   const auto t0 = std::chrono::steady_clock::now();
-  if (mode == GASP_BATCH_GRAPH) {
-    if (!b->exec || b->graph_check_int != check_int || b->graph_up != up_thr) {
-      if (b->exec) {
-        cudaGraphExecDestroy(b->exec);
-        b->exec = nullptr;
-      }
-      // An uncaptured interval first sets the kernels' launch attributes.
-      if ((rc = batch_issue_interval(b, s, check_int, up_thr))) return rc;
-      GASP_CUDA(cudaStreamSynchronize(s));
-      cudaGraph_t graph;
-      GASP_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
-      rc = batch_issue_interval(b, s, check_int, up_thr);
-      cudaError_t e = cudaStreamEndCapture(s, &graph);
-      if (rc) return rc;
-      if (e != cudaSuccess) return cuda_fail(e, "graph capture", __FILE__, __LINE__);
-      e = cudaGraphInstantiate(&b->exec, graph, 0);
-      cudaGraphDestroy(graph);
-      if (e != cudaSuccess) return cuda_fail(e, "graph instantiate", __FILE__, __LINE__);
-      b->graph_check_int = check_int;
-      b->graph_up = up_thr;
-      // restart from a clean state after the warm-up interval
-      if ((rc = batch_reset(b, s))) return rc;
+  if (mode == GASP_BATCH_GRAPH || mode == GASP_BATCH_MULTI) {
+    const int layout = mode == GASP_BATCH_MULTI ? 1 : b->layout;
+    if (layout == 1 && !multi_possible(b)) {
+      set_error("gasp_batch_swarm: one persistent launch needs integer thresholds and "
+                "lattices in shared memory for every group");
+      return GASP_ERR_UNSUPPORTED;
     }
+    if ((rc = batch_build_graph(b, s, check_int, up_thr, layout))) return rc;
     for (int i = 0; i < nint; ++i) GASP_CUDA(cudaGraphLaunch(b->exec, s));
     GASP_CUDA(cudaStreamSynchronize(s));
     for (int g = 0; g < b->ngroups; ++g) {
@@ -524,13 +603,42 @@ int gasp_batch_autotune(gasp_batch_t *b, int nsweeps, int *choice_out) {
       choice_out[2 * g + 1] = cand[best_i].second;
     }
   }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  if (b->exec) {  // kernel choices changed: recapture on the next run
+  // Layout of the interval graph: one kernel per group (concurrent branches)
+  // or every group in one persistent launch.  Each is timed on three interval
+  // replays of nsweeps sweeps in which no replica finishes (up = 2).
+  b->layout = 0;
+  b->layout_ms[0] = b->layout_ms[1] = -1.f;
+  if (rc == GASP_OK && b->exec) {  // kernel choices changed: recapture
     cudaGraphExecDestroy(b->exec);
     b->exec = nullptr;
   }
+  if (rc == GASP_OK && multi_possible(b)) {
+    for (int layout = 0; layout < 2 && rc == GASP_OK; ++layout) {
+      if ((rc = batch_build_graph(b, s, nsweeps, 2.0, layout))) break;
+      GASP_CUDA(cudaGraphLaunch(b->exec, s));  // warm-up replay
+      GASP_CUDA(cudaEventRecord(e0, s));
+      for (int i = 0; i < 3; ++i) GASP_CUDA(cudaGraphLaunch(b->exec, s));
+      GASP_CUDA(cudaEventRecord(e1, s));
+      GASP_CUDA(cudaEventSynchronize(e1));
+      GASP_CUDA(cudaEventElapsedTime(&b->layout_ms[layout], e0, e1));
+    }
+    if (rc == GASP_OK && b->layout_ms[1] < b->layout_ms[0]) b->layout = 1;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (b->exec) {  // built for timing only: the next run captures its own
+    cudaGraphExecDestroy(b->exec);
+    b->exec = nullptr;
+  }
+  if (rc == GASP_OK) rc = batch_reset(b, s);
   return rc;
+}
+
+int gasp_batch_layout(const gasp_batch_t *b, float *ms_per_group_kernels, float *ms_one_launch) {
+  if (!b) return -1;
+  if (ms_per_group_kernels) *ms_per_group_kernels = b->layout_ms[0];
+  if (ms_one_launch) *ms_one_launch = b->layout_ms[1];
+  return b->layout;
 }
 
 }  // extern "C"

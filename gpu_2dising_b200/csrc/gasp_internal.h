@@ -95,6 +95,9 @@ struct SweepLaunch {
 // Sweep parameters of a replica set + RNG whose tables are ready
 // (prepare_tables called for the set's beta, h); gasp_api.cu.
 SweepLaunch launch_for(gasp_grids_t *g, gasp_rng_t *r);
+// Re-seeds an RNG state set in place (gasp_api.cu); its buffer is kept, so
+// graphs that captured it stay valid.
+int rng_reseed(gasp_rng_t *r, unsigned long long seed);
 int prepare_tables(gasp_grids_t *g, double beta, double h);
 
 // Device-side committor check + compaction (gasp_batch.cu): fates of active
@@ -117,6 +120,11 @@ int launch_rng_init(uint32_t *rng, int ngrids, int stride, unsigned long long se
 int launch_build_thresholds(const float *d_pacc20, uint32_t *d_thr10, int *d_flags, cudaStream_t s);
 int launch_sweep_exact(const SweepLaunch &p, cudaStream_t s);
 int launch_sweep_trace_cpu(const SweepLaunch &p, cudaStream_t s);
+// One launch over several groups (gasp_kernels.cu k_sweep_multi): d_groups
+// [ngroups] sweep parameters in device memory, d_tile_begin [ngroups + 1] the
+// first CTA of each group; integer thresholds, one RNG kind for all.
+int launch_sweep_multi(const SweepLaunch *d_groups, const int *d_tile_begin, int ngroups,
+                       int total_tiles, int max_L, int rng_kind, cudaStream_t s);
 // One warp per replica, either stream (gasp_tail.cu); p.n_active is the
 // launch shape (an upper bound of *p.n_active_dev when that is set).
 int launch_sweep_tail(const SweepLaunch &p, cudaStream_t s);

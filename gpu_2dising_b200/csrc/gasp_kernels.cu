@@ -209,6 +209,48 @@ __device__ __forceinline__ void epilogue_mag(const uint32_t *my, const SweepLaun
   }
 }
 
+// One lane's attempts of a generic-kernel batch on its staged lattice `my`
+// (word w at my[w*32]); L_ > 0 compile-time side length, else L.
+template <int L_, bool kFloatCmp, int kRng, bool kStoreAlways>
+__device__ __forceinline__ void exact_run(const SweepLaunch &p, int rep, uint32_t *my, int L,
+                                          const uint32_t *thr_s, const float *pacc_s) {
+  const int N = L * L;
+  RngPolicy<kRng> rg;
+  rg.load(p.rng, p.rng_stride, rep);
+  const float shrink = (1.0f - FLT_EPSILON) * (float)N;
+  for (int sw = 0; sw < p.nsweeps; ++sw) {
+    // unroll 4: 1.2-1.5x over the compiler's choice on the reference stream
+    // (L=48: 2.45e11 vs 2.04e11 attempts/s at 32768 replicas; L=100: 3.3e10 vs 2.2e10)
+#pragma unroll 4
+    for (int a = 0; a < N; ++a) {
+      const int s = (int)rg.template site<(L_ > 0 ? L_ * L_ : 0)>(shrink, N);
+      const int row = s / L;
+      const int col = s - row * L;
+      const int su = row == 0 ? s + N - L : s - L;
+      const int sd = row == L - 1 ? s - N + L : s + L;
+      const int sl = col == 0 ? s + L - 1 : s - 1;
+      const int sr = col == L - 1 ? s - L + 1 : s + 1;
+      const uint32_t wc = my[(s >> 5) * kTile];
+      const uint32_t bs = (wc >> (s & 31)) & 1u;
+      const uint32_t k = bit_at(my, su) + bit_at(my, sd) + bit_at(my, sl) + bit_at(my, sr);
+      const uint32_t cls = 5u * bs + k;
+      const uint32_t x2 = rg.next();
+      bool acc;
+      if (kFloatCmp) {
+        acc = _curand_uniform(x2) < pacc_s[2 * cls];  // index 10*bs + 2k
+      } else {
+        acc = x2 <= thr_s[cls];
+      }
+      if constexpr (kStoreAlways) {  // written back unchanged when rejected: no branch
+        my[(s >> 5) * kTile] = acc ? wc ^ (1u << (s & 31)) : wc;
+      } else {
+        if (acc) my[(s >> 5) * kTile] = wc ^ (1u << (s & 31));
+      }
+    }
+  }
+  rg.store(p.rng, p.rng_stride, rep);
+}
+
 // ---------------------------------------------------------------------------
 // Exact sweep.  L_ > 0: compile-time side length; L_ == 0: runtime p.L.
 // ---------------------------------------------------------------------------
@@ -239,42 +281,7 @@ __global__ void __launch_bounds__(256) k_sweep_exact(SweepLaunch p) {
   if (!tile_live) return;
 
   uint32_t *my = lat_s + lane;
-  if (live) {
-    RngPolicy<kRng> rg;
-    rg.load(p.rng, p.rng_stride, rep);
-    const float shrink = (1.0f - FLT_EPSILON) * (float)N;
-    for (int sw = 0; sw < p.nsweeps; ++sw) {
-      // unroll 4: 1.2-1.5x over the compiler's choice on the reference stream
-      // (L=48: 2.45e11 vs 2.04e11 attempts/s at 32768 replicas; L=100: 3.3e10 vs 2.2e10)
-#pragma unroll 4
-      for (int a = 0; a < N; ++a) {
-        const int s = (int)rg.template site<(L_ > 0 ? L_ * L_ : 0)>(shrink, N);
-        const int row = s / L;
-        const int col = s - row * L;
-        const int su = row == 0 ? s + N - L : s - L;
-        const int sd = row == L - 1 ? s - N + L : s + L;
-        const int sl = col == 0 ? s + L - 1 : s - 1;
-        const int sr = col == L - 1 ? s - L + 1 : s + 1;
-        const uint32_t wc = my[(s >> 5) * kTile];
-        const uint32_t bs = (wc >> (s & 31)) & 1u;
-        const uint32_t k = bit_at(my, su) + bit_at(my, sd) + bit_at(my, sl) + bit_at(my, sr);
-        const uint32_t cls = 5u * bs + k;
-        const uint32_t x2 = rg.next();
-        bool acc;
-        if (kFloatCmp) {
-          acc = _curand_uniform(x2) < pacc_s[2 * cls];  // index 10*bs + 2k
-        } else {
-          acc = x2 <= thr_s[cls];
-        }
-        if constexpr (kStoreAlways) {  // written back unchanged when rejected: no branch
-          my[(s >> 5) * kTile] = acc ? wc ^ (1u << (s & 31)) : wc;
-        } else {
-          if (acc) my[(s >> 5) * kTile] = wc ^ (1u << (s & 31));
-        }
-      }
-    }
-    rg.store(p.rng, p.rng_stride, rep);
-  }
+  if (live) exact_run<L_, kFloatCmp, kRng, kStoreAlways>(p, rep, my, L, thr_s, pacc_s);
   __syncwarp();
   epilogue_mag(my, p, N, W, live, rep);
   stage_out(lat_s, p, W, tile, lane, live, rep);
@@ -356,14 +363,15 @@ struct LatticeStore<Words, false> {
   __device__ __forceinline__ static uint32_t *get(uint32_t *dyn) { return dyn; }
 };
 
-// One attempt of k_sweep_rows on site s.  kLookahead: also draw the next
-// attempt's site (after this attempt's acceptance draw, as the reference's
-// stream order requires) so its conversion overlaps this attempt's
-// shared-memory round trips.
-template <int L, bool kFloatCmp, bool kLookahead, bool kStoreAlways, typename Rng>
-__device__ __forceinline__ void row_attempt(uint32_t &s, Rng &rg, const char *latb,
-                                            const char *thrb, const char *paccb, uint32_t lane4,
-                                            float shrink) {
+// The lattice step of one row-kernel attempt: site s, raw acceptance draw
+// x2.  Reads the site's row word(s) and the words above and below, forms the
+// 5-spin pattern, compares x2 with the pattern's threshold and writes the
+// site's word back (flipped on acceptance; kStoreAlways: unchanged otherwise,
+// else only on acceptance).  kKind picks the row-window form measured faster
+// with that stream.
+template <int L, bool kFloatCmp, bool kStoreAlways, int kKind>
+__device__ __forceinline__ void row_apply(uint32_t s, uint32_t x2, const char *latb,
+                                          const char *thrb, const char *paccb, uint32_t lane4) {
   constexpr int N = L * L;
   constexpr int R = L / 32;
   constexpr bool kPow2 = (L & (L - 1)) == 0;
@@ -388,7 +396,7 @@ __device__ __forceinline__ void row_attempt(uint32_t &s, Rng &rg, const char *la
   } else if constexpr (R == 2) {
     wc = *reinterpret_cast<const uint32_t *>(latb + offc);
     const uint32_t wx = *reinterpret_cast<const uint32_t *>(latb + (offc ^ 128u));
-    if constexpr (Rng::kKind == kRngXorwow) {
+    if constexpr (kKind == kRngXorwow) {
       // The row is the circular 64 bits (wx:wc) seen from the site's word: for
       // b >= 3 the bits b-1..b+1 sit in (wx:wc) >> (b-3) (b = 31 reaches wx
       // bit 0); for b < 3 the left neighbour wraps to the top of wx, so the
@@ -415,9 +423,7 @@ __device__ __forceinline__ void row_attempt(uint32_t &s, Rng &rg, const char *la
   const uint32_t u = __funnelshift_r(wu, wu, b + 27u);  // bit 5: up
   const uint32_t d = __funnelshift_r(wd, wd, b + 26u);  // bit 6: down
   const uint32_t p4 = (t & 0x1Cu) | (u & 0x20u) | (d & 0x40u);
-  const uint32_t x2 = rg.next();
   const uint32_t sc = s;
-  if constexpr (kLookahead) s = rg.template site<N>(shrink, N);
   bool acc;
   if constexpr (kFloatCmp) {
     acc = _curand_uniform(x2) < *reinterpret_cast<const float *>(paccb + p4);
@@ -432,6 +438,72 @@ __device__ __forceinline__ void row_attempt(uint32_t &s, Rng &rg, const char *la
   }
 }
 
+
+// One attempt of k_sweep_rows on site s: the acceptance draw, then (kLookahead)
+// the next attempt's site -- the reference's stream order -- so its
+// conversion overlaps this attempt's shared-memory round trips.
+template <int L, bool kFloatCmp, bool kLookahead, bool kStoreAlways, typename Rng>
+__device__ __forceinline__ void row_attempt(uint32_t &s, Rng &rg, const char *latb,
+                                            const char *thrb, const char *paccb, uint32_t lane4,
+                                            float shrink) {
+  constexpr int N = L * L;
+  const uint32_t x2 = rg.next();
+  const uint32_t sc = s;
+  if constexpr (kLookahead) s = rg.template site<N>(shrink, N);
+  row_apply<L, kFloatCmp, kStoreAlways, Rng::kKind>(sc, x2, latb, thrb, paccb, lane4);
+}
+
+// Threshold and float tables of the row kernels, indexed by the 5-spin
+// pattern (bits 0 left, 1 centre, 2 right, 3 up, 4 down; 1 == spin +1).
+__device__ __forceinline__ void pattern_tables(const SweepLaunch &p, uint32_t *thrP, float *paccP,
+                                               int lane) {
+  const int c = (lane >> 1) & 1;
+  const int cls = 5 * c + __popc(lane & 0x1D);
+  thrP[lane] = p.thr[cls];
+  paccP[lane] = p.pacc_f[2 * cls];
+}
+
+// One lane's attempts of a row-kernel batch (N * nsweeps of them) on its
+// staged lattice, software-pipelined: draw order x1(a), x2(a), x1(a+1), ...
+// as in the reference.  The host keeps N*nsweeps < 2^31.
+template <int L, bool kFloatCmp, bool kStoreAlways, int kRng>
+__device__ __forceinline__ void rows_run(const SweepLaunch &p, int rep, const uint32_t *lat,
+                                         const uint32_t *thrP, const float *paccP, int lane) {
+  constexpr int N = L * L;
+  const char *latb = reinterpret_cast<const char *>(lat);
+  const char *thrb = reinterpret_cast<const char *>(thrP);
+  const char *paccb = reinterpret_cast<const char *>(paccP);
+  RngPolicy<kRng> rg;
+  rg.load(p.rng, p.rng_stride, rep);
+  const float shrink = (1.0f - FLT_EPSILON) * (float)N;
+  const uint32_t lane4 = (uint32_t)lane << 2;
+  uint32_t s = rg.template site<N>(shrink, N);
+  const int total = N * p.nsweeps;
+  if constexpr (L == 64 && kRng == kRngXorwow) {
+    // unroll measured at L=64 on the reference stream: 8 -> 4.40e11, 5 -> 4.23e11,
+    // 16 -> 4.36e11, 10 -> 4.28e11 attempts/s (the MWC64X stream is fastest at 5)
+#pragma unroll 8
+    for (int a = 0; a < total - 1; ++a)
+      row_attempt<L, kFloatCmp, true, kStoreAlways>(s, rg, latb, thrb, paccb, lane4, shrink);
+    row_attempt<L, kFloatCmp, false, kStoreAlways>(s, rg, latb, thrb, paccb, lane4, shrink);
+  } else if constexpr (L == 128 || (L == 32 && kRng == kRngXorwow) ||
+                       (L == 96 && kRng == kRngMwc)) {
+    // unroll 16 measured 2-4 % faster than 5 for these (L, stream) pairs
+    // (e.g. L=128, 16384 replicas: 1.27e11 vs 1.23e11 exact, 1.45e11 vs 1.42e11
+    // MWC64X; L=32 exact, 16384 replicas: 2.85e11 vs 2.74e11) and slower for the others
+#pragma unroll 16
+    for (int a = 0; a < total - 1; ++a)
+      row_attempt<L, kFloatCmp, true, kStoreAlways>(s, rg, latb, thrb, paccb, lane4, shrink);
+    row_attempt<L, kFloatCmp, false, kStoreAlways>(s, rg, latb, thrb, paccb, lane4, shrink);
+  } else {
+#pragma unroll 5
+    for (int a = 0; a < total - 1; ++a)
+      row_attempt<L, kFloatCmp, true, kStoreAlways>(s, rg, latb, thrb, paccb, lane4, shrink);
+    row_attempt<L, kFloatCmp, false, kStoreAlways>(s, rg, latb, thrb, paccb, lane4, shrink);
+  }
+  rg.store(p.rng, p.rng_stride, rep);
+}
+
 template <int L, bool kStatic, bool kFloatCmp, int kRng, bool kStoreAlways = false,
           bool kBulk = false>
 __global__ void __launch_bounds__(32) k_sweep_rows(SweepLaunch p) {
@@ -444,13 +516,7 @@ __global__ void __launch_bounds__(32) k_sweep_rows(SweepLaunch p) {
   uint32_t *lat = LatticeStore<W * kTile, kStatic>::get(dyn);
 
   const int lane = threadIdx.x;
-  {
-    // pattern bits: 0 left, 1 centre, 2 right, 3 up, 4 down (1 == spin +1)
-    const int c = (lane >> 1) & 1;
-    const int cls = 5 * c + __popc(lane & 0x1D);
-    thrP[lane] = p.thr[cls];
-    paccP[lane] = p.pacc_f[2 * cls];
-  }
+  pattern_tables(p, thrP, paccP, lane);
   const int n_act = live_count(p);
   const int tile = blockIdx.x;
   if (tile * kTile >= n_act) return;  // whole CTA (one warp) idle this batch
@@ -470,42 +536,8 @@ __global__ void __launch_bounds__(32) k_sweep_rows(SweepLaunch p) {
   }
   __syncwarp();
 
-  const char *latb = reinterpret_cast<const char *>(lat);
-  const char *thrb = reinterpret_cast<const char *>(thrP);
-  const char *paccb = reinterpret_cast<const char *>(paccP);
-  if (live && staged && p.nsweeps > 0) {
-    RngPolicy<kRng> rg;
-    rg.load(p.rng, p.rng_stride, rep);
-    const float shrink = (1.0f - FLT_EPSILON) * (float)N;
-    const uint32_t lane4 = (uint32_t)lane << 2;
-    // Software pipeline over the batch's attempts; draw order x1(a), x2(a),
-    // x1(a+1), ... as in the reference.  The host keeps N*nsweeps < 2^31.
-    uint32_t s = rg.template site<N>(shrink, N);
-    const int total = N * p.nsweeps;
-    if constexpr (L == 64 && kRng == kRngXorwow) {
-      // unroll measured at L=64 on the reference stream: 8 -> 4.40e11, 5 -> 4.23e11,
-      // 16 -> 4.36e11, 10 -> 4.28e11 attempts/s (the MWC64X stream is fastest at 5)
-#pragma unroll 8
-      for (int a = 0; a < total - 1; ++a)
-        row_attempt<L, kFloatCmp, true, kStoreAlways>(s, rg, latb, thrb, paccb, lane4, shrink);
-      row_attempt<L, kFloatCmp, false, kStoreAlways>(s, rg, latb, thrb, paccb, lane4, shrink);
-    } else if constexpr (L == 128 || (L == 32 && kRng == kRngXorwow) ||
-                         (L == 96 && kRng == kRngMwc)) {
-      // unroll 16 measured 2-4 % faster than 5 for these (L, stream) pairs
-      // (e.g. L=128, 16384 replicas: 1.27e11 vs 1.23e11 exact, 1.45e11 vs 1.42e11
-      // MWC64X; L=32 exact, 16384 replicas: 2.85e11 vs 2.74e11) and slower for the others
-#pragma unroll 16
-      for (int a = 0; a < total - 1; ++a)
-        row_attempt<L, kFloatCmp, true, kStoreAlways>(s, rg, latb, thrb, paccb, lane4, shrink);
-      row_attempt<L, kFloatCmp, false, kStoreAlways>(s, rg, latb, thrb, paccb, lane4, shrink);
-    } else {
-#pragma unroll 5
-      for (int a = 0; a < total - 1; ++a)
-        row_attempt<L, kFloatCmp, true, kStoreAlways>(s, rg, latb, thrb, paccb, lane4, shrink);
-      row_attempt<L, kFloatCmp, false, kStoreAlways>(s, rg, latb, thrb, paccb, lane4, shrink);
-    }
-    rg.store(p.rng, p.rng_stride, rep);
-  }
+  if (live && staged && p.nsweeps > 0)
+    rows_run<L, kFloatCmp, kStoreAlways, kRng>(p, rep, lat, thrP, paccP, lane);
   __syncwarp();
   if (!staged) return;  // the bulk load timed out: flagged, nothing written back
   epilogue_mag(lat + lane, p, N, W, live, rep);
@@ -517,6 +549,173 @@ __global__ void __launch_bounds__(32) k_sweep_rows(SweepLaunch p) {
   } else {
     stage_out(lat, p, W, tile, lane, live, rep);
   }
+}
+
+// ---------------------------------------------------------------------------
+// Warp-specialised row kernel (sweep variant 10): two warps per tile of 32
+// replicas.  Warp 0 draws every attempt's site and acceptance value in the
+// replica's own stream order (site x1(a), acceptance x2(a), x1(a+1), ...) and
+// queues them in shared memory, kWsChunk attempts per lane per slot, two
+// slots; warp 1 runs the lattice steps (row_apply).  The lattice chain holds
+// no RNG work, and each scheduler gets twice the warps to issue from.  Slot
+// hand-over on mbarriers (32 arrivals, one per lane) with bounded waits: on
+// expiry g_stage_timeout is set and both warps stop.  Same draws, same
+// arithmetic, same result as k_sweep_rows.
+// ---------------------------------------------------------------------------
+constexpr int kWsChunk = 16;
+constexpr int kWsSlots = 2;
+
+__device__ __forceinline__ void ws_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(
+                   (uint32_t)__cvta_generic_to_shared(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ bool ws_wait(uint64_t *bar, uint32_t parity) {
+  const uint32_t b = (uint32_t)__cvta_generic_to_shared(bar);
+  for (int i = 0; i < kStagePolls; ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(done)
+        : "r"(b), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+template <int L, bool kStatic, bool kFloatCmp, int kRng>
+__global__ void __launch_bounds__(64) k_sweep_ws(SweepLaunch p) {
+  static_assert(L % 32 == 0, "rows of whole words");
+  constexpr int N = L * L;
+  constexpr int W = N / 32;
+  static_assert(N % kWsChunk == 0, "a batch is a whole number of chunks");
+  __shared__ __align__(16) uint32_t thrP[32];
+  __shared__ __align__(16) float paccP[32];
+  __shared__ __align__(16) uint2 q[kWsSlots][kWsChunk][kTile];  // (site, acceptance draw)
+  __shared__ __align__(8) uint64_t full[kWsSlots], empty[kWsSlots];
+  extern __shared__ __align__(16) uint32_t dyn[];
+  uint32_t *lat = LatticeStore<W * kTile, kStatic>::get(dyn);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (warp == 0) pattern_tables(p, thrP, paccP, lane);
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < kWsSlots; ++i) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 32;" ::"r"(
+                       (uint32_t)__cvta_generic_to_shared(&full[i]))
+                   : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 32;" ::"r"(
+                       (uint32_t)__cvta_generic_to_shared(&empty[i]))
+                   : "memory");
+    }
+  }
+  const int n_act = live_count(p);
+  const int tile = blockIdx.x;
+  if (tile * kTile >= n_act) return;  // whole CTA idle this batch
+  const int slot = tile * kTile + lane;
+  const bool live = slot < n_act;
+  const int rep = live ? (p.active ? p.active[slot] : slot) : 0;
+  if (warp == 1) stage_in(lat, p, W, tile, lane, live, rep);
+  __syncthreads();
+  const int nch = N / kWsChunk * p.nsweeps;
+  bool ok = true;
+  if (warp == 0) {  // producer
+    RngPolicy<kRng> rg;
+    if (live) rg.load(p.rng, p.rng_stride, rep);
+    const float shrink = (1.0f - FLT_EPSILON) * (float)N;
+    for (int k = 0; k < nch; ++k) {
+      const int sl = k % kWsSlots;
+      if (k >= kWsSlots && !ws_wait(&empty[sl], (uint32_t)((k / kWsSlots) - 1) & 1u)) {
+        ok = false;
+        break;
+      }
+      if (live) {
+#pragma unroll
+        for (int i = 0; i < kWsChunk; ++i) {
+          const uint32_t site = rg.template site<N>(shrink, N);
+          const uint32_t x2 = rg.next();
+          q[sl][i][lane] = make_uint2(site, x2);
+        }
+      }
+      ws_arrive(&full[sl]);
+    }
+    if (live && ok) rg.store(p.rng, p.rng_stride, rep);
+  } else {  // consumer: the lattice chain
+    const char *latb = reinterpret_cast<const char *>(lat);
+    const char *thrb = reinterpret_cast<const char *>(thrP);
+    const char *paccb = reinterpret_cast<const char *>(paccP);
+    const uint32_t lane4 = (uint32_t)lane << 2;
+    for (int k = 0; k < nch; ++k) {
+      const int sl = k % kWsSlots;
+      if (!ws_wait(&full[sl], (uint32_t)(k / kWsSlots) & 1u)) {
+        ok = false;
+        break;
+      }
+      uint2 e[kWsChunk];
+#pragma unroll
+      for (int i = 0; i < kWsChunk; ++i) e[i] = q[sl][i][lane];
+      ws_arrive(&empty[sl]);
+      if (live) {
+#pragma unroll
+        for (int i = 0; i < kWsChunk; ++i)
+          row_apply<L, kFloatCmp, true, kRng>(e[i].x, e[i].y, latb, thrb, paccb, lane4);
+      }
+    }
+  }
+  if (!ok && lane == 0) atomicOr(&g_stage_timeout, 1);
+  const bool all_ok = __syncthreads_and(ok ? 1 : 0) != 0;
+  if (!all_ok) return;  // flagged; the tile is not written back
+  if (warp == 1) {
+    epilogue_mag(lat + lane, p, N, W, live, rep);
+    stage_out(lat, p, W, tile, lane, live, rep);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Several replica groups of different L in one launch (the batched path).
+// CTA b sweeps tile b - tile_begin[g] of the group g whose CTA range holds b,
+// with that group's L-specialised attempt loop (the row loop for L = 32, 64,
+// 96, 128; the generic loop otherwise) and its own tables, RNG states, active
+// list and device live count.  Integer thresholds only.  The dynamic shared
+// memory is the largest group's tile; the host orders groups by decreasing
+// work per tile, so the longest chains start first.
+// ---------------------------------------------------------------------------
+template <int kRng>
+__global__ void __launch_bounds__(32) k_sweep_multi(const SweepLaunch *groups,
+                                                    const int *tile_begin, int ngroups) {
+  __shared__ __align__(16) uint32_t thrP[32];
+  __shared__ __align__(16) float paccP[32];
+  extern __shared__ __align__(16) uint32_t dyn[];
+  int g = 0;
+  while (g + 1 < ngroups && (int)blockIdx.x >= tile_begin[g + 1]) ++g;
+  const SweepLaunch &p = groups[g];
+  const int lane = threadIdx.x;
+  const int L = p.L, N = L * L, W = (N + 31) >> 5;
+  const int n_act = live_count(p);
+  const int tile = (int)blockIdx.x - tile_begin[g];
+  if (tile * kTile >= n_act) return;  // whole CTA idle this batch
+  const int slot = tile * kTile + lane;
+  const bool live = slot < n_act;
+  const int rep = live ? (p.active ? p.active[slot] : slot) : 0;
+  const bool rows = L == 32 || L == 64 || L == 96 || L == 128;
+  if (rows) pattern_tables(p, thrP, paccP, lane);
+  else if (lane < 10) thrP[lane] = p.thr[lane];
+  stage_in(dyn, p, W, tile, lane, live, rep);
+  __syncwarp();
+  if (live && p.nsweeps > 0) {
+    switch (L) {
+      case 32: rows_run<32, false, true, kRng>(p, rep, dyn, thrP, paccP, lane); break;
+      case 64: rows_run<64, false, true, kRng>(p, rep, dyn, thrP, paccP, lane); break;
+      case 96: rows_run<96, false, true, kRng>(p, rep, dyn, thrP, paccP, lane); break;
+      case 128: rows_run<128, false, true, kRng>(p, rep, dyn, thrP, paccP, lane); break;
+      case 48: exact_run<48, false, kRng, false>(p, rep, dyn + lane, L, thrP, paccP); break;
+      default: exact_run<0, false, kRng, false>(p, rep, dyn + lane, L, thrP, paccP); break;
+    }
+  }
+  __syncwarp();
+  epilogue_mag(dyn + lane, p, N, W, live, rep);
+  stage_out(dyn, p, W, tile, lane, live, rep);
 }
 
 // ---------------------------------------------------------------------------
@@ -713,6 +912,18 @@ int launch_rows(Kern kern, const SweepLaunch &p, size_t dyn_smem, cudaStream_t s
   return GASP_OK;
 }
 
+// Two warps (producer, consumer) per tile.
+template <typename Kern>
+int launch_ws(Kern kern, const SweepLaunch &p, size_t dyn_smem, cudaStream_t s) {
+  const int tiles = tiles_for(p.n_active);
+  if (tiles == 0) return GASP_OK;
+  if (dyn_smem > 0)
+    GASP_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_smem));
+  kern<<<tiles, 64, dyn_smem, s>>>(p);
+  GASP_CUDA(cudaGetLastError());
+  return GASP_OK;
+}
+
 template <bool F, int K>
 int dispatch_kind(const SweepLaunch &p, cudaStream_t s) {
   if (p.lattice_in_global) {
@@ -728,6 +939,15 @@ int dispatch_kind(const SweepLaunch &p, cudaStream_t s) {
   }
   const size_t dyn128 = (size_t)words_per_replica(128) * kTile * sizeof(uint32_t);
   const size_t dyn96 = (size_t)words_per_replica(96) * kTile * sizeof(uint32_t);
+  if (p.variant == 10) {  // warp-specialised row kernel (draws in one warp, lattice in the other)
+    switch (p.L) {
+      case 32: return launch_ws(k_sweep_ws<32, true, F, K>, p, 0, s);
+      case 64: return launch_ws(k_sweep_ws<64, true, F, K>, p, 0, s);
+      case 96: return launch_ws(k_sweep_ws<96, false, F, K>, p, dyn96, s);
+      case 128: return launch_ws(k_sweep_ws<128, false, F, K>, p, dyn128, s);
+      default: break;  // other L: the default kernels
+    }
+  }
   if (p.variant == 9) {  // variant 0 with bulk-copy staging of the tiles (measured slower)
     switch (p.L) {
       case 32: return launch_rows(k_sweep_rows<32, true, F, K, true, true>, p, 0, s);
@@ -804,7 +1024,7 @@ int launch_sweep_exact(const SweepLaunch &p, cudaStream_t s) {
     const int rc = p.float_compare ? dispatch_exact<true>(q, s) : dispatch_exact<false>(q, s);
     if (rc) return rc;
   }
-  if (p.variant == 9) {  // bulk staging: report a timed-out copy (not while a graph is captured)
+  if (p.variant == 9 || p.variant == 10) {  // report a timed-out wait (not while capturing)
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     GASP_CUDA(cudaStreamIsCapturing(s, &cs));
     if (cs == cudaStreamCaptureStatusNone) {
@@ -821,6 +1041,17 @@ int launch_sweep_exact(const SweepLaunch &p, cudaStream_t s) {
       }
     }
   }
+  return GASP_OK;
+}
+
+int launch_sweep_multi(const SweepLaunch *d_groups, const int *d_tile_begin, int ngroups,
+                       int total_tiles, int max_L, int rng_kind, cudaStream_t s) {
+  if (total_tiles <= 0) return GASP_OK;
+  const size_t smem = (size_t)words_per_replica(max_L) * kTile * sizeof(uint32_t);
+  auto kern = rng_kind == kRngMwc ? k_sweep_multi<kRngMwc> : k_sweep_multi<kRngXorwow>;
+  GASP_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  kern<<<total_tiles, 32, smem, s>>>(d_groups, d_tile_begin, ngroups);
+  GASP_CUDA(cudaGetLastError());
   return GASP_OK;
 }
 

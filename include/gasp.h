@@ -138,8 +138,13 @@ int gasp_grids_shape(const gasp_grids_t *grids, int *L_out, int *ngrids_out);
  * loads and stores (L = 32, 64, 96, 128 in replica order, i.e. without an
  * active list; bit-identical to 0, measured slower; each launch reads back
  * a device flag, so a copy that did not complete within its bounded wait
- * returns GASP_ERR_TIMEOUT).  Values 3, 4 and 8 (retired kernels that were
- * measured slower) and values outside 0..9 return GASP_ERR_INVALID.
+ * returns GASP_ERR_TIMEOUT); 10 the warp-specialised row kernel (L = 32, 64,
+ * 96, 128): per tile of 32 replicas one warp draws the attempts' sites and
+ * acceptance values in each replica's stream order into a shared-memory
+ * queue and a second warp applies them to the lattices (bit-identical to 0;
+ * a wait that does not complete within its bound returns GASP_ERR_TIMEOUT).
+ * Values 3, 4 and 8 (retired kernels that were measured slower) and values
+ * outside 0..10 return GASP_ERR_INVALID.
  * GASP_OPT_WARPS_PER_CTA: tiles per CTA of the generic kernel (1..8).
  * GASP_OPT_TAIL_REPLICAS: device-side committor shooting (itask 1 with
  * compaction) sweeps with variant 6 once at most this many replicas are
@@ -334,24 +339,35 @@ int gasp_batch_create(const gasp_group_t *groups, int ngroups, unsigned long lon
                       int rng_kind, gasp_batch_t **out);
 int gasp_batch_free(gasp_batch_t *batch);
 
-enum { GASP_BATCH_PLAIN = 0, GASP_BATCH_GRAPH = 1 };
+enum { GASP_BATCH_PLAIN = 0, GASP_BATCH_GRAPH = 1, GASP_BATCH_MULTI = 2 };
 /* Nucleation swarm of every group from all spins -1, re-seeded each call:
  * every check_int sweeps a replica whose magnetisation exceeds up_thr is
  * finished (absorbing).  GASP_BATCH_GRAPH: each interval is one CUDA graph
  * running all groups concurrently, finished replicas compacted out on the
  * device, no host synchronisation until the end.  GASP_BATCH_PLAIN: one launch
  * per group per interval over all its replicas, groups in turn, checks on the
- * host (the comparison path).  Both modes give identical counts.
+ * host (the comparison path).  GASP_BATCH_MULTI: as GASP_BATCH_GRAPH with
+ * the sweeps of all groups in one persistent launch (each CTA runs its
+ * group's L-specialised loop; integer thresholds and lattices in shared
+ * memory only, else GASP_ERR_UNSUPPORTED); GASP_BATCH_GRAPH uses that layout
+ * too when the autotuner found it faster.  All modes give identical counts.
  * counts_out[i*ngroups + g] (tot_nsweeps/check_int rows): finished replicas
  * of group g after interval i.  attempts_out: attempted flips credited to
  * unfinished replicas only (the same workload for both modes). */
 int gasp_batch_swarm(gasp_batch_t *batch, int tot_nsweeps, int check_int, double up_thr,
                      int mode, int *counts_out, long long *attempts_out, double *elapsed_out);
-/* Autotuner: times the candidate kernels (row kernel with or without pairwise
- * speculation; tiles per CTA of the generic kernel) for each group on an
- * nsweeps run and keeps the fastest.  choice_out (2*ngroups ints, may be
+/* Autotuner: times the candidate kernels (row kernel with or without the
+ * every-attempt store; tiles per CTA of the generic kernel) for each group on
+ * an nsweeps run and keeps the fastest; then times the interval graph in both
+ * layouts (one kernel per group, or one persistent launch for all groups) and
+ * keeps the faster for GASP_BATCH_GRAPH.  choice_out (2*ngroups ints, may be
  * NULL): (variant, warps per CTA) chosen per group. */
 int gasp_batch_autotune(gasp_batch_t *batch, int nsweeps, int *choice_out);
+/* The layout the autotuner chose (0: one kernel per group, 1: one persistent
+ * launch; -1 for a NULL batch) and its timings of the two (ms for three
+ * intervals; -1 when not timed). */
+int gasp_batch_layout(const gasp_batch_t *batch, float *ms_per_group_kernels,
+                      float *ms_one_launch);
 
 /* ---------------------------------------------- committor surrogate CNN */
 /* A small network predicting pB from a spin grid (no reference counterpart):

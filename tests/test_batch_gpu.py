@@ -1,5 +1,6 @@
 """Batched groups of uneven L, beta, h on a B200: the graph-captured,
-compacting path gives exactly the plain per-group path's results."""
+compacting path -- one kernel per group, or all groups in one persistent
+launch -- gives exactly the plain per-group path's results."""
 import ctypes as C
 
 import numpy as np
@@ -50,6 +51,10 @@ def test_graph_batch_equals_plain(kind):
         # a second graph run (graph reused) reproduces the first
         cg2, ag2, _ = _swarm(h, len(GROUPS), tot, chk, up, nat.BATCH_GRAPH)
         assert np.array_equal(cg, cg2) and ag == ag2
+        # all groups in one persistent launch: the same trajectories, twice
+        for _ in range(2):
+            cm, am, _ = _swarm(h, len(GROUPS), tot, chk, up, nat.BATCH_MULTI)
+            assert np.array_equal(cp, cm) and ap == am
     finally:
         nat.lib().gasp_batch_free(h)
 
@@ -81,7 +86,12 @@ def test_autotune_choices_valid():
         for g, (L, *_r) in enumerate(GROUPS):
             v, w = choice[2 * g], choice[2 * g + 1]
             assert v in (0, 2) and 1 <= w <= 8
+        t0, t1 = C.c_float(), C.c_float()
+        layout = nat.lib().gasp_batch_layout(h, C.byref(t0), C.byref(t1))
+        assert layout in (0, 1) and t0.value > 0 and t1.value > 0
+        assert layout == (1 if t1.value < t0.value else 0)
         c, a, _ = _swarm(h, len(GROUPS), 100, 10, 0.5, nat.BATCH_GRAPH)
-        assert a > 0
+        cp, ap, _ = _swarm(h, len(GROUPS), 100, 10, 0.5, nat.BATCH_PLAIN)
+        assert a > 0 and a == ap and np.array_equal(c, cp)
     finally:
         nat.lib().gasp_batch_free(h)
