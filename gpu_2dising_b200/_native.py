@@ -58,6 +58,7 @@ EXPORTED = (
     "gasp_batch_create", "gasp_batch_free", "gasp_batch_swarm", "gasp_batch_autotune",
     "gasp_batch_layout",
     "gasp_cnn_param_count", "gasp_cnn_create", "gasp_cnn_free", "gasp_cnn_set_params",
+    "gasp_cnn_set_fused",
     "gasp_cnn_get_params", "gasp_cnn_predict", "gasp_cnn_predict_ex", "gasp_cnn_gradients",
     "gasp_cnn_train_step",
 )
@@ -189,6 +190,7 @@ def _bind(lib):
         "gasp_cnn_create": (I, [I, I, C.POINTER(P)]),
         "gasp_cnn_free": (I, [P]),
         "gasp_cnn_set_params": (I, [P, _f32p]),
+        "gasp_cnn_set_fused": (I, [P, I]),
         "gasp_cnn_get_params": (I, [P, _f32p]),
         "gasp_cnn_predict": (I, [P, _i8p, I, _f32p]),
         "gasp_cnn_predict_ex": (I, [P, _i8p, I, _f32p, C.c_void_p]),

@@ -493,6 +493,258 @@ __global__ void __launch_bounds__(128) k_conv_win(ConvArgs a) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Inference forward of the whole network for L = 64 in one kernel.  A work
+// item is an image band of kFzRows output rows; the four layers run back to
+// back on the chip and only the band's spins come from HBM (the pooled sums
+// go out by atomicAdd): layer l computes its rows of the band plus the halo
+// the next layer needs (a1: 14 rows, a2: 12, a3: 10, a4: 8, pooled).
+// Activations stay in shared memory, K-major like k_conv_win's windows
+// ([channel chunk][position][16 B]), in rows of kFzPitch = 66 positions: a
+// ghost column, the 64 pixels, a ghost column, the ghosts holding the
+// circularly wrapped neighbours.  With that pitch the A operand of tap
+// (dy, dx) for 128 consecutive output positions is 128 consecutive input
+// positions starting (1 + dy) * 66 + dx further on, a plain descriptor offset;
+// an M tile covers 128 padded positions, and its ghost positions (3 %) are
+// computed and dropped.  Two TMEM accumulators: while one 4-warp group runs
+// the epilogue of tile t (bias, ReLU, BF16 rounding, stores into the next
+// layer's buffer and the ghost copies, or the pool sums), warp 8 issues the
+// MMAs of tile t + 1.  Same arithmetic as the layer-by-layer kernels (BF16
+// activations, FP32 accumulation, the same K order).
+// ---------------------------------------------------------------------------
+constexpr int kFzRows = 8;     // output rows per band
+constexpr int kFzPitch = 66;   // positions per padded row
+constexpr int kFzLead = 8;     // positions before position 0 (tap reads reach -1)
+constexpr int kFzPosA = 1048;  // positions per chunk, buffer A (a1: 14 rows, a3: 10)
+constexpr int kFzPosB = 912;   // buffer B (a2: 12 rows)
+constexpr int kFzIm = 1024;    // layer-1 im2col rows (8 tiles of 128)
+constexpr int kFzThreads = 288;  // warps 0-7: epilogue (two groups of four), warp 8: MMA issue
+// shared-memory layout (bytes)
+constexpr uint32_t kFzW = 0;                                 // W2..W4, 3 x 32 x 288 bf16
+constexpr uint32_t kFzW1 = kFzW + 3u * kC * 288 * 2;         // W1, 32 x 16 bf16
+constexpr uint32_t kFzBufA = kFzW1 + (uint32_t)kC * 16 * 2;  // [4][kFzPosA][16 B]
+constexpr uint32_t kFzBufB = kFzBufA + 4u * kFzPosA * 16;    // [4][kFzPosB][16 B]
+constexpr uint32_t kFzImB = kFzBufB + 4u * kFzPosB * 16;     // im2col, 1024 x 16 bf16
+constexpr uint32_t kFzSp = kFzImB + (uint32_t)kFzIm * 16 * 2;  // spins, 16 rows x 66 (+pad)
+constexpr uint32_t kFzBias = kFzSp + 16u * kFzPitch + 32;      // 4 x 32 floats
+constexpr uint32_t kFzPool = kFzBias + 4u * kC * 4;            // 32 floats
+constexpr uint32_t kFzBar = kFzPool + (uint32_t)kC * 4;        // 4 mbarriers + TMEM slot
+constexpr size_t kFzSmem = kFzBar + 64;
+static_assert(kFzSmem <= 227 * 1024, "fused kernel shared memory");
+static_assert(kFzBufA % 16 == 0 && kFzBufB % 16 == 0 && kFzImB % 16 == 0, "16-byte operands");
+
+struct FusedArgs {
+  const int8_t *spins;           // [B][4096]
+  const __nv_bfloat16 *w1;       // [32][16] (taps padded)
+  const __nv_bfloat16 *w;        // W2..W4 [3][32][288]
+  const float *params;           // biases (kOffB1.. in the flat parameter vector)
+  float *pool;                   // [B][32] channel sums of a4 (added to)
+  int *err;                      // set on a timed-out wait
+  int nbands;                    // B * (64 / kFzRows)
+};
+
+__global__ void __launch_bounds__(kFzThreads, 1) k_cnn_fused64(FusedArgs a) {
+  constexpr int L = 64, N = L * L;
+  constexpr int K = 9 * kC;       // 288
+  constexpr int SBO_W = K * 16;   // weights: bytes between 8-row groups
+  constexpr int kBands = L / kFzRows;
+  extern __shared__ __align__(1024) unsigned char smem[];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  uint64_t *bar = reinterpret_cast<uint64_t *>(smem + kFzBar);  // mma_done[2], acc_free[2]
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(smem + kFzBar + 32);
+  volatile int *abort_flag = reinterpret_cast<volatile int *>(smem + kFzBar + 40);
+  float *bias = reinterpret_cast<float *>(smem + kFzBias);
+  float *spool = reinterpret_cast<float *>(smem + kFzPool);
+  int8_t *sp = reinterpret_cast<int8_t *>(smem + kFzSp);
+  const uint32_t sbase = smem_u32(smem);
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(tslot)),
+                 "r"(64)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    mbar_init(smem_u32(&bar[0]), 1);
+    mbar_init(smem_u32(&bar[1]), 1);
+    mbar_init(smem_u32(&bar[2]), 128);
+    mbar_init(smem_u32(&bar[3]), 128);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  // weights, once per CTA: W2..W4 as k_conv_win stages them, W1 as k_conv_tc
+  for (int i = tid; i < 3 * kC * (K / 8); i += blockDim.x) {
+    const int l = i / (kC * (K / 8)), r = i % (kC * (K / 8));
+    const int n = r / (K / 8), kc = r % (K / 8);
+    cp_async16(sbase + kFzW + (uint32_t)(l * kC * K * 2) + il_off(n, kc * 8, SBO_W),
+               a.w + (size_t)l * kC * K + (size_t)n * K + kc * 8);
+  }
+  for (int i = tid; i < kC * 2; i += blockDim.x)
+    cp_async16(sbase + kFzW1 + il_off(i >> 1, (i & 1) * 8, 256), a.w1 + (i >> 1) * 16 + (i & 1) * 8);
+  for (int i = tid; i < 4 * kC; i += blockDim.x) {
+    const int l = i / kC, c = i % kC;
+    bias[i] = a.params[l == 0 ? kOffB1 + c : kOffB2 + (l - 1) * (9216 + 32) + c];
+  }
+  cp_async_wait_all();
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t taddr = *tslot;
+
+  const int grp = warp >> 2, quad = warp & 3;  // epilogue warps (warp < 8)
+  uint32_t use0 = 0, use1 = 0;                 // issuer: uses of each accumulator
+  uint32_t my_use = 0;                         // epilogue: uses of its group's accumulator
+  uint32_t seq = 0;                            // tiles issued so far (same on every thread)
+  float psum[kC];
+#pragma unroll
+  for (int c = 0; c < kC; ++c) psum[c] = 0.f;
+
+  for (int band = blockIdx.x; band < a.nbands; band += gridDim.x) {
+    const int img = band / kBands, y0 = (band % kBands) * kFzRows;
+    // spins of image rows y0-4 .. y0+11, with the wrapped ghost columns
+    const int8_t *sg = a.spins + (size_t)img * N;
+    for (int i = tid; i < 16 * kFzPitch; i += blockDim.x) {
+      const int r = i / kFzPitch, j = i - r * kFzPitch;
+      const int x = (j - 1 + L) % L, y = (y0 - 4 + r + L) % L;
+      sp[i] = sg[y * L + x];
+    }
+    if (tid < kC) spool[tid] = 0.f;
+    __syncthreads();
+    // layer-1 im2col: row q is a1 position q (local row q / 66, padded column q % 66)
+    for (int q = tid; q < kFzIm; q += blockDim.x) {
+      const int i = q / kFzPitch, j = q - i * kFzPitch;
+      __align__(16) __nv_bfloat16 v[16];
+#pragma unroll
+      for (int k = 0; k < 16; ++k) {
+        float f = 0.0f;
+        if (k < 9) {
+          const int r = min(i + 1 + k / 3 - 1, 15);
+          const int jj = min(max(j + k % 3 - 1, 0), kFzPitch - 1);
+          f = (float)sp[r * kFzPitch + jj];
+        }
+        v[k] = __float2bfloat16_rn(f);
+      }
+      *reinterpret_cast<uint4 *>(smem + kFzImB + il_off(q, 0, 256)) =
+          *reinterpret_cast<const uint4 *>(&v[0]);
+      *reinterpret_cast<uint4 *>(smem + kFzImB + il_off(q, 8, 256)) =
+          *reinterpret_cast<const uint4 *>(&v[8]);
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+
+    for (int layer = 0; layer < 4; ++layer) {
+      const int npos = (14 - 2 * layer) * kFzPitch;  // output positions of this layer
+      const int ntiles = (npos + 127) / 128;
+      // layer 1 (index 1) reads buffer A and writes B; layer 2 reads B, writes A; layer 3 reads A
+      const uint32_t in_off = layer == 2 ? kFzBufB : kFzBufA;
+      const uint32_t in_lbo = (layer == 2 ? kFzPosB : kFzPosA) * 16u;
+      const uint32_t out_off = layer == 1 ? kFzBufB : kFzBufA;
+      const uint32_t out_lbo = (layer == 1 ? kFzPosB : kFzPosA) * 16u;
+      if (warp == 8) {
+        if (lane == 0) {
+          for (int t = 0; t < ntiles; ++t) {
+            const int g = (int)((seq + (uint32_t)t) & 1u);
+            const uint32_t u = g ? use1 : use0;
+            if (u > 0 && !*abort_flag && !mbar_wait(smem_u32(&bar[2 + g]), (u - 1) & 1u))
+              *abort_flag = 1;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            if (!*abort_flag) {
+              const uint32_t d = taddr + (uint32_t)(g * 32);
+              if (layer == 0) {
+                umma_bf16(d, umma_desc(sbase + kFzImB + (uint32_t)t * 4096u, 128, 256),
+                          umma_desc(sbase + kFzW1, 128, 256), 0u);
+              } else {
+                const uint32_t wb = sbase + kFzW + (uint32_t)((layer - 1) * kC * K * 2);
+#pragma unroll
+                for (int tap = 0; tap < 9; ++tap) {
+                  const int dy = tap / 3 - 1, dx = tap % 3 - 1;
+                  const uint32_t pos = (uint32_t)(kFzLead + 128 * t + (1 + dy) * kFzPitch + dx);
+#pragma unroll
+                  for (int j = 0; j < 2; ++j)
+                    umma_bf16(d, umma_desc(sbase + in_off + 2u * j * in_lbo + pos * 16u, in_lbo, 128),
+                              umma_desc(wb + (uint32_t)(tap * 2 + j) * 256, 128, SBO_W),
+                              (tap | j) ? 1u : 0u);
+                }
+              }
+              umma_commit(smem_u32(&bar[g]));
+            }
+            if (g) ++use1; else ++use0;
+          }
+        }
+      } else {
+        for (int t = 0; t < ntiles; ++t) {
+          if ((int)((seq + (uint32_t)t) & 1u) != grp) continue;
+          if (!*abort_flag && !mbar_wait(smem_u32(&bar[grp]), my_use & 1u)) *abort_flag = 1;
+          ++my_use;
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          float acc[32];
+          tmem_ld32(taddr + ((uint32_t)(quad * 32) << 16) + (uint32_t)(grp * 32), acc);
+          asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+          // the accumulator is in registers: hand it back to the issuer now
+          asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&bar[2 + grp]))
+                       : "memory");
+          const int q = 128 * t + quad * 32 + lane;
+          const int i = q / kFzPitch, j = q - i * kFzPitch;
+          if (*abort_flag || q >= npos || j < 1 || j > L) continue;  // ghost or beyond the band
+          const float *bl = bias + layer * kC;
+          if (layer < 3) {
+            __align__(16) __nv_bfloat16 o[32];
+#pragma unroll
+            for (int c = 0; c < 32; ++c) {
+              const float z = acc[c] + bl[c];
+              o[c] = __float2bfloat16_rn(z > 0.0f ? z : 0.0f);
+            }
+            const uint32_t p0 = (uint32_t)(kFzLead + q) * 16u;
+            const uint32_t pg = (uint32_t)(kFzLead + i * kFzPitch + (j == 1 ? L + 1 : 0)) * 16u;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+              const uint4 val = reinterpret_cast<const uint4 *>(o)[c];
+              *reinterpret_cast<uint4 *>(smem + out_off + c * out_lbo + p0) = val;
+              if (j == 1 || j == L) *reinterpret_cast<uint4 *>(smem + out_off + c * out_lbo + pg) = val;
+            }
+          } else {
+#pragma unroll
+            for (int c = 0; c < 32; ++c) {
+              const float z = acc[c] + bl[c];
+              psum[c] += __bfloat162float(__float2bfloat16_rn(z > 0.0f ? z : 0.0f));
+            }
+          }
+        }
+      }
+      seq += (uint32_t)ntiles;
+      // the layer's outputs, to the tensor cores' (async) view, before the next layer
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncthreads();
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    }
+    // pooled sums of the band: warp reduce, then shared, then one atomicAdd per channel
+    if (warp < 8) {
+#pragma unroll
+      for (int c = 0; c < kC; ++c) {
+        float v = psum[c];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) atomicAdd(&spool[c], v);
+        psum[c] = 0.f;
+      }
+    }
+    __syncthreads();
+    if (tid < kC && !*abort_flag) atomicAdd(&a.pool[img * kC + tid], spool[tid]);
+  }
+  if (tid == 0 && *abort_flag && a.err) atomicExch(a.err, 1);
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(64)
+                 : "memory");
+  }
+}
+
 size_t conv_win_smem(int L, bool pool) {
   const size_t W = (size_t)kTileM + 2 * (size_t)L;
   return 3 * 4 * W * 16 + (size_t)kC * 9 * kC * 2 + 64 + (pool ? (size_t)kTileM * 33 * 4 : 0);
@@ -986,6 +1238,7 @@ struct gasp_cnn {
   __nv_bfloat16 *d_dz[2];   // ping-pong data gradients
   int *d_err;
   int adam_t;
+  int fused;  // inference through k_cnn_fused64 (L = 64); gasp_cnn_set_fused
 };
 
 namespace {
@@ -1096,6 +1349,32 @@ int cnn_forward(gasp_cnn *c, int batch, cudaStream_t s, const int8_t *spins = nu
   return GASP_OK;
 }
 
+// Inference forward (pooled sums in d_pool): the fused whole-network kernel
+// for L = 64 unless switched off, the layer-by-layer kernels otherwise.
+int cnn_infer(gasp_cnn *c, int batch, cudaStream_t s, const int8_t *spins = nullptr) {
+  if (c->L != 64 || !c->fused) return cnn_forward(c, batch, s, spins);
+  k_pack_weights<<<(3 * 9216 + 255) / 256, 256, 0, s>>>(c->d_params, c->d_w1, c->d_w, c->d_wt);
+  GASP_CUDA(cudaGetLastError());
+  GASP_CUDA(cudaMemsetAsync(c->d_pool, 0, (size_t)batch * kC * sizeof(float), s));
+  FusedArgs f;
+  f.spins = spins ? spins : c->d_spins;
+  f.w1 = c->d_w1;
+  f.w = c->d_w;
+  f.params = c->d_params;
+  f.pool = c->d_pool;
+  f.err = c->d_err;
+  f.nbands = batch * (64 / kFzRows);
+  GASP_CUDA(cudaFuncSetAttribute(k_cnn_fused64, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kFzSmem));
+  int dev = 0, nsm = 0;
+  GASP_CUDA(cudaGetDevice(&dev));
+  GASP_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  const int grid = f.nbands < nsm ? f.nbands : nsm;  // one CTA per SM, persistent
+  k_cnn_fused64<<<grid, kFzThreads, kFzSmem, s>>>(f);
+  GASP_CUDA(cudaGetLastError());
+  return GASP_OK;
+}
+
 int cnn_check_err(gasp_cnn *c, cudaStream_t s) {
   int err = 0;
   GASP_CUDA(cudaMemcpyAsync(&err, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -1149,7 +1428,7 @@ int predict_chunked(gasp_cnn *c, const int8_t *spins, int batch, float *q_out, f
   for (int i = 0; i < nch; ++i) {
     const int b = i & 1, n = rows(i);
     GASP_CUDA(cudaStreamWaitEvent(s, c->ev_copied[b], 0));
-    if ((rc = cnn_forward(c, n, s, buf[b]))) return rc;
+    if ((rc = cnn_infer(c, n, s, buf[b]))) return rc;
     k_head<<<(n + 7) / 8, 256, 0, s>>>(n, c->N, c->d_pool, c->d_params, nullptr, c->d_q, nullptr,
                                        nullptr, nullptr);
     GASP_CUDA(cudaGetLastError());
@@ -1252,6 +1531,7 @@ int gasp_cnn_create(int L, int max_batch, gasp_cnn_t **out) {
   c->L = L;
   c->N = L * L;
   c->max_batch = max_batch;
+  c->fused = 1;
   const size_t act = (size_t)max_batch * c->N * kC * sizeof(__nv_bfloat16);
   cudaError_t e = cudaSuccess;
   auto A = [&](void **p, size_t n) {
@@ -1326,7 +1606,7 @@ int gasp_cnn_predict_ex(gasp_cnn_t *c, const int8_t *spins, int batch, float *q_
   int rc;
   if (batch > c->max_batch) return predict_chunked(c, spins, batch, q_out, mag_out, s);
   if ((rc = cnn_upload(c, spins, nullptr, batch))) return rc;
-  if ((rc = cnn_forward(c, batch, s))) return rc;
+  if ((rc = cnn_infer(c, batch, s))) return rc;
   k_head<<<(batch + 7) / 8, 256, 0, s>>>(batch, c->N, c->d_pool, c->d_params, nullptr, c->d_q,
                                          nullptr, nullptr, nullptr);
   GASP_CUDA(cudaGetLastError());
@@ -1342,6 +1622,12 @@ int gasp_cnn_predict_ex(gasp_cnn_t *c, const int8_t *spins, int batch, float *q_
 
 int gasp_cnn_predict(gasp_cnn_t *c, const int8_t *spins, int batch, float *q_out) {
   return gasp_cnn_predict_ex(c, spins, batch, q_out, nullptr);
+}
+
+int gasp_cnn_set_fused(gasp_cnn_t *c, int on) {
+  if (!c) return GASP_ERR_INVALID;
+  c->fused = on != 0;
+  return GASP_OK;
 }
 
 int gasp_cnn_gradients(gasp_cnn_t *c, const int8_t *spins, const float *labels, int batch,

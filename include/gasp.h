@@ -393,6 +393,12 @@ int gasp_cnn_predict(gasp_cnn_t *cnn, const int8_t *spins, int batch, float *q_o
  * allocates a second input buffer and a copy stream). */
 int gasp_cnn_predict_ex(gasp_cnn_t *cnn, const int8_t *spins, int batch, float *q_out,
                         float *mag_out);
+/* Prediction path for L = 64: on (the default) the whole network runs as one
+ * kernel per band of 8 rows with the activations kept on the chip; off, layer
+ * by layer through HBM as training does.  Same arithmetic either way (BF16
+ * activations, FP32 accumulation); only the order of the pooled FP32 sums
+ * differs.  Other L always run layer by layer. */
+int gasp_cnn_set_fused(gasp_cnn_t *cnn, int on);
 /* Loss (mean over the batch) and its gradient for labels in [0, 1]. */
 int gasp_cnn_gradients(gasp_cnn_t *cnn, const int8_t *spins, const float *labels, int batch,
                        float *loss_out, float *grad_out);

@@ -113,3 +113,30 @@ def test_predict_returns_magnetisation_and_screen_shoots_out_of_window_grids():
                                    window=(-0.93, -0.65), seed=4)
     assert shot.tolist() == [False, False, True, True]
     assert pb[2] == 1.0 and pb[3] == 0.0  # all up is in B, all down in A at once
+
+
+def test_fused_forward_matches_layer_by_layer_and_oracle():
+    """The whole-network kernel of the L=64 prediction path (one band of 8
+    rows per work item, activations on the chip, ghost columns for the wrap)
+    against the layer-by-layer kernels and the FP64 oracle with the same BF16
+    rounding points; biases and head non-zero.  37 grids in a 16-grid handle:
+    the chunked path with a ragged last chunk."""
+    from gpu_2dising_b200._native import check, lib
+    rs = np.random.default_rng(11)
+    f = rs.uniform(0.05, 0.95, size=37)
+    g = np.where(rs.random((37, L, L)) < f[:, None, None], 1, -1).astype(np.int8)
+    params = surrogate.init_params(13)
+    params[288:320] = rs.normal(0, 0.3, 32)                    # layer-1 bias
+    for l in range(3):                                          # layer 2-4 biases
+        o = 320 + 9216 + l * (9216 + 32)
+        params[o:o + 32] = rs.normal(0, 0.2, 32)
+    params[-33:] = rs.normal(0, 0.5, 33).astype(np.float32)
+    net = surrogate.CommittorCNN(L, 16, params)
+    q_fused = net.predict(g)
+    check(lib().gasp_cnn_set_fused(net._h, 0))
+    q_layers = net.predict(g)
+    check(lib().gasp_cnn_set_fused(net._h, 1))
+    assert np.max(np.abs(q_fused - q_layers)) < 2e-5, np.max(np.abs(q_fused - q_layers))
+    ref = ocnn.forward(params.astype(np.float64), g[:6].astype(np.float64), bf16=True)["q"]
+    assert np.max(np.abs(q_fused[:6] - ref)) < 2e-3, (q_fused[:6], ref)
+    assert np.max(np.abs(net.predict(g[:5]) - q_fused[:5])) < 2e-5  # one unchunked batch
