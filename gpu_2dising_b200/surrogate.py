@@ -98,8 +98,8 @@ class CommittorCNN:
 
     def train(self, grids, labels, epochs=20, batch=256, lr=2e-3, seed=0, augment=True,
               val=None, log=None):
-        """Mini-batch Adam.  augment: random lattice translations and the
-        8 square symmetries (the Hamiltonian's), which leave pB unchanged."""
+        """Mini-batch Adam.  augment: the 8 square symmetries (the
+        Hamiltonian's), which leave pB unchanged."""
         g = self._spins(grids)
         y = np.asarray(labels, np.float32)
         rs = np.random.default_rng(seed)
@@ -134,15 +134,21 @@ class CommittorCNN:
 
 
 def _augment(xb, rs):
+    """Each grid of the batch under one of the 8 symmetries of the square
+    (k quarter turns, then an optional flip), drawn per grid; the grids of
+    each symmetry are transformed together.  Circular translations are not
+    drawn: with circular padding and a global average pool the network's
+    output does not depend on them."""
     out = np.empty_like(xb)
-    L = xb.shape[1]
-    for i in range(xb.shape[0]):
-        x = np.roll(xb[i], (int(rs.integers(L)), int(rs.integers(L))), axis=(0, 1))
-        k = int(rs.integers(4))
-        x = np.rot90(x, k)
-        if rs.integers(2):
-            x = x[:, ::-1]
-        out[i] = x
+    sym = rs.integers(8, size=xb.shape[0])
+    for s_ in range(8):
+        idx = np.nonzero(sym == s_)[0]
+        if idx.size == 0:
+            continue
+        x = np.rot90(xb[idx], s_ & 3, axes=(1, 2))
+        if s_ >= 4:
+            x = x[:, :, ::-1]
+        out[idx] = x
     return out
 
 
