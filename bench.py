@@ -816,12 +816,14 @@ def surrogate_measure(args):
     from gpu_2dising_b200 import engine, surrogate
     engine.init_device(0)
     res = surrogate.run_experiment(n_train=args.surrogate_train, n_test=args.surrogate_test,
-                                   n_screen=args.surrogate_screen, epochs=args.surrogate_epochs)
+                                   n_screen=args.surrogate_screen, epochs=args.surrogate_epochs,
+                                   focus=args.surrogate_focus)
     hist = res.pop("history")
     line = {"metric": "committor evaluations/s, surrogate-screened vs shooting alone",
             "value": res["screen_grids_per_s"], "unit": "grids/s", "n_gpus": 1,
             "speedup_vs_shooting": res["speedup"], **res,
             "val_mae_by_epoch": [round(h["val_mae"], 4) for h in hist],
+            "epochs": args.surrogate_epochs, "focus": args.surrogate_focus,
             "config": {"workload": f"{res['n_train']} L=64 swarm snapshots (beta=0.54, h=0.07, "
                                    "m in (-0.93,-0.65)) labelled by 256-shot pB, "
                                    f"{res['n_test']} held out with 1024-shot pB, "
@@ -928,6 +930,8 @@ def main(argv=None):
     ap.add_argument("--surrogate-test", type=int, default=2000)
     ap.add_argument("--surrogate-screen", type=int, default=100000)
     ap.add_argument("--surrogate-epochs", type=int, default=40)
+    ap.add_argument("--surrogate-focus", type=float, default=0.0,
+                    help="training draws grids with weight 1 + focus*4y(1-y)")
     ap.add_argument("--batched-sweeps", type=int, default=1000)
     ap.add_argument("--rng", default="xorwow", choices=["xorwow", "mwc64x"],
                     help="xorwow: the reference stream (bit-exact); mwc64x: production stream")

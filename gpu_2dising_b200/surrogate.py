@@ -97,15 +97,20 @@ class CommittorCNN:
         return float(loss.value)
 
     def train(self, grids, labels, epochs=20, batch=256, lr=2e-3, seed=0, augment=True,
-              val=None, log=None):
+              val=None, log=None, focus=0.0):
         """Mini-batch Adam.  augment: the 8 square symmetries (the
-        Hamiltonian's), which leave pB unchanged."""
+        Hamiltonian's), which leave pB unchanged.  focus > 0: each epoch draws
+        its grids (with replacement) with weights 1 + focus * 4 y (1 - y), so
+        grids with pB near 0.5 are seen more often than committed ones."""
         g = self._spins(grids)
         y = np.asarray(labels, np.float32)
         rs = np.random.default_rng(seed)
+        w = 1.0 + focus * 4.0 * y.astype(np.float64) * (1.0 - y)
+        w /= w.sum()
         hist = []
         for ep in range(epochs):
-            order = rs.permutation(g.shape[0])
+            order = (rs.permutation(g.shape[0]) if focus <= 0.0 else
+                     rs.choice(g.shape[0], size=g.shape[0], p=w))
             losses = []
             for i in range(0, g.shape[0] - batch + 1, batch):
                 idx = order[i:i + batch]
@@ -251,7 +256,7 @@ def screen(cnn, grids, beta, h, fallback_shots=128, band=0.1, window=None, **sho
 
 def run_experiment(n_train=20000, train_shots=256, n_test=2000, test_shots=1024,
                    n_screen=100000, baseline_shots=64, epochs=40, batch=1024, lr=2e-3, beta=0.54,
-                   h=0.07, seed=0, log=None):
+                   h=0.07, seed=0, log=None, focus=0.0):
     """Train the surrogate on shooting labels and measure what it gains.
 
     Returns a dict with the held-out MAE (surrogate alone and screened with
@@ -273,7 +278,7 @@ def run_experiment(n_train=20000, train_shots=256, n_test=2000, test_shots=1024,
     net = CommittorCNN(64, batch, init_params(seed))
     t0 = time.perf_counter()
     hist = net.train(tr, y_tr, epochs=epochs, batch=batch, lr=lr, seed=seed,
-                     val=(te, y_te), log=log)
+                     val=(te, y_te), log=log, focus=focus)
     t["train_s"] = time.perf_counter() - t0
     pred_te = net.predict(te).astype(np.float64)
     mae_surrogate = float(np.mean(np.abs(pred_te - y_te)))
