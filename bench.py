@@ -651,6 +651,9 @@ def cnn_measure(args):
     grids = np.where(rs.random((n, L, L)) < 0.1, 1, -1).astype(np.int8)
     labels = rs.random(1024).astype(np.float32)
     net = surrogate.CommittorCNN(L, 1024, surrogate.init_params(0))
+    if args.cnn_fused:  # the whole-network kernel for prediction (L = 64)
+        from gpu_2dising_b200._native import check, lib
+        check(lib().gasp_cnn_set_fused(net._h, 1))
     for _ in range(args.warmup):
         net.predict(grids[:2048])
     t0 = time.perf_counter()
@@ -670,7 +673,9 @@ def cnn_measure(args):
             "effective_tflops": flop * n / pred_s / 1e12,
             "train_step_ms_batch1024": 1e3 * step_s,
             "config": {"workload": f"predict on {n} int8 L=64 grids (host memory, batches of "
-                                   "1024); 4x conv3x3(32) tcgen05, pool, 32->1"}}
+                                   "1024); 4x conv3x3(32) tcgen05, pool, 32->1",
+                       "prediction_kernels": "fused whole network" if args.cnn_fused
+                       else "layer by layer"}}
     net.close()
     return line
 
@@ -915,6 +920,8 @@ def main(argv=None):
                     help="swarm: the headline single-group swarm; batched: uneven groups; "
                          "committor: seeded droplet shooting")
     ap.add_argument("--cnn-grids", type=int, default=100000)
+    ap.add_argument("--cnn-fused", action="store_true",
+                    help="cnn workload: predict through the fused whole-network kernel")
     ap.add_argument("--rate-sweeps", type=int, default=50000)
     ap.add_argument("--tail-replicas", type=int, default=0,
                     help="tail workload: one replica count (default: a range)")

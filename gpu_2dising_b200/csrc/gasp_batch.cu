@@ -604,8 +604,10 @@ int gasp_batch_autotune(gasp_batch_t *b, int nsweeps, int *choice_out) {
     }
   }
   // Layout of the interval graph: one kernel per group (concurrent branches)
-  // or every group in one persistent launch.  Each is timed on three interval
-  // replays of nsweeps sweeps in which no replica finishes (up = 2).
+  // or every group in one persistent launch.  Each is timed on intervals of
+  // max(nsweeps, 20) sweeps in which no replica finishes (up = 2), at three
+  // live fractions of every group (all, half, 15 %: a swarm's intervals run
+  // with more and more of each group compacted out), two intervals each.
   b->layout = 0;
   b->layout_ms[0] = b->layout_ms[1] = -1.f;
   if (rc == GASP_OK && b->exec) {  // kernel choices changed: recapture
@@ -613,14 +615,29 @@ int gasp_batch_autotune(gasp_batch_t *b, int nsweeps, int *choice_out) {
     b->exec = nullptr;
   }
   if (rc == GASP_OK && multi_possible(b)) {
+    const double fracs[3] = {1.0, 0.5, 0.15};
+    std::vector<int> small((size_t)2 * b->ngroups, 0);
     for (int layout = 0; layout < 2 && rc == GASP_OK; ++layout) {
-      if ((rc = batch_build_graph(b, s, nsweeps, 2.0, layout))) break;
+      if ((rc = batch_build_graph(b, s, nsweeps > 20 ? nsweeps : 20, 2.0, layout))) break;
       GASP_CUDA(cudaGraphLaunch(b->exec, s));  // warm-up replay
-      GASP_CUDA(cudaEventRecord(e0, s));
-      for (int i = 0; i < 3; ++i) GASP_CUDA(cudaGraphLaunch(b->exec, s));
-      GASP_CUDA(cudaEventRecord(e1, s));
-      GASP_CUDA(cudaEventSynchronize(e1));
-      GASP_CUDA(cudaEventElapsedTime(&b->layout_ms[layout], e0, e1));
+      float total = 0.f;
+      for (double f : fracs) {
+        for (int g = 0; g < b->ngroups; ++g) {
+          const int n = (int)(f * b->groups[g].ngrids);
+          small[(size_t)2 * g] = n > 1 ? n : 1;  // live count; the active list is 0..n-1
+          small[(size_t)2 * g + 1] = 0;
+        }
+        GASP_CUDA(cudaMemcpyAsync(b->d_small, small.data(), small.size() * sizeof(int),
+                                  cudaMemcpyHostToDevice, s));
+        GASP_CUDA(cudaEventRecord(e0, s));
+        for (int i = 0; i < 2; ++i) GASP_CUDA(cudaGraphLaunch(b->exec, s));
+        GASP_CUDA(cudaEventRecord(e1, s));
+        GASP_CUDA(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        GASP_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        total += ms;
+      }
+      b->layout_ms[layout] = total;
     }
     if (rc == GASP_OK && b->layout_ms[1] < b->layout_ms[0]) b->layout = 1;
   }

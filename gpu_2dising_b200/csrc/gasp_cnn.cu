@@ -568,8 +568,8 @@ __global__ void __launch_bounds__(kFzThreads, 1) k_cnn_fused64(FusedArgs a) {
   if (tid == 0) {
     mbar_init(smem_u32(&bar[0]), 1);
     mbar_init(smem_u32(&bar[1]), 1);
-    mbar_init(smem_u32(&bar[2]), 128);
-    mbar_init(smem_u32(&bar[3]), 128);
+    mbar_init(smem_u32(&bar[2]), 4);  // one arrival per epilogue warp
+    mbar_init(smem_u32(&bar[3]), 4);
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -658,16 +658,21 @@ __global__ void __launch_bounds__(kFzThreads, 1) k_cnn_fused64(FusedArgs a) {
                 umma_bf16(d, umma_desc(sbase + kFzImB + (uint32_t)t * 4096u, 128, 256),
                           umma_desc(sbase + kFzW1, 128, 256), 0u);
               } else {
-                const uint32_t wb = sbase + kFzW + (uint32_t)((layer - 1) * kC * K * 2);
+                // descriptors differ only in their start address (bits 0-13,
+                // in 16-byte units): one base each, offsets added per MMA
+                const uint64_t da0 =
+                    umma_desc(sbase + in_off + (uint32_t)(kFzLead + 128 * t) * 16u, in_lbo, 128);
+                const uint64_t db0 =
+                    umma_desc(sbase + kFzW + (uint32_t)((layer - 1) * kC * K * 2), 128, SBO_W);
+                const uint32_t lbo16 = in_lbo >> 4;
 #pragma unroll
                 for (int tap = 0; tap < 9; ++tap) {
                   const int dy = tap / 3 - 1, dx = tap % 3 - 1;
-                  const uint32_t pos = (uint32_t)(kFzLead + 128 * t + (1 + dy) * kFzPitch + dx);
+                  const int pos = (1 + dy) * kFzPitch + dx;  // >= -1, base is kFzLead in
 #pragma unroll
                   for (int j = 0; j < 2; ++j)
-                    umma_bf16(d, umma_desc(sbase + in_off + 2u * j * in_lbo + pos * 16u, in_lbo, 128),
-                              umma_desc(wb + (uint32_t)(tap * 2 + j) * 256, 128, SBO_W),
-                              (tap | j) ? 1u : 0u);
+                    umma_bf16(d, da0 + (uint64_t)(int64_t)(pos + (int)(2u * j * lbo16)),
+                              db0 + (uint64_t)((tap * 2 + j) * 16), (tap | j) ? 1u : 0u);
                 }
               }
               umma_commit(smem_u32(&bar[g]));
@@ -678,15 +683,22 @@ __global__ void __launch_bounds__(kFzThreads, 1) k_cnn_fused64(FusedArgs a) {
       } else {
         for (int t = 0; t < ntiles; ++t) {
           if ((int)((seq + (uint32_t)t) & 1u) != grp) continue;
-          if (!*abort_flag && !mbar_wait(smem_u32(&bar[grp]), my_use & 1u)) *abort_flag = 1;
+          // one lane polls the MMA barrier (32 x 8 spinning lanes would keep
+          // the shared-memory pipe busy); the warp barrier passes it on
+          if (lane == 0 && !*abort_flag && !mbar_wait(smem_u32(&bar[grp]), my_use & 1u))
+            *abort_flag = 1;
+          __syncwarp();
           ++my_use;
           asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
           float acc[32];
           tmem_ld32(taddr + ((uint32_t)(quad * 32) << 16) + (uint32_t)(grp * 32), acc);
           asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+          __syncwarp();
           // the accumulator is in registers: hand it back to the issuer now
-          asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&bar[2 + grp]))
-                       : "memory");
+          if (lane == 0)
+            asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(
+                             smem_u32(&bar[2 + grp]))
+                         : "memory");
           const int q = 128 * t + quad * 32 + lane;
           const int i = q / kFzPitch, j = q - i * kFzPitch;
           if (*abort_flag || q >= npos || j < 1 || j > L) continue;  // ghost or beyond the band
@@ -1238,7 +1250,7 @@ struct gasp_cnn {
   __nv_bfloat16 *d_dz[2];   // ping-pong data gradients
   int *d_err;
   int adam_t;
-  int fused;  // inference through k_cnn_fused64 (L = 64); gasp_cnn_set_fused
+  int fused;  // inference through k_cnn_fused64 (L = 64); gasp_cnn_set_fused, default off
 };
 
 namespace {
@@ -1350,7 +1362,7 @@ int cnn_forward(gasp_cnn *c, int batch, cudaStream_t s, const int8_t *spins = nu
 }
 
 // Inference forward (pooled sums in d_pool): the fused whole-network kernel
-// for L = 64 unless switched off, the layer-by-layer kernels otherwise.
+// for L = 64 when switched on, the layer-by-layer kernels otherwise.
 int cnn_infer(gasp_cnn *c, int batch, cudaStream_t s, const int8_t *spins = nullptr) {
   if (c->L != 64 || !c->fused) return cnn_forward(c, batch, s, spins);
   k_pack_weights<<<(3 * 9216 + 255) / 256, 256, 0, s>>>(c->d_params, c->d_w1, c->d_w, c->d_wt);
@@ -1531,7 +1543,7 @@ int gasp_cnn_create(int L, int max_batch, gasp_cnn_t **out) {
   c->L = L;
   c->N = L * L;
   c->max_batch = max_batch;
-  c->fused = 1;
+  c->fused = 0;  // the layer-by-layer path measured faster (1.0M vs 0.62M grids/s)
   const size_t act = (size_t)max_batch * c->N * kC * sizeof(__nv_bfloat16);
   cudaError_t e = cudaSuccess;
   auto A = [&](void **p, size_t n) {

@@ -363,15 +363,14 @@ struct LatticeStore<Words, false> {
   __device__ __forceinline__ static uint32_t *get(uint32_t *dyn) { return dyn; }
 };
 
-// The lattice step of one row-kernel attempt: site s, raw acceptance draw
-// x2.  Reads the site's row word(s) and the words above and below, forms the
-// 5-spin pattern, compares x2 with the pattern's threshold and writes the
-// site's word back (flipped on acceptance; kStoreAlways: unchanged otherwise,
-// else only on acceptance).  kKind picks the row-window form measured faster
-// with that stream.
-template <int L, bool kFloatCmp, bool kStoreAlways, int kKind>
-__device__ __forceinline__ void row_apply(uint32_t s, uint32_t x2, const char *latb,
-                                          const char *thrb, const char *paccb, uint32_t lane4) {
+// One attempt of k_sweep_rows on site s.  kLookahead: also draw the next
+// attempt's site (after this attempt's acceptance draw, as the reference's
+// stream order requires) so its conversion overlaps this attempt's
+// shared-memory round trips.
+template <int L, bool kFloatCmp, bool kLookahead, bool kStoreAlways, typename Rng>
+__device__ __forceinline__ void row_attempt(uint32_t &s, Rng &rg, const char *latb,
+                                            const char *thrb, const char *paccb, uint32_t lane4,
+                                            float shrink) {
   constexpr int N = L * L;
   constexpr int R = L / 32;
   constexpr bool kPow2 = (L & (L - 1)) == 0;
@@ -396,7 +395,7 @@ __device__ __forceinline__ void row_apply(uint32_t s, uint32_t x2, const char *l
   } else if constexpr (R == 2) {
     wc = *reinterpret_cast<const uint32_t *>(latb + offc);
     const uint32_t wx = *reinterpret_cast<const uint32_t *>(latb + (offc ^ 128u));
-    if constexpr (kKind == kRngXorwow) {
+    if constexpr (Rng::kKind == kRngXorwow) {
       // The row is the circular 64 bits (wx:wc) seen from the site's word: for
       // b >= 3 the bits b-1..b+1 sit in (wx:wc) >> (b-3) (b = 31 reaches wx
       // bit 0); for b < 3 the left neighbour wraps to the top of wx, so the
@@ -423,7 +422,9 @@ __device__ __forceinline__ void row_apply(uint32_t s, uint32_t x2, const char *l
   const uint32_t u = __funnelshift_r(wu, wu, b + 27u);  // bit 5: up
   const uint32_t d = __funnelshift_r(wd, wd, b + 26u);  // bit 6: down
   const uint32_t p4 = (t & 0x1Cu) | (u & 0x20u) | (d & 0x40u);
+  const uint32_t x2 = rg.next();
   const uint32_t sc = s;
+  if constexpr (kLookahead) s = rg.template site<N>(shrink, N);
   bool acc;
   if constexpr (kFloatCmp) {
     acc = _curand_uniform(x2) < *reinterpret_cast<const float *>(paccb + p4);
@@ -436,21 +437,6 @@ __device__ __forceinline__ void row_apply(uint32_t s, uint32_t x2, const char *l
   } else {
     if (acc) *dst = wc ^ (1u << (sc & 31u));
   }
-}
-
-
-// One attempt of k_sweep_rows on site s: the acceptance draw, then (kLookahead)
-// the next attempt's site -- the reference's stream order -- so its
-// conversion overlaps this attempt's shared-memory round trips.
-template <int L, bool kFloatCmp, bool kLookahead, bool kStoreAlways, typename Rng>
-__device__ __forceinline__ void row_attempt(uint32_t &s, Rng &rg, const char *latb,
-                                            const char *thrb, const char *paccb, uint32_t lane4,
-                                            float shrink) {
-  constexpr int N = L * L;
-  const uint32_t x2 = rg.next();
-  const uint32_t sc = s;
-  if constexpr (kLookahead) s = rg.template site<N>(shrink, N);
-  row_apply<L, kFloatCmp, kStoreAlways, Rng::kKind>(sc, x2, latb, thrb, paccb, lane4);
 }
 
 // Threshold and float tables of the row kernels, indexed by the 5-spin
@@ -547,127 +533,6 @@ __global__ void __launch_bounds__(32) k_sweep_rows(SweepLaunch p) {
     else
       stage_out(lat, p, W, tile, lane, live, rep);
   } else {
-    stage_out(lat, p, W, tile, lane, live, rep);
-  }
-}
-
-// ---------------------------------------------------------------------------
-// Warp-specialised row kernel (sweep variant 10): two warps per tile of 32
-// replicas.  Warp 0 draws every attempt's site and acceptance value in the
-// replica's own stream order (site x1(a), acceptance x2(a), x1(a+1), ...) and
-// queues them in shared memory, kWsChunk attempts per lane per slot, two
-// slots; warp 1 runs the lattice steps (row_apply).  The lattice chain holds
-// no RNG work, and each scheduler gets twice the warps to issue from.  Slot
-// hand-over on mbarriers (32 arrivals, one per lane) with bounded waits: on
-// expiry g_stage_timeout is set and both warps stop.  Same draws, same
-// arithmetic, same result as k_sweep_rows.
-// ---------------------------------------------------------------------------
-constexpr int kWsChunk = 16;
-constexpr int kWsSlots = 2;
-
-__device__ __forceinline__ void ws_arrive(uint64_t *bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(
-                   (uint32_t)__cvta_generic_to_shared(bar))
-               : "memory");
-}
-
-__device__ __forceinline__ bool ws_wait(uint64_t *bar, uint32_t parity) {
-  const uint32_t b = (uint32_t)__cvta_generic_to_shared(bar);
-  for (int i = 0; i < kStagePolls; ++i) {
-    uint32_t done;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-        " selp.u32 %0, 1, 0, p;\n}"
-        : "=r"(done)
-        : "r"(b), "r"(parity)
-        : "memory");
-    if (done) return true;
-  }
-  return false;
-}
-
-template <int L, bool kStatic, bool kFloatCmp, int kRng>
-__global__ void __launch_bounds__(64) k_sweep_ws(SweepLaunch p) {
-  static_assert(L % 32 == 0, "rows of whole words");
-  constexpr int N = L * L;
-  constexpr int W = N / 32;
-  static_assert(N % kWsChunk == 0, "a batch is a whole number of chunks");
-  __shared__ __align__(16) uint32_t thrP[32];
-  __shared__ __align__(16) float paccP[32];
-  __shared__ __align__(16) uint2 q[kWsSlots][kWsChunk][kTile];  // (site, acceptance draw)
-  __shared__ __align__(8) uint64_t full[kWsSlots], empty[kWsSlots];
-  extern __shared__ __align__(16) uint32_t dyn[];
-  uint32_t *lat = LatticeStore<W * kTile, kStatic>::get(dyn);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (warp == 0) pattern_tables(p, thrP, paccP, lane);
-  if (threadIdx.x == 0) {
-    for (int i = 0; i < kWsSlots; ++i) {
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], 32;" ::"r"(
-                       (uint32_t)__cvta_generic_to_shared(&full[i]))
-                   : "memory");
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], 32;" ::"r"(
-                       (uint32_t)__cvta_generic_to_shared(&empty[i]))
-                   : "memory");
-    }
-  }
-  const int n_act = live_count(p);
-  const int tile = blockIdx.x;
-  if (tile * kTile >= n_act) return;  // whole CTA idle this batch
-  const int slot = tile * kTile + lane;
-  const bool live = slot < n_act;
-  const int rep = live ? (p.active ? p.active[slot] : slot) : 0;
-  if (warp == 1) stage_in(lat, p, W, tile, lane, live, rep);
-  __syncthreads();
-  const int nch = N / kWsChunk * p.nsweeps;
-  bool ok = true;
-  if (warp == 0) {  // producer
-    RngPolicy<kRng> rg;
-    if (live) rg.load(p.rng, p.rng_stride, rep);
-    const float shrink = (1.0f - FLT_EPSILON) * (float)N;
-    for (int k = 0; k < nch; ++k) {
-      const int sl = k % kWsSlots;
-      if (k >= kWsSlots && !ws_wait(&empty[sl], (uint32_t)((k / kWsSlots) - 1) & 1u)) {
-        ok = false;
-        break;
-      }
-      if (live) {
-#pragma unroll
-        for (int i = 0; i < kWsChunk; ++i) {
-          const uint32_t site = rg.template site<N>(shrink, N);
-          const uint32_t x2 = rg.next();
-          q[sl][i][lane] = make_uint2(site, x2);
-        }
-      }
-      ws_arrive(&full[sl]);
-    }
-    if (live && ok) rg.store(p.rng, p.rng_stride, rep);
-  } else {  // consumer: the lattice chain
-    const char *latb = reinterpret_cast<const char *>(lat);
-    const char *thrb = reinterpret_cast<const char *>(thrP);
-    const char *paccb = reinterpret_cast<const char *>(paccP);
-    const uint32_t lane4 = (uint32_t)lane << 2;
-    for (int k = 0; k < nch; ++k) {
-      const int sl = k % kWsSlots;
-      if (!ws_wait(&full[sl], (uint32_t)(k / kWsSlots) & 1u)) {
-        ok = false;
-        break;
-      }
-      uint2 e[kWsChunk];
-#pragma unroll
-      for (int i = 0; i < kWsChunk; ++i) e[i] = q[sl][i][lane];
-      ws_arrive(&empty[sl]);
-      if (live) {
-#pragma unroll
-        for (int i = 0; i < kWsChunk; ++i)
-          row_apply<L, kFloatCmp, true, kRng>(e[i].x, e[i].y, latb, thrb, paccb, lane4);
-      }
-    }
-  }
-  if (!ok && lane == 0) atomicOr(&g_stage_timeout, 1);
-  const bool all_ok = __syncthreads_and(ok ? 1 : 0) != 0;
-  if (!all_ok) return;  // flagged; the tile is not written back
-  if (warp == 1) {
-    epilogue_mag(lat + lane, p, N, W, live, rep);
     stage_out(lat, p, W, tile, lane, live, rep);
   }
 }
@@ -912,18 +777,6 @@ int launch_rows(Kern kern, const SweepLaunch &p, size_t dyn_smem, cudaStream_t s
   return GASP_OK;
 }
 
-// Two warps (producer, consumer) per tile.
-template <typename Kern>
-int launch_ws(Kern kern, const SweepLaunch &p, size_t dyn_smem, cudaStream_t s) {
-  const int tiles = tiles_for(p.n_active);
-  if (tiles == 0) return GASP_OK;
-  if (dyn_smem > 0)
-    GASP_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_smem));
-  kern<<<tiles, 64, dyn_smem, s>>>(p);
-  GASP_CUDA(cudaGetLastError());
-  return GASP_OK;
-}
-
 template <bool F, int K>
 int dispatch_kind(const SweepLaunch &p, cudaStream_t s) {
   if (p.lattice_in_global) {
@@ -939,15 +792,6 @@ int dispatch_kind(const SweepLaunch &p, cudaStream_t s) {
   }
   const size_t dyn128 = (size_t)words_per_replica(128) * kTile * sizeof(uint32_t);
   const size_t dyn96 = (size_t)words_per_replica(96) * kTile * sizeof(uint32_t);
-  if (p.variant == 10) {  // warp-specialised row kernel (draws in one warp, lattice in the other)
-    switch (p.L) {
-      case 32: return launch_ws(k_sweep_ws<32, true, F, K>, p, 0, s);
-      case 64: return launch_ws(k_sweep_ws<64, true, F, K>, p, 0, s);
-      case 96: return launch_ws(k_sweep_ws<96, false, F, K>, p, dyn96, s);
-      case 128: return launch_ws(k_sweep_ws<128, false, F, K>, p, dyn128, s);
-      default: break;  // other L: the default kernels
-    }
-  }
   if (p.variant == 9) {  // variant 0 with bulk-copy staging of the tiles (measured slower)
     switch (p.L) {
       case 32: return launch_rows(k_sweep_rows<32, true, F, K, true, true>, p, 0, s);
@@ -1024,7 +868,7 @@ int launch_sweep_exact(const SweepLaunch &p, cudaStream_t s) {
     const int rc = p.float_compare ? dispatch_exact<true>(q, s) : dispatch_exact<false>(q, s);
     if (rc) return rc;
   }
-  if (p.variant == 9 || p.variant == 10) {  // report a timed-out wait (not while capturing)
+  if (p.variant == 9) {  // bulk staging: report a timed-out copy (not while a graph is captured)
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     GASP_CUDA(cudaStreamIsCapturing(s, &cs));
     if (cs == cudaStreamCaptureStatusNone) {

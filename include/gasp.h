@@ -138,13 +138,8 @@ int gasp_grids_shape(const gasp_grids_t *grids, int *L_out, int *ngrids_out);
  * loads and stores (L = 32, 64, 96, 128 in replica order, i.e. without an
  * active list; bit-identical to 0, measured slower; each launch reads back
  * a device flag, so a copy that did not complete within its bounded wait
- * returns GASP_ERR_TIMEOUT); 10 the warp-specialised row kernel (L = 32, 64,
- * 96, 128): per tile of 32 replicas one warp draws the attempts' sites and
- * acceptance values in each replica's stream order into a shared-memory
- * queue and a second warp applies them to the lattices (bit-identical to 0;
- * a wait that does not complete within its bound returns GASP_ERR_TIMEOUT).
- * Values 3, 4 and 8 (retired kernels that were measured slower) and values
- * outside 0..10 return GASP_ERR_INVALID.
+ * returns GASP_ERR_TIMEOUT).  Values 3, 4 and 8 (retired kernels that were
+ * measured slower) and values outside 0..9 return GASP_ERR_INVALID.
  * GASP_OPT_WARPS_PER_CTA: tiles per CTA of the generic kernel (1..8).
  * GASP_OPT_TAIL_REPLICAS: device-side committor shooting (itask 1 with
  * compaction) sweeps with variant 6 once at most this many replicas are
@@ -359,13 +354,14 @@ int gasp_batch_swarm(gasp_batch_t *batch, int tot_nsweeps, int check_int, double
 /* Autotuner: times the candidate kernels (row kernel with or without the
  * every-attempt store; tiles per CTA of the generic kernel) for each group on
  * an nsweeps run and keeps the fastest; then times the interval graph in both
- * layouts (one kernel per group, or one persistent launch for all groups) and
- * keeps the faster for GASP_BATCH_GRAPH.  choice_out (2*ngroups ints, may be
+ * layouts (one kernel per group, or one persistent launch for all groups) on
+ * intervals of max(nsweeps, 20) sweeps with all, half and 15 % of every
+ * group live, and keeps the faster for GASP_BATCH_GRAPH.  choice_out (2*ngroups ints, may be
  * NULL): (variant, warps per CTA) chosen per group. */
 int gasp_batch_autotune(gasp_batch_t *batch, int nsweeps, int *choice_out);
 /* The layout the autotuner chose (0: one kernel per group, 1: one persistent
- * launch; -1 for a NULL batch) and its timings of the two (ms for three
- * intervals; -1 when not timed). */
+ * launch; -1 for a NULL batch) and its timings of the two (ms over the six
+ * timed intervals; -1 when not timed). */
 int gasp_batch_layout(const gasp_batch_t *batch, float *ms_per_group_kernels,
                       float *ms_one_launch);
 
@@ -393,11 +389,11 @@ int gasp_cnn_predict(gasp_cnn_t *cnn, const int8_t *spins, int batch, float *q_o
  * allocates a second input buffer and a copy stream). */
 int gasp_cnn_predict_ex(gasp_cnn_t *cnn, const int8_t *spins, int batch, float *q_out,
                         float *mag_out);
-/* Prediction path for L = 64: on (the default) the whole network runs as one
- * kernel per band of 8 rows with the activations kept on the chip; off, layer
- * by layer through HBM as training does.  Same arithmetic either way (BF16
- * activations, FP32 accumulation); only the order of the pooled FP32 sums
- * differs.  Other L always run layer by layer. */
+/* Prediction path for L = 64: on, the whole network runs as one kernel per
+ * band of 8 rows with the activations kept on the chip; off (the default,
+ * measured faster so far), layer by layer through HBM as training does.  Same
+ * arithmetic either way (BF16 activations, FP32 accumulation); only the order
+ * of the pooled FP32 sums differs.  Other L always run layer by layer. */
 int gasp_cnn_set_fused(gasp_cnn_t *cnn, int on);
 /* Loss (mean over the batch) and its gradient for labels in [0, 1]. */
 int gasp_cnn_gradients(gasp_cnn_t *cnn, const int8_t *spins, const float *labels, int batch,

@@ -132,6 +132,7 @@ def test_fused_forward_matches_layer_by_layer_and_oracle():
         params[o:o + 32] = rs.normal(0, 0.2, 32)
     params[-33:] = rs.normal(0, 0.5, 33).astype(np.float32)
     net = surrogate.CommittorCNN(L, 16, params)
+    check(lib().gasp_cnn_set_fused(net._h, 1))
     q_fused = net.predict(g)
     check(lib().gasp_cnn_set_fused(net._h, 0))
     q_layers = net.predict(g)

@@ -179,8 +179,8 @@ def test_cli_committor_reads_gridinput(ref_gpu, tmp_path):
 @pytest.mark.parametrize("beta,h", [(0.45, 0.1), (0.5, 0.0), (1e-9, 0.1)])
 def test_kernel_variants_agree(L, kind, beta, h):
     """The generic (with and without the every-attempt store), row (with
-    and without it), bulk-staged and warp-specialised kernels give identical
-    results for both RNG kinds (96 replicas: three tiles).  h = 0 leaves six classes that can
+    and without it) and bulk-staged kernels give identical results for both
+    RNG kinds (96 replicas: three tiles).  h = 0 leaves six classes that can
     reject; at beta = 1e-9 every P rounds to 1.0 and ten classes can reject.
     The retired variants 3, 4 and 8 are refused."""
     ng, seed = 96, 31 + L
@@ -190,7 +190,7 @@ def test_kernel_variants_agree(L, kind, beta, h):
     for variant in (3, 4, 8, 10, -1):
         assert lib().gasp_grids_set_option(probe.handle, 1, variant) != 0
     probe.close()
-    for variant in (0, 1, 2, 5, 9, 10):
+    for variant in (0, 1, 2, 5, 9):
         dg = engine.DeviceGrids(L, ng, g0)
         dg.set_option(1, variant)
         r = engine.RngStates(ng, seed, kind=kind)
