@@ -936,8 +936,8 @@ def main(argv=None):
     ap.add_argument("--surrogate-train", type=int, default=20000)
     ap.add_argument("--surrogate-test", type=int, default=2000)
     ap.add_argument("--surrogate-screen", type=int, default=100000)
-    ap.add_argument("--surrogate-epochs", type=int, default=40)
-    ap.add_argument("--surrogate-focus", type=float, default=0.0,
+    ap.add_argument("--surrogate-epochs", type=int, default=120)
+    ap.add_argument("--surrogate-focus", type=float, default=3.0,
                     help="training draws grids with weight 1 + focus*4y(1-y)")
     ap.add_argument("--batched-sweeps", type=int, default=1000)
     ap.add_argument("--rng", default="xorwow", choices=["xorwow", "mwc64x"],

@@ -263,9 +263,11 @@ __global__ void __launch_bounds__(128) k_conv_tc(ConvArgs a) {
           o[c] = __float2bfloat16_rn(acc[c]);
         }
       }
-      uint4 *dst = reinterpret_cast<uint4 *>(a.y + ((size_t)img * N + p) * kC);
+      if (a.y != nullptr) {  // prediction does not keep the last layer's activations
+        uint4 *dst = reinterpret_cast<uint4 *>(a.y + ((size_t)img * N + p) * kC);
 #pragma unroll
-      for (int c = 0; c < 4; ++c) dst[c] = reinterpret_cast<uint4 *>(o)[c];
+        for (int c = 0; c < 4; ++c) dst[c] = reinterpret_cast<uint4 *>(o)[c];
+      }
       if (MODE == kFwd && a.pool != nullptr) {
         // channel sums of the rounded activations over the tile
 #pragma unroll
@@ -463,9 +465,11 @@ __global__ void __launch_bounds__(128) k_conv_win(ConvArgs a) {
           o[c] = __float2bfloat16_rn(acc[c]);
         }
       }
-      uint4 *dst = reinterpret_cast<uint4 *>(a.y + ((size_t)img * N + p) * kC);
+      if (a.y != nullptr) {  // prediction does not keep the last layer's activations
+        uint4 *dst = reinterpret_cast<uint4 *>(a.y + ((size_t)img * N + p) * kC);
 #pragma unroll
-      for (int c = 0; c < 4; ++c) dst[c] = reinterpret_cast<uint4 *>(o)[c];
+        for (int c = 0; c < 4; ++c) dst[c] = reinterpret_cast<uint4 *>(o)[c];
+      }
       if (MODE == kFwd && a.pool != nullptr) {
 #pragma unroll
         for (int c = 0; c < 32; ++c) red[tid * 33 + c] = __bfloat162float(o[c]);
@@ -518,7 +522,9 @@ constexpr int kFzLead = 8;     // positions before position 0 (tap reads reach -
 constexpr int kFzPosA = 1048;  // positions per chunk, buffer A (a1: 14 rows, a3: 10)
 constexpr int kFzPosB = 912;   // buffer B (a2: 12 rows)
 constexpr int kFzIm = 1024;    // layer-1 im2col rows (8 tiles of 128)
-constexpr int kFzThreads = 288;  // warps 0-7: epilogue (two groups of four), warp 8: MMA issue
+constexpr int kFzGroups = 4;                    // TMEM accumulators = epilogue groups of 4 warps
+constexpr int kFzThreads = (4 * kFzGroups + 1) * 32;  // + one MMA-issue warp (the last)
+constexpr int kFzTilesMax = 8;                  // M tiles per layer and band, at most
 // shared-memory layout (bytes)
 constexpr uint32_t kFzW = 0;                                 // W2..W4, 3 x 32 x 288 bf16
 constexpr uint32_t kFzW1 = kFzW + 3u * kC * 288 * 2;         // W1, 32 x 16 bf16
@@ -528,8 +534,11 @@ constexpr uint32_t kFzImB = kFzBufB + 4u * kFzPosB * 16;     // im2col, 1024 x 1
 constexpr uint32_t kFzSp = kFzImB + (uint32_t)kFzIm * 16 * 2;  // spins, 16 rows x 66 (+pad)
 constexpr uint32_t kFzBias = kFzSp + 16u * kFzPitch + 32;      // 4 x 32 floats
 constexpr uint32_t kFzPool = kFzBias + 4u * kC * 4;            // 32 floats
-constexpr uint32_t kFzBar = kFzPool + (uint32_t)kC * 4;        // 4 mbarriers + TMEM slot
-constexpr size_t kFzSmem = kFzBar + 64;
+// mbarriers: mma_done[4], acc_free[4], tile_done[4 layers][8]; then the TMEM
+// slot and the abort flag
+constexpr uint32_t kFzBar = kFzPool + (uint32_t)kC * 4;
+constexpr uint32_t kFzNBar = 2 * kFzGroups + 4 * kFzTilesMax;
+constexpr size_t kFzSmem = kFzBar + kFzNBar * 8 + 16;
 static_assert(kFzSmem <= 227 * 1024, "fused kernel shared memory");
 static_assert(kFzBufA % 16 == 0 && kFzBufB % 16 == 0 && kFzImB % 16 == 0, "16-byte operands");
 
@@ -548,11 +557,15 @@ __global__ void __launch_bounds__(kFzThreads, 1) k_cnn_fused64(FusedArgs a) {
   constexpr int K = 9 * kC;       // 288
   constexpr int SBO_W = K * 16;   // weights: bytes between 8-row groups
   constexpr int kBands = L / kFzRows;
+  constexpr int kIssuer = 4 * kFzGroups;  // the MMA warp
   extern __shared__ __align__(1024) unsigned char smem[];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  uint64_t *bar = reinterpret_cast<uint64_t *>(smem + kFzBar);  // mma_done[2], acc_free[2]
-  uint32_t *tslot = reinterpret_cast<uint32_t *>(smem + kFzBar + 32);
-  volatile int *abort_flag = reinterpret_cast<volatile int *>(smem + kFzBar + 40);
+  uint64_t *bar = reinterpret_cast<uint64_t *>(smem + kFzBar);
+  uint64_t *mma_done = bar;                        // [kFzGroups], one commit each
+  uint64_t *acc_free = bar + kFzGroups;            // [kFzGroups], one arrival per warp
+  uint64_t *tile_done = bar + 2 * kFzGroups;       // [4][kFzTilesMax], one arrival per warp
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(smem + kFzBar + kFzNBar * 8);
+  volatile int *abort_flag = reinterpret_cast<volatile int *>(smem + kFzBar + kFzNBar * 8 + 8);
   float *bias = reinterpret_cast<float *>(smem + kFzBias);
   float *spool = reinterpret_cast<float *>(smem + kFzPool);
   int8_t *sp = reinterpret_cast<int8_t *>(smem + kFzSp);
@@ -561,15 +574,16 @@ __global__ void __launch_bounds__(kFzThreads, 1) k_cnn_fused64(FusedArgs a) {
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                      smem_u32(tslot)),
-                 "r"(64)
+                 "r"(32 * kFzGroups)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
   if (tid == 0) {
-    mbar_init(smem_u32(&bar[0]), 1);
-    mbar_init(smem_u32(&bar[1]), 1);
-    mbar_init(smem_u32(&bar[2]), 4);  // one arrival per epilogue warp
-    mbar_init(smem_u32(&bar[3]), 4);
+    for (int i = 0; i < kFzGroups; ++i) {
+      mbar_init(smem_u32(&mma_done[i]), 1);
+      mbar_init(smem_u32(&acc_free[i]), 4);
+    }
+    for (int i = 0; i < 4 * kFzTilesMax; ++i) mbar_init(smem_u32(&tile_done[i]), 4);
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -593,15 +607,13 @@ __global__ void __launch_bounds__(kFzThreads, 1) k_cnn_fused64(FusedArgs a) {
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t taddr = *tslot;
 
-  const int grp = warp >> 2, quad = warp & 3;  // epilogue warps (warp < 8)
-  uint32_t use0 = 0, use1 = 0;                 // issuer: uses of each accumulator
+  const int grp = warp >> 2, quad = warp & 3;  // epilogue warps (warp < kIssuer)
+  uint32_t use[kFzGroups] = {};                // issuer: uses of each accumulator
   uint32_t my_use = 0;                         // epilogue: uses of its group's accumulator
-  uint32_t seq = 0;                            // tiles issued so far (same on every thread)
-  float psum[kC];
-#pragma unroll
-  for (int c = 0; c < kC; ++c) psum[c] = 0.f;
+  uint32_t my_base = 0;                        // tiles of earlier bands (accumulator = tile % 4)
+  uint32_t nband = 0;                          // bands done (tile_done parity)
 
-  for (int band = blockIdx.x; band < a.nbands; band += gridDim.x) {
+  for (int band = blockIdx.x; band < a.nbands; band += gridDim.x, ++nband) {
     const int img = band / kBands, y0 = (band % kBands) * kFzRows;
     // spins of image rows y0-4 .. y0+11, with the wrapped ghost columns
     const int8_t *sg = a.spins + (size_t)img * N;
@@ -635,22 +647,28 @@ __global__ void __launch_bounds__(kFzThreads, 1) k_cnn_fused64(FusedArgs a) {
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-
-    for (int layer = 0; layer < 4; ++layer) {
-      const int npos = (14 - 2 * layer) * kFzPitch;  // output positions of this layer
-      const int ntiles = (npos + 127) / 128;
-      // layer 1 (index 1) reads buffer A and writes B; layer 2 reads B, writes A; layer 3 reads A
-      const uint32_t in_off = layer == 2 ? kFzBufB : kFzBufA;
-      const uint32_t in_lbo = (layer == 2 ? kFzPosB : kFzPosA) * 16u;
-      const uint32_t out_off = layer == 1 ? kFzBufB : kFzBufA;
-      const uint32_t out_lbo = (layer == 1 ? kFzPosB : kFzPosA) * 16u;
-      if (warp == 8) {
-        if (lane == 0) {
+    // The band's 26 M tiles, layer after layer (8, 7, 6, 5 tiles).  Tile t of
+    // layer l reads layer l-1 positions up to 128 t + 260 (taps and ghost
+    // columns), all written by tiles 0..t+2 of layer l-1, so it waits for
+    // those tiles only: no barrier between layers.  The same bound keeps
+    // every buffer write clear of the reads still in flight.
+    if (warp == kIssuer) {
+      if (lane == 0) {
+        for (int layer = 0; layer < 4; ++layer) {
+          const int ntiles = ((14 - 2 * layer) * kFzPitch + 127) / 128;
+          const int nprev = layer > 0 ? ((16 - 2 * layer) * kFzPitch + 127) / 128 : 0;
+          const uint32_t in_off = layer == 2 ? kFzBufB : kFzBufA;
+          const uint32_t in_lbo = (layer == 2 ? kFzPosB : kFzPosA) * 16u;
+          int ready = 0;
           for (int t = 0; t < ntiles; ++t) {
-            const int g = (int)((seq + (uint32_t)t) & 1u);
-            const uint32_t u = g ? use1 : use0;
-            if (u > 0 && !*abort_flag && !mbar_wait(smem_u32(&bar[2 + g]), (u - 1) & 1u))
+            const int g = (int)(use[0] + use[1] + use[2] + use[3]) & (kFzGroups - 1);
+            if (use[g] > 0 && !*abort_flag &&
+                !mbar_wait(smem_u32(&acc_free[g]), (use[g] - 1) & 1u))
               *abort_flag = 1;
+            const int need = min(t + 3, nprev);
+            for (; ready < need && !*abort_flag; ++ready)
+              if (!mbar_wait(smem_u32(&tile_done[(layer - 1) * kFzTilesMax + ready]), nband & 1u))
+                *abort_flag = 1;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             if (!*abort_flag) {
               const uint32_t d = taddr + (uint32_t)(g * 32);
@@ -667,25 +685,32 @@ __global__ void __launch_bounds__(kFzThreads, 1) k_cnn_fused64(FusedArgs a) {
                 const uint32_t lbo16 = in_lbo >> 4;
 #pragma unroll
                 for (int tap = 0; tap < 9; ++tap) {
-                  const int dy = tap / 3 - 1, dx = tap % 3 - 1;
-                  const int pos = (1 + dy) * kFzPitch + dx;  // >= -1, base is kFzLead in
+                  const int pos = (tap / 3) * kFzPitch + tap % 3 - 1;  // >= -1; base is kFzLead in
 #pragma unroll
                   for (int j = 0; j < 2; ++j)
                     umma_bf16(d, da0 + (uint64_t)(int64_t)(pos + (int)(2u * j * lbo16)),
                               db0 + (uint64_t)((tap * 2 + j) * 16), (tap | j) ? 1u : 0u);
                 }
               }
-              umma_commit(smem_u32(&bar[g]));
+              umma_commit(smem_u32(&mma_done[g]));
             }
-            if (g) ++use1; else ++use0;
+            ++use[g];
           }
         }
-      } else {
-        for (int t = 0; t < ntiles; ++t) {
-          if ((int)((seq + (uint32_t)t) & 1u) != grp) continue;
-          // one lane polls the MMA barrier (32 x 8 spinning lanes would keep
-          // the shared-memory pipe busy); the warp barrier passes it on
-          if (lane == 0 && !*abort_flag && !mbar_wait(smem_u32(&bar[grp]), my_use & 1u))
+      }
+      __syncwarp();
+    } else {
+      uint32_t seqb = 0;  // tiles of this band so far
+      for (int layer = 0; layer < 4; ++layer) {
+        const int npos = (14 - 2 * layer) * kFzPitch;  // output positions of this layer
+        const int ntiles = (npos + 127) / 128;
+        // layer index 1 writes buffer B, 2 writes A, 3 (pooled) writes B; 0 writes A
+        const uint32_t out_off = (layer & 1) ? kFzBufB : kFzBufA;
+        const uint32_t out_lbo = ((layer & 1) ? kFzPosB : kFzPosA) * 16u;
+        for (int t = 0; t < ntiles; ++t, ++seqb) {
+          if ((int)((my_base + seqb) & (kFzGroups - 1)) != grp) continue;
+          // one lane polls; the warp barrier passes it on
+          if (lane == 0 && !*abort_flag && !mbar_wait(smem_u32(&mma_done[grp]), my_use & 1u))
             *abort_flag = 1;
           __syncwarp();
           ++my_use;
@@ -696,14 +721,12 @@ __global__ void __launch_bounds__(kFzThreads, 1) k_cnn_fused64(FusedArgs a) {
           __syncwarp();
           // the accumulator is in registers: hand it back to the issuer now
           if (lane == 0)
-            asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(
-                             smem_u32(&bar[2 + grp]))
+            asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&acc_free[grp]))
                          : "memory");
           const int q = 128 * t + quad * 32 + lane;
           const int i = q / kFzPitch, j = q - i * kFzPitch;
-          if (*abort_flag || q >= npos || j < 1 || j > L) continue;  // ghost or beyond the band
-          const float *bl = bias + layer * kC;
-          if (layer < 3) {
+          if (!*abort_flag && q < npos && j >= 1 && j <= L) {  // a pixel (not a ghost) of the band
+            const float *bl = bias + layer * kC;
             __align__(16) __nv_bfloat16 o[32];
 #pragma unroll
             for (int c = 0; c < 32; ++c) {
@@ -711,39 +734,37 @@ __global__ void __launch_bounds__(kFzThreads, 1) k_cnn_fused64(FusedArgs a) {
               o[c] = __float2bfloat16_rn(z > 0.0f ? z : 0.0f);
             }
             const uint32_t p0 = (uint32_t)(kFzLead + q) * 16u;
+            const bool ghost = layer < 3 && (j == 1 || j == L);
             const uint32_t pg = (uint32_t)(kFzLead + i * kFzPitch + (j == 1 ? L + 1 : 0)) * 16u;
 #pragma unroll
             for (int c = 0; c < 4; ++c) {
               const uint4 val = reinterpret_cast<const uint4 *>(o)[c];
               *reinterpret_cast<uint4 *>(smem + out_off + c * out_lbo + p0) = val;
-              if (j == 1 || j == L) *reinterpret_cast<uint4 *>(smem + out_off + c * out_lbo + pg) = val;
-            }
-          } else {
-#pragma unroll
-            for (int c = 0; c < 32; ++c) {
-              const float z = acc[c] + bl[c];
-              psum[c] += __bfloat162float(__float2bfloat16_rn(z > 0.0f ? z : 0.0f));
+              if (ghost) *reinterpret_cast<uint4 *>(smem + out_off + c * out_lbo + pg) = val;
             }
           }
+          // this warp's rows of the tile are written: visible to the MMA (async proxy)
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+          __syncwarp();
+          if (lane == 0)
+            asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(
+                             smem_u32(&tile_done[layer * kFzTilesMax + t]))
+                         : "memory");
         }
       }
-      seq += (uint32_t)ntiles;
-      // the layer's outputs, to the tensor cores' (async) view, before the next layer
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-      __syncthreads();
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     }
-    // pooled sums of the band: warp reduce, then shared, then one atomicAdd per channel
-    if (warp < 8) {
-#pragma unroll
-      for (int c = 0; c < kC; ++c) {
-        float v = psum[c];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        if (lane == 0) atomicAdd(&spool[c], v);
-        psum[c] = 0.f;
-      }
+    my_base += 26;  // tiles per band (8 + 7 + 6 + 5)
+    __syncthreads();
+    // pooled sums of the band's 8 rows of a4 (buffer B): thread (row, channel)
+    if (tid < kFzRows * kC) {
+      const int c = tid & (kC - 1), i = tid >> 5;
+      const unsigned char *src = smem + kFzBufB + (c >> 3) * (kFzPosB * 16) +
+                                 (kFzLead + i * kFzPitch + 1) * 16 + (c & 7) * 2;
+      float sum = 0.f;
+#pragma unroll 8
+      for (int x = 0; x < L; ++x)
+        sum += __bfloat162float(*reinterpret_cast<const __nv_bfloat16 *>(src + x * 16));
+      atomicAdd(&spool[c], sum);
     }
     __syncthreads();
     if (tid < kC && !*abort_flag) atomicAdd(&a.pool[img * kC + tid], spool[tid]);
@@ -752,7 +773,8 @@ __global__ void __launch_bounds__(kFzThreads, 1) k_cnn_fused64(FusedArgs a) {
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 0) {
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(64)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr),
+                 "r"(32 * kFzGroups)
                  : "memory");
   }
 }
@@ -1335,7 +1357,10 @@ int launch_conv(const ConvArgs &a, int batch, cudaStream_t s) {
   return launch_persistent(k_conv_tc<MODE>, smem_max, smem, b, s);
 }
 
-int cnn_forward(gasp_cnn *c, int batch, cudaStream_t s, const int8_t *spins = nullptr) {
+// keep_last: store the last layer's activations (training's ReLU mask); the
+// prediction path only needs their pooled sums.
+int cnn_forward(gasp_cnn *c, int batch, cudaStream_t s, const int8_t *spins = nullptr,
+                bool keep_last = true) {
   int rc;
   const int B = batch;
   k_pack_weights<<<(3 * 9216 + 255) / 256, 256, 0, s>>>(c->d_params, c->d_w1, c->d_w, c->d_wt);
@@ -1354,7 +1379,7 @@ int cnn_forward(gasp_cnn *c, int batch, cudaStream_t s, const int8_t *spins = nu
     a.x = c->d_act[l];
     a.w = c->d_w + l * 9216;
     a.bias = c->d_params + kOffB2 + l * (9216 + 32);
-    a.y = c->d_act[l + 1];
+    a.y = (l == 2 && !keep_last) ? nullptr : c->d_act[l + 1];
     a.pool = (l == 2) ? c->d_pool : nullptr;
     if ((rc = launch_conv<kFwd>(a, B, s))) return rc;
   }
@@ -1364,7 +1389,7 @@ int cnn_forward(gasp_cnn *c, int batch, cudaStream_t s, const int8_t *spins = nu
 // Inference forward (pooled sums in d_pool): the fused whole-network kernel
 // for L = 64 when switched on, the layer-by-layer kernels otherwise.
 int cnn_infer(gasp_cnn *c, int batch, cudaStream_t s, const int8_t *spins = nullptr) {
-  if (c->L != 64 || !c->fused) return cnn_forward(c, batch, s, spins);
+  if (c->L != 64 || !c->fused) return cnn_forward(c, batch, s, spins, false);
   k_pack_weights<<<(3 * 9216 + 255) / 256, 256, 0, s>>>(c->d_params, c->d_w1, c->d_w, c->d_wt);
   GASP_CUDA(cudaGetLastError());
   GASP_CUDA(cudaMemsetAsync(c->d_pool, 0, (size_t)batch * kC * sizeof(float), s));

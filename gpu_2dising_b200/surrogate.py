@@ -255,8 +255,8 @@ def screen(cnn, grids, beta, h, fallback_shots=128, band=0.1, window=None, **sho
 
 
 def run_experiment(n_train=20000, train_shots=256, n_test=2000, test_shots=1024,
-                   n_screen=100000, baseline_shots=64, epochs=40, batch=1024, lr=2e-3, beta=0.54,
-                   h=0.07, seed=0, log=None, focus=0.0):
+                   n_screen=100000, baseline_shots=64, epochs=120, batch=1024, lr=2e-3, beta=0.54,
+                   h=0.07, seed=0, log=None, focus=3.0):
     """Train the surrogate on shooting labels and measure what it gains.
 
     Returns a dict with the held-out MAE (surrogate alone and screened with
