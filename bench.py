@@ -881,6 +881,7 @@ def secondary_measure(args):
             "n_test", "n_screen", "times_s", "clocks")
     out["surrogate"] = {"metric": su["metric"], **{k: su[k] for k in keys if k in su},
                         "equal_mae": su.get("by_cap", {}).get("equal_mae"),
+                        "bar_0.05": su.get("by_cap", {}).get("bar_0.05"),
                         "workload": su["config"]["workload"]}
     out["quick"] = bool(args.secondary_quick)
     return out
