@@ -449,6 +449,91 @@ __device__ __forceinline__ void pattern_tables(const SweepLaunch &p, uint32_t *t
   paccP[lane] = p.pacc_f[2 * cls];
 }
 
+// The L=64 row kernel on the reference stream (integer thresholds, centre
+// word written back on every attempt) runs its attempts in blocks of K, each
+// in two phases: row_draw64 takes the block's 2K draws in the reference's
+// order (site, acceptance, site, ...) and each site's word offset, then
+// row_apply64 applies the K attempts in order.  The applies form a chain of
+// shared-memory round trips with only their own arithmetic in between, and
+// the draws are independent work the scheduler can issue back to back; the
+// trajectory is the row_attempt loop's (same draws, same attempts, same
+// order).
+//   The site is floor(fl(shrink * u)) as in the reference.  With f =
+// fl(shrink * u) in [0, N), the sum f + 2^23 rounded down is 2^23 + floor(f)
+// (the floats in [2^23, 2^24) are the integers), whose bit pattern is
+// sb = 0x4B000000 + floor(f).  0x4B000000 has no bit below bit 24, so sb
+// stands in for the site wherever only its low bits count: the word offset
+// (sb << 2 masked), the funnel-shift amounts (taken mod 32), the flip bit
+// (a funnel shift, also mod 32) and the wrap test on the bit position
+// (sb << 27 keeps the five low bits on top).
+// Measured on the headline workload (32768 replicas, 100 sweeps per launch,
+// exact stream, one B200): 4.58e11 attempts/s against 4.41e11 for the
+// unrolled row_attempt loop.  Blocks of 8 or 32, the up/down offsets computed
+// in the draw phase, the next block's draws interleaved with this block's
+// applies, and starting odd tiles half a block ahead were all slower; the
+// MWC64X instantiation keeps the unrolled loop (blocks: 4.87e11 against
+// 4.92e11).
+
+// Five opaque register constants materialised at the top of each block.
+// They take no part in the arithmetic; they change how the compiler orders
+// a block's draws against the previous block's applies.  Measured: 4.57-4.59e11
+// attempts/s with them, 4.48e11 without, 4.47-4.55e11 with 1, 2, 3 or 8 of
+// them or with an empty asm statement or a memory clobber instead.  Results
+// are bit-identical either way.
+__device__ __forceinline__ void block_marks() {
+  [[maybe_unused]] uint32_t m0, m1, m2, m3, m4;
+  asm volatile("mov.u32 %0, 16;" : "=r"(m0));
+  asm volatile("mov.u32 %0, 2;" : "=r"(m1));
+  asm volatile("mov.u32 %0, 1073741824;" : "=r"(m2));
+  asm volatile("mov.u32 %0, 1;" : "=r"(m3));
+  asm volatile("mov.u32 %0, 362437;" : "=r"(m4));
+}
+
+template <int L, int K, typename Rng>
+__device__ __forceinline__ void row_draw64(Rng &rg, uint32_t (&offc)[K], uint32_t (&sbits)[K],
+                                           uint32_t (&x2)[K], uint32_t lane4, float shrink) {
+  static_assert(L == 64, "rows of two words");
+  constexpr int N = L * L;
+  constexpr uint32_t kMask = (uint32_t)(4 * N - 1) & ~127u;  // word part of a byte offset
+  block_marks();
+#pragma unroll
+  for (int j = 0; j < K; ++j) {
+    const uint32_t sb =
+        __float_as_uint(__fadd_rd(shrink * _curand_uniform(rg.next()), 8388608.0f));
+    x2[j] = rg.next();
+    offc[j] = ((sb << 2) & kMask) | lane4;
+    sbits[j] = sb;
+  }
+}
+
+template <int L, int K>
+__device__ __forceinline__ void row_apply64(const uint32_t (&offc)[K], const uint32_t (&sbits)[K],
+                                            const uint32_t (&x2)[K], const char *latb,
+                                            const char *thrb, uint32_t lane4) {
+  constexpr int N = L * L;
+  constexpr uint32_t kMask = (uint32_t)(4 * N - 1) & ~127u;
+#pragma unroll
+  for (int j = 0; j < K; ++j) {
+    const uint32_t oc = offc[j], sb = sbits[j];
+    const uint32_t wu = *reinterpret_cast<const uint32_t *>(latb + (((oc - 256u) & kMask) | lane4));
+    const uint32_t wd = *reinterpret_cast<const uint32_t *>(latb + (((oc + 256u) & kMask) | lane4));
+    const uint32_t wc = *reinterpret_cast<const uint32_t *>(latb + oc);
+    const uint32_t wx = *reinterpret_cast<const uint32_t *>(latb + (oc ^ 128u));
+    // the row's circular 64 bits seen from the site's word (see row_attempt):
+    // bit position b = sb mod 32 below 3 reads the pair the other way round
+    const bool wrap = (sb << 27) < (3u << 27);
+    const uint32_t lo = wrap ? wx : wc;
+    const uint32_t hi = wrap ? wc : wx;
+    const uint32_t t = __funnelshift_r(lo, hi, sb + 29u);  // bits 2,3,4: left, centre, right
+    const uint32_t u = __funnelshift_r(wu, wu, sb + 27u);  // bit 5: up
+    const uint32_t d = __funnelshift_r(wd, wd, sb + 26u);  // bit 6: down
+    const uint32_t p4 = (t & 0x1Cu) | (u & 0x20u) | (d & 0x40u);
+    const bool acc = x2[j] <= *reinterpret_cast<const uint32_t *>(thrb + p4);
+    const uint32_t bit = __funnelshift_l(0u, 1u, sb);  // 1 << b
+    *reinterpret_cast<uint32_t *>(const_cast<char *>(latb) + oc) = acc ? wc ^ bit : wc;
+  }
+}
+
 // One lane's attempts of a row-kernel batch (N * nsweeps of them) on its
 // staged lattice, software-pipelined: draw order x1(a), x2(a), x1(a+1), ...
 // as in the reference.  The host keeps N*nsweeps < 2^31.
@@ -463,8 +548,19 @@ __device__ __forceinline__ void rows_run(const SweepLaunch &p, int rep, const ui
   rg.load(p.rng, p.rng_stride, rep);
   const float shrink = (1.0f - FLT_EPSILON) * (float)N;
   const uint32_t lane4 = (uint32_t)lane << 2;
-  uint32_t s = rg.template site<N>(shrink, N);
   const int total = N * p.nsweeps;
+  if constexpr (L == 64 && kRng == kRngXorwow && !kFloatCmp && kStoreAlways) {
+    // the default L=64 kernel on the reference stream: blocks of 16 attempts
+    // (total = 4096 * nsweeps is a multiple of 16)
+    uint32_t offc[16], sbits[16], x2[16];
+    for (int a = 0; a < total; a += 16) {
+      row_draw64<L, 16>(rg, offc, sbits, x2, lane4, shrink);
+      row_apply64<L, 16>(offc, sbits, x2, latb, thrb, lane4);
+    }
+    rg.store(p.rng, p.rng_stride, rep);
+    return;
+  }
+  uint32_t s = rg.template site<N>(shrink, N);
   if constexpr (L == 64 && kRng == kRngXorwow) {
     // unroll measured at L=64 on the reference stream: 8 -> 4.40e11, 5 -> 4.23e11,
     // 16 -> 4.36e11, 10 -> 4.28e11 attempts/s (the MWC64X stream is fastest at 5)
