@@ -472,7 +472,9 @@ __device__ __forceinline__ void pattern_tables(const SweepLaunch &p, uint32_t *t
 // in the draw phase, the next block's draws interleaved with this block's
 // applies, and starting odd tiles half a block ahead were all slower; the
 // MWC64X instantiation keeps the unrolled loop (blocks: 4.87e11 against
-// 4.92e11).
+// 4.92e11); with the marks below, blocks of 8 (4.50e11) or 32 (4.46e11), a
+// second set of marks before the applies (4.50e11) and a store only on
+// acceptance (4.35e11) were slower.
 
 // Five opaque register constants materialised at the top of each block.
 // They take no part in the arithmetic; they change how the compiler orders
