@@ -536,6 +536,96 @@ __device__ __forceinline__ void row_apply64(const uint32_t (&offc)[K], const uin
   }
 }
 
+// The same blocks for the other row-kernel sides (L = 32, 96, 128) on the
+// reference stream: row_draw / row_apply below are the L=64 pair written for
+// rows of one, two or more words.  L=64 keeps its own pair: compiled from the
+// generic source its schedule came out 4 % slower (4.41e11 against 4.59e11).
+// Measured against the unrolled row_attempt loop: L=96 +8.7 % (2048 and 32768
+// replicas), L=128 +2.9 % (512 and 16384), L=32 +3.6 % (32768; 16384: -0.3 %);
+// the uneven batch 3 % faster on both its paths.  The MWC64X instantiations
+// keep the unrolled loop (blocks: -0.5 to -2 % at most sizes).
+// Word part of a byte offset into a tile image of 4N bytes, rounded up to a
+// power of two (the offset of the site's word is (site << 2) under it).
+template <int L>
+__host__ __device__ constexpr uint32_t row_word_mask() {
+  uint32_t m = 128;
+  while (m < 4u * L * L) m <<= 1;
+  return (m - 1) & ~127u;
+}
+
+template <int L, int K, typename Rng>
+__device__ __forceinline__ void row_draw(Rng &rg, uint32_t (&offc)[K], uint32_t (&sbits)[K],
+                                         uint32_t (&x2)[K], uint32_t lane4, float shrink) {
+  static_assert(Rng::kKind == kRngXorwow, "reference stream");
+  static_assert(L * L <= (1 << 15), "site bits and word offsets below 2^17");
+  constexpr uint32_t kMaskD = row_word_mask<L>();
+  block_marks();
+#pragma unroll
+  for (int j = 0; j < K; ++j) {
+    const uint32_t sb =
+        __float_as_uint(__fadd_rd(shrink * _curand_uniform(rg.next()), 8388608.0f));
+    x2[j] = rg.next();
+    offc[j] = ((sb << 2) & kMaskD) | lane4;
+    sbits[j] = sb;
+  }
+}
+
+template <int L, int K>
+__device__ __forceinline__ void row_apply(const uint32_t (&offc)[K], const uint32_t (&sbits)[K],
+                                          const uint32_t (&x2)[K], const char *latb,
+                                          const char *thrb, uint32_t lane4) {
+  constexpr int N = L * L;
+  constexpr int R = L / 32;
+  constexpr bool kPow2 = (L & (L - 1)) == 0;
+  constexpr uint32_t kMask = (uint32_t)(4 * N - 1) & ~127u;
+#pragma unroll
+  for (int j = 0; j < K; ++j) {
+    const uint32_t oc = offc[j], sb = sbits[j];
+    const uint32_t bt = sb << 27;  // bit position b on top
+    uint32_t offu, offd;
+    if constexpr (kPow2) {
+      offu = ((oc - 128u * R) & kMask) | lane4;
+      offd = ((oc + 128u * R) & kMask) | lane4;
+    } else {  // rows of R words, R not a power of two: wrap by compare
+      offu = oc >= 128u * R ? oc - 128u * R : oc + (4u * N - 128u * R);
+      offd = oc + 128u * R < 4u * N ? oc + 128u * R : oc - (4u * N - 128u * R);
+    }
+    const uint32_t wu = *reinterpret_cast<const uint32_t *>(latb + offu);
+    const uint32_t wd = *reinterpret_cast<const uint32_t *>(latb + offd);
+    uint32_t wc, lo, hi;
+    if constexpr (R == 1) {
+      wc = *reinterpret_cast<const uint32_t *>(latb + oc);
+      lo = hi = wc;
+    } else if constexpr (R == 2) {
+      // the row's circular 64 bits seen from the site's word (see row_attempt):
+      // b below 3 reads the pair the other way round
+      wc = *reinterpret_cast<const uint32_t *>(latb + oc);
+      const uint32_t wx = *reinterpret_cast<const uint32_t *>(latb + (oc ^ 128u));
+      const bool wrap = bt < (3u << 27);
+      lo = wrap ? wx : wc;
+      hi = wrap ? wc : wx;
+    } else {
+      // word of the site within its row; at b = 0 / 31 the left / right
+      // neighbour is in the previous / next word of the row (circularly)
+      const uint32_t wi =
+          kPow2 ? (oc >> 7) & (uint32_t)(R - 1) : ((sb & 0x7FFFFFu) >> 5) % (uint32_t)R;
+      const uint32_t offl = (bt == 0u) ? (wi == 0u ? oc + 128u * (R - 1) : oc - 128u) : oc;
+      const uint32_t offr =
+          (bt == (31u << 27)) ? (wi == (uint32_t)(R - 1) ? oc - 128u * (R - 1) : oc + 128u) : oc;
+      lo = *reinterpret_cast<const uint32_t *>(latb + offl);
+      hi = *reinterpret_cast<const uint32_t *>(latb + offr);
+      wc = (bt == 0u) ? hi : lo;
+    }
+    const uint32_t t = __funnelshift_r(lo, hi, sb + 29u);  // bits 2,3,4: left, centre, right
+    const uint32_t u = __funnelshift_r(wu, wu, sb + 27u);  // bit 5: up
+    const uint32_t d = __funnelshift_r(wd, wd, sb + 26u);  // bit 6: down
+    const uint32_t p4 = (t & 0x1Cu) | (u & 0x20u) | (d & 0x40u);
+    const bool acc = x2[j] <= *reinterpret_cast<const uint32_t *>(thrb + p4);
+    const uint32_t bit = __funnelshift_l(0u, 1u, sb);  // 1 << b
+    *reinterpret_cast<uint32_t *>(const_cast<char *>(latb) + oc) = acc ? wc ^ bit : wc;
+  }
+}
+
 // One lane's attempts of a row-kernel batch (N * nsweeps of them) on its
 // staged lattice, software-pipelined: draw order x1(a), x2(a), x1(a+1), ...
 // as in the reference.  The host keeps N*nsweeps < 2^31.
@@ -558,6 +648,17 @@ __device__ __forceinline__ void rows_run(const SweepLaunch &p, int rep, const ui
     for (int a = 0; a < total; a += 16) {
       row_draw64<L, 16>(rg, offc, sbits, x2, lane4, shrink);
       row_apply64<L, 16>(offc, sbits, x2, latb, thrb, lane4);
+    }
+    rg.store(p.rng, p.rng_stride, rep);
+    return;
+  }
+  if constexpr (L != 64 && kRng == kRngXorwow && !kFloatCmp && kStoreAlways) {
+    // blocks of 16 attempts (total = L * L * nsweeps, a multiple of 16 for
+    // L = 32, 96, 128)
+    uint32_t offc[16], sbits[16], x2[16];
+    for (int a = 0; a < total; a += 16) {
+      row_draw<L, 16>(rg, offc, sbits, x2, lane4, shrink);
+      row_apply<L, 16>(offc, sbits, x2, latb, thrb, lane4);
     }
     rg.store(p.rng, p.rng_stride, rep);
     return;
