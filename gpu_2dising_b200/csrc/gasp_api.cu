@@ -1173,6 +1173,27 @@ extern "C" int gasp_mc_driver_gpu_ex(gasp_gpu_grids_t grids, double beta, double
 
   long long attempts = 0;
   int n_active = ngrids;
+  // A check's read-backs (magnetisation, cluster sizes, frame) go on a side
+  // stream once the state they read has been produced (`ready`, recorded on
+  // the sweep stream before the interval's sweep is launched), so the copies
+  // overlap that sweep and the sweeps queue back to back; the host waits on
+  // `copied` for the data it reads.  The next write of a buffer being copied
+  // (the other half of the magnetisation pair, the frame) is launched only
+  // after the host has waited.
+  cudaStream_t rs = nullptr;
+  cudaEvent_t ready = nullptr, copied = nullptr;
+  struct SideGuard {
+    cudaStream_t &st;
+    cudaEvent_t &a, &b;
+    ~SideGuard() {
+      if (st) { cudaStreamSynchronize(st); cudaStreamDestroy(st); }
+      if (a) cudaEventDestroy(a);
+      if (b) cudaEventDestroy(b);
+    }
+  } side_guard{rs, ready, copied};
+  GASP_CUDA(cudaStreamCreateWithFlags(&rs, cudaStreamNonBlocking));
+  GASP_CUDA(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
+  GASP_CUDA(cudaEventCreateWithFlags(&copied, cudaEventDisableTiming));
   const auto t0 = std::chrono::steady_clock::now();
   if ((rc = launch_measure(g->d_lat, L, ngrids, d_mag_cur, s))) return rc;
 
@@ -1183,22 +1204,20 @@ extern "C" int gasp_mc_driver_gpu_ex(gasp_gpu_grids_t grids, double beta, double
   while (isweep < tot) {
     const bool dump_now = dumps && (isweep % grid_int == 0);
     const bool mag_now = isweep % mag_int == 0;
-    if (dump_now) {
+    if (dump_now)
       if ((rc = launch_pack_frame(g->d_lat, g->d_frame, L, ngrids, s))) return rc;
-      GASP_CUDA(cudaMemcpyAsync(hframe, g->d_frame, g->frame_bytes, cudaMemcpyDeviceToHost, s));
-    }
-    if (mag_now)
-      GASP_CUDA(cudaMemcpyAsync(hmag, d_mag_cur, (size_t)ngrids * sizeof(float),
-                                cudaMemcpyDeviceToHost, s));
-    if (mag_now && use_lclus) {  // on the lattice before this interval's sweeps
+    if (mag_now && use_lclus)  // on the lattice before this interval's sweeps
       if ((rc = measure_largest_cluster(g, -calc.initial_spin, s))) return rc;
-      GASP_CUDA(cudaMemcpyAsync(hlclus, x.d_lclus, (size_t)ngrids * sizeof(float),
-                                cudaMemcpyDeviceToHost, s));
-    }
     bool fates_done = false;
     int nA = 0, nB = 0;
     if (compact && mag_now) {
-      // Fates at this check decide which replicas the next batch simulates.
+      // Fates at this check decide which replicas the next batch simulates:
+      // read back on the sweep stream and wait before launching it.
+      GASP_CUDA(cudaMemcpyAsync(hmag, d_mag_cur, (size_t)ngrids * sizeof(float),
+                                cudaMemcpyDeviceToHost, s));
+      if (use_lclus)
+        GASP_CUDA(cudaMemcpyAsync(hlclus, x.d_lclus, (size_t)ngrids * sizeof(float),
+                                  cudaMemcpyDeviceToHost, s));
       GASP_CUDA(cudaStreamSynchronize(s));
       take_check();
       n_active = 0;
@@ -1230,11 +1249,28 @@ extern "C" int gasp_mc_driver_gpu_ex(gasp_gpu_grids_t grids, double beta, double
         GASP_CUDA(cudaMemcpyAsync(d_mag_next, d_mag_cur, (size_t)ngrids * sizeof(float),
                                   cudaMemcpyDeviceToDevice, s));
       }
+      GASP_CUDA(cudaEventRecord(ready, s));  // this check's state (before the sweep below)
       if ((rc = launch_sweep_exact(p, s))) return rc;
       attempts += (long long)n_active * N * spc;
+    } else {
+      GASP_CUDA(cudaEventRecord(ready, s));
+    }
+    if (dump_now || (mag_now && !fates_done)) {
+      // the check's read-backs, on the side stream while the sweep runs
+      GASP_CUDA(cudaStreamWaitEvent(rs, ready, 0));
+      if (dump_now)
+        GASP_CUDA(cudaMemcpyAsync(hframe, g->d_frame, g->frame_bytes, cudaMemcpyDeviceToHost, rs));
+      if (mag_now && !fates_done) {
+        GASP_CUDA(cudaMemcpyAsync(hmag, d_mag_cur, (size_t)ngrids * sizeof(float),
+                                  cudaMemcpyDeviceToHost, rs));
+        if (use_lclus)
+          GASP_CUDA(cudaMemcpyAsync(hlclus, x.d_lclus, (size_t)ngrids * sizeof(float),
+                                    cudaMemcpyDeviceToHost, rs));
+      }
+      GASP_CUDA(cudaEventRecord(copied, rs));
     }
     if (dump_now || (dumps && isweep == tot - 1)) {
-      GASP_CUDA(cudaStreamSynchronize(s));
+      GASP_CUDA(cudaEventSynchronize(copied));
       if (dump_now) {
         have_frame = true;
         if (outfunc) expand_frame(hframe, grids.ising_grids, (long long)N * ngrids);
@@ -1258,7 +1294,7 @@ extern "C" int gasp_mc_driver_gpu_ex(gasp_gpu_grids_t grids, double beta, double
     bool stop = false;
     if (mag_now || isweep == tot - 1) {
       if (mag_now && !fates_done) {
-        GASP_CUDA(cudaStreamSynchronize(s));
+        GASP_CUDA(cudaEventSynchronize(copied));
         take_check();
       }
       if (itask == 0) {
