@@ -18,6 +18,7 @@
 #include <cuda_bf16.h>
 
 #include <cmath>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <vector>
@@ -493,6 +494,217 @@ __global__ void __launch_bounds__(128) k_conv_win(ConvArgs a) {
   }
   if (warp == 0) {
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(32)
+                 : "memory");
+  }
+}
+
+// ---------------------------------------------------------------------------
+// The 32-channel forward layers at L = 64 with one staged copy of the window.
+// Positions run in rows of kGhP = 66: a ghost column on each side of the 64
+// pixels holds the circularly wrapped neighbour (left ghost = pixel 63 of the
+// row, right ghost = pixel 0), so the A operand of tap (dy, dx) for 128
+// consecutive positions is 128 consecutive window positions (1 + dy) * 66 +
+// dx + 1 further on -- a plain descriptor offset, with no rotated copies.  An
+// image is 64 * 66 = 33 * 128 positions: 33 M tiles of 128 consecutive
+// positions, whose ghost outputs (3 %) are computed and dropped.  A tile's
+// window is the 262 positions from 67 before its first position, staged once
+// (4 x 264 x 16 B = 17 KB against k_conv_win's three rotated copies, 48 KB).
+// Same arithmetic as k_conv_win (same K order: tap-major, 32 channels per
+// tap; same FP32 accumulation per MMA), so the same outputs.
+// Measured (one B200, prediction of 100 000 grids, bench.py --workload cnn):
+// 1.163M grids/s against 1.036M with k_conv_win's rotated copies (one
+// buffer, no double buffering: 1.098M); per 1024-image layer 244 us against
+// 277 us (ncu), shared-memory stores 5.8 M wavefronts against 14.1 M, the
+// tensor core's operand reads (24.3 M wavefronts) now the bulk of l1tex 75 %.
+// ---------------------------------------------------------------------------
+constexpr int kGhP = 66;                 // positions per padded row
+constexpr int kGhTiles = 64 * kGhP / kTileM;  // 33 M tiles per image
+constexpr int kGhLead = kGhP + 1;        // window positions before the tile's first
+constexpr int kGhWin = 264;              // window positions staged (262, rounded up to 8)
+static_assert(kGhTiles * kTileM == 64 * kGhP, "whole tiles per image");
+static_assert(kGhWin >= kTileM + 2 * kGhLead, "window covers every tap");
+
+size_t conv_gh64_smem(bool pool) {
+  return 2 * 4 * (size_t)kGhWin * 16 + (size_t)kC * 9 * kC * 2 + 64 +
+         (pool ? (size_t)kTileM * 33 * 4 : 0);
+}
+
+// Two window buffers and two TMEM accumulators: while the epilogue of tile
+// i reads accumulator i % 2, the MMAs of tile i+1 (staged into the other
+// buffer just before) run into the other accumulator.  A buffer is
+// restaged only after the MMAs that read it have completed (waited for one
+// iteration earlier), an accumulator is rewritten only after its epilogue's
+// tcgen05.ld (also one iteration earlier).
+__global__ void __launch_bounds__(128) k_conv_gh64(ConvArgs a) {
+  constexpr int L = 64, N = L * L;
+  constexpr int K = 9 * kC;
+  constexpr int SBO_B = K * 16;                    // weights: bytes between 8-row groups
+  constexpr uint32_t lbo = (uint32_t)kGhWin * 16;  // bytes between 8-channel chunks
+  constexpr uint32_t kBuf = 4 * lbo;               // bytes per window buffer
+  constexpr int kPerW = (kGhWin * 4 + 127) / 128;  // 16-byte chunks per thread (9)
+  extern __shared__ __align__(1024) unsigned char smem[];
+  unsigned char *sA = smem;                        // [2][4][kGhWin][16 B]
+  unsigned char *sB = smem + 2 * kBuf;             // 32 x K bf16 (interleaved)
+  uint64_t *mbar = reinterpret_cast<uint64_t *>(sB + kC * K * 2);  // [2]
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(mbar + 2);
+  float *red = reinterpret_cast<float *>(tslot + 4);  // [128][33] (pool)
+
+  const int tid = threadIdx.x, warp = tid >> 5;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(tslot)),
+                 "r"(64)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    mbar_init(smem_u32(&mbar[0]), 1);
+    mbar_init(smem_u32(&mbar[1]), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  for (int i = tid; i < kC * (K / 8); i += blockDim.x) {
+    const int n = i / (K / 8), kc = i % (K / 8);
+    cp_async16(smem_u32(sB + il_off(n, kc * 8, SBO_B)), a.w + (size_t)n * K + kc * 8);
+  }
+  cp_async_wait_all();
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t taddr = *tslot;
+
+  // A tile's window is loaded into registers ahead of its staging, so the
+  // global loads are in flight during the MMAs and epilogue before it.  A
+  // quarter-warp (8 lanes) takes one 16-byte channel chunk of 8 consecutive
+  // positions: each shared store is one conflict-free 128-byte row.
+  uint4 v4[kPerW];
+  auto load_window = [&](int t) {
+    const int timg = t / kGhTiles, m = t - timg * kGhTiles;
+    const __nv_bfloat16 *xs = a.x + (size_t)timg * N * kC;
+    const int c = (tid & 31) >> 3;
+#pragma unroll
+    for (int j = 0; j < kPerW; ++j) {
+      const int w = j * 32 + (tid >> 5) * 8 + (tid & 7);
+      if (w < kGhWin) {
+        int q = m * kTileM - kGhLead + w;  // padded position, rows wrap
+        q = q < 0 ? q + L * kGhP : (q >= L * kGhP ? q - L * kGhP : q);
+        const int r = q / kGhP, col = q - r * kGhP;
+        const int pc = col == 0 ? L - 1 : (col == kGhP - 1 ? 0 : col - 1);
+        v4[j] = *reinterpret_cast<const uint4 *>(xs + ((size_t)r * L + pc) * kC + 8 * c);
+      }
+    }
+  };
+  // stage the registers' window into buffer b, then (one thread) issue the
+  // tile's 18 MMAs into accumulator b with a commit to mbar[b]
+  auto stage_and_issue = [&](int b) {
+    const int c = (tid & 31) >> 3;
+    unsigned char *buf = sA + b * kBuf;
+#pragma unroll
+    for (int j = 0; j < kPerW; ++j) {
+      const int w = j * 32 + (tid >> 5) * 8 + (tid & 7);
+      if (w < kGhWin) *reinterpret_cast<uint4 *>(buf + c * lbo + (uint32_t)w * 16) = v4[j];
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (tid == 0) {
+      const uint32_t a0 = smem_u32(buf), b0 = smem_u32(sB);
+#pragma unroll
+      for (int tap = 0; tap < 9; ++tap) {
+        const int dy = tap / 3 - 1, dx = tap % 3 - 1;
+        const uint32_t abase = a0 + (uint32_t)(kGhLead + dy * kGhP + dx) * 16u;
+#pragma unroll
+        for (int j = 0; j < 2; ++j)
+          umma_bf16(taddr + (uint32_t)(b * 32), umma_desc(abase + 2u * j * lbo, lbo, 128),
+                    umma_desc(b0 + (uint32_t)(tap * 2 + j) * 256, 128, SBO_B),
+                    (tap | j) ? 1u : 0u);
+      }
+      umma_commit(smem_u32(&mbar[b]));
+    }
+  };
+
+  // thread 0's view: bit b of `phase` is the parity of mbar[b]'s next
+  // completion; bit b of `outstanding` marks MMAs committed to mbar[b] and
+  // not yet waited for
+  uint32_t phase = 0, outstanding = 0;
+  int tile = blockIdx.x;
+  if (tile < a.ntiles) {
+    load_window(tile);
+    stage_and_issue(0);
+    outstanding |= 1u;
+    if (tile + (int)gridDim.x < a.ntiles) load_window(tile + (int)gridDim.x);
+  }
+  for (int it = 0; tile < a.ntiles; tile += gridDim.x, ++it) {
+    const int cur = it & 1;
+    const int img = tile / kGhTiles, m = tile - img * kGhTiles;
+    const int nt = tile + (int)gridDim.x;
+    if (nt < a.ntiles) {  // the next tile's MMAs run during this tile's epilogue
+      stage_and_issue(cur ^ 1);
+      outstanding |= 1u << (cur ^ 1);
+      if (nt + (int)gridDim.x < a.ntiles) load_window(nt + (int)gridDim.x);
+    }
+    // One thread polls the MMA barrier; the CTA barrier passes the result on.
+    bool waited = true;
+    if (tid == 0) {
+      waited = mbar_wait(smem_u32(&mbar[cur]), (phase >> cur) & 1u);
+      if (waited) {
+        phase ^= 1u << cur;
+        outstanding &= ~(1u << cur);
+      }
+    }
+    const bool ok = __syncthreads_and(waited ? 1 : 0) != 0;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    float acc[32];
+    tmem_ld32(taddr + ((uint32_t)(warp * 32) << 16) + (uint32_t)(cur * 32), acc);
+
+    const int q = m * kTileM + tid;  // this thread's padded position
+    const int r = q / kGhP, col = q - r * kGhP;
+    const bool pixel = col >= 1 && col <= L;
+    if (ok) {
+      __align__(16) __nv_bfloat16 o[32];
+#pragma unroll
+      for (int c = 0; c < 32; ++c) {
+        const float z = acc[c] + a.bias[c];
+        acc[c] = z > 0.0f ? z : 0.0f;
+        o[c] = __float2bfloat16_rn(acc[c]);
+      }
+      if (a.y != nullptr && pixel) {  // prediction does not keep the last layer's activations
+        uint4 *dst = reinterpret_cast<uint4 *>(a.y + ((size_t)img * N + r * L + col - 1) * kC);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) dst[c] = reinterpret_cast<uint4 *>(o)[c];
+      }
+      if (a.pool != nullptr) {
+#pragma unroll
+        for (int c = 0; c < 32; ++c) red[tid * 33 + c] = pixel ? __bfloat162float(o[c]) : 0.0f;
+      }
+    }
+    if (a.pool != nullptr) {
+      __syncthreads();
+      if (ok && tid < 32) {
+        float sum = 0.f;
+        for (int rr = 0; rr < kTileM; ++rr) sum += red[rr * 33 + tid];
+        atomicAdd(&a.pool[img * kC + tid], sum);
+      }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    const int bad = __syncthreads_or(ok ? 0 : 1);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (bad) {
+      if (tid == 0 && a.err) atomicExch(a.err, 1);
+      break;
+    }
+  }
+  // After an abort MMAs may still be in flight into either accumulator: wait
+  // for their commits (bounded) before the columns are released.
+  if (tid == 0) {
+    for (int b = 0; b < 2; ++b)
+      if ((outstanding >> b) & 1u) mbar_wait(smem_u32(&mbar[b]), (phase >> b) & 1u);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(64)
                  : "memory");
   }
 }
@@ -1332,6 +1544,16 @@ int launch_dw(Kern kern, size_t smem, int tmem_cols, const DwArgs &b, cudaStream
   return GASP_OK;
 }
 
+// The ghost-column forward kernel at L = 64 (GASP_CNN_WINDOW_COPIES=3 selects
+// k_conv_win's three rotated copies instead, for comparisons).
+bool conv_gh64_enabled() {
+  static const bool on = [] {
+    const char *e = getenv("GASP_CNN_WINDOW_COPIES");
+    return !(e && e[0] == '3');
+  }();
+  return on;
+}
+
 // Largest shared-memory footprint the window kernel is used with.
 constexpr size_t kWinSmemLimit = 110 * 1024;
 
@@ -1339,6 +1561,13 @@ template <int MODE>
 int launch_conv(const ConvArgs &a, int batch, cudaStream_t s) {
   ConvArgs b = a;
   b.ntiles = batch * (a.L * a.L / kTileM);
+  if constexpr (MODE == kFwd) {
+    if (a.L == 64 && conv_gh64_enabled()) {  // one staged window copy (ghost columns)
+      b.ntiles = batch * kGhTiles;
+      return launch_persistent(k_conv_gh64, conv_gh64_smem(true), conv_gh64_smem(a.pool != nullptr),
+                               b, s);
+    }
+  }
   if constexpr (MODE != kFwd1) {
     const size_t win_max = conv_win_smem(a.L, MODE == kFwd);
     if (win_max <= kWinSmemLimit) {
