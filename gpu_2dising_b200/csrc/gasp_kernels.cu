@@ -467,14 +467,18 @@ __device__ __forceinline__ void pattern_tables(const SweepLaunch &p, uint32_t *t
 // (a funnel shift, also mod 32) and the wrap test on the bit position
 // (sb << 27 keeps the five low bits on top).
 // Measured on the headline workload (32768 replicas, 100 sweeps per launch,
-// exact stream, one B200): 4.58e11 attempts/s against 4.41e11 for the
-// unrolled row_attempt loop.  Blocks of 8 or 32, the up/down offsets computed
-// in the draw phase, the next block's draws interleaved with this block's
-// applies, and starting odd tiles half a block ahead were all slower; the
-// MWC64X instantiation keeps the unrolled loop (blocks: 4.87e11 against
-// 4.92e11); with the marks below, blocks of 8 (4.50e11) or 32 (4.46e11), a
-// second set of marks before the applies (4.50e11) and a store only on
-// acceptance (4.35e11) were slower.
+// exact stream, one B200): 4.78-4.80e11 attempts/s with two blocks per loop
+// iteration and the site's row loaded before the up/down words (one block
+// per iteration: 4.58e11, 4.62e11 with the row first; the unrolled
+// row_attempt loop: 4.41e11).  Blocks of 8 or 32, the up/down offsets
+// computed in the draw phase, the next block's draws interleaved with this
+// block's applies, and starting odd tiles half a block ahead were all
+// slower; the MWC64X instantiation keeps the unrolled loop (blocks: 4.87e11
+// against 4.92e11); with the marks below, blocks of 8 (4.50e11) or 32
+// (4.46e11), a second set of marks before the applies (4.50e11), a store
+// only on acceptance (4.35e11), a two-compare row window (4.51e11), four
+// blocks per iteration (2.7e11) and a register cap of 80 (4.42e11) were
+// slower.
 
 // Five opaque register constants materialised at the top of each block.
 // They take no part in the arithmetic; they change how the compiler orders
@@ -517,10 +521,11 @@ __device__ __forceinline__ void row_apply64(const uint32_t (&offc)[K], const uin
 #pragma unroll
   for (int j = 0; j < K; ++j) {
     const uint32_t oc = offc[j], sb = sbits[j];
-    const uint32_t wu = *reinterpret_cast<const uint32_t *>(latb + (((oc - 256u) & kMask) | lane4));
-    const uint32_t wd = *reinterpret_cast<const uint32_t *>(latb + (((oc + 256u) & kMask) | lane4));
+    // the site's row first (its words end the chain's critical path soonest)
     const uint32_t wc = *reinterpret_cast<const uint32_t *>(latb + oc);
     const uint32_t wx = *reinterpret_cast<const uint32_t *>(latb + (oc ^ 128u));
+    const uint32_t wu = *reinterpret_cast<const uint32_t *>(latb + (((oc - 256u) & kMask) | lane4));
+    const uint32_t wd = *reinterpret_cast<const uint32_t *>(latb + (((oc + 256u) & kMask) | lane4));
     // the row's circular 64 bits seen from the site's word (see row_attempt):
     // bit position b = sb mod 32 below 3 reads the pair the other way round
     const bool wrap = (sb << 27) < (3u << 27);
@@ -540,10 +545,14 @@ __device__ __forceinline__ void row_apply64(const uint32_t (&offc)[K], const uin
 // reference stream: row_draw / row_apply below are the L=64 pair written for
 // rows of one, two or more words.  L=64 keeps its own pair: compiled from the
 // generic source its schedule came out 4 % slower (4.41e11 against 4.59e11).
-// Measured against the unrolled row_attempt loop: L=96 +8.7 % (2048 and 32768
-// replicas), L=128 +2.9 % (512 and 16384), L=32 +3.6 % (32768; 16384: -0.3 %);
-// the uneven batch 3 % faster on both its paths.  The MWC64X instantiations
-// keep the unrolled loop (blocks: -0.5 to -2 % at most sizes).
+// Measured against the unrolled row_attempt loop, one block per iteration:
+// L=96 +8.7 % (2048 and 32768 replicas), L=128 +2.9 % (512 and 16384), L=32
+// +3.6 % (32768; 16384: -0.3 %); the uneven batch 3 % faster on both its
+// paths.  Two blocks per iteration then gave L=32 a further 3.9 % and, with
+// the site's row loaded first, L=128 3.3 %; L=96 lost 4-10 % with either.
+// The MWC64X instantiations keep the unrolled loop (blocks: -0.5 to -2 % at
+// most sizes).
+
 // Word part of a byte offset into a tile image of 4N bytes, rounded up to a
 // power of two (the offset of the site's word is (site << 2) under it).
 template <int L>
@@ -590,8 +599,14 @@ __device__ __forceinline__ void row_apply(const uint32_t (&offc)[K], const uint3
       offu = oc >= 128u * R ? oc - 128u * R : oc + (4u * N - 128u * R);
       offd = oc + 128u * R < 4u * N ? oc + 128u * R : oc - (4u * N - 128u * R);
     }
-    const uint32_t wu = *reinterpret_cast<const uint32_t *>(latb + offu);
-    const uint32_t wd = *reinterpret_cast<const uint32_t *>(latb + offd);
+    // L=128 loads the site's row before the up/down words (3.3 % faster; the
+    // other sides keep up/down first)
+    constexpr bool kRowFirst = L == 128;
+    uint32_t wu = 0, wd = 0;
+    if constexpr (!kRowFirst) {
+      wu = *reinterpret_cast<const uint32_t *>(latb + offu);
+      wd = *reinterpret_cast<const uint32_t *>(latb + offd);
+    }
     uint32_t wc, lo, hi;
     if constexpr (R == 1) {
       wc = *reinterpret_cast<const uint32_t *>(latb + oc);
@@ -615,6 +630,10 @@ __device__ __forceinline__ void row_apply(const uint32_t (&offc)[K], const uint3
       lo = *reinterpret_cast<const uint32_t *>(latb + offl);
       hi = *reinterpret_cast<const uint32_t *>(latb + offr);
       wc = (bt == 0u) ? hi : lo;
+    }
+    if constexpr (kRowFirst) {
+      wu = *reinterpret_cast<const uint32_t *>(latb + offu);
+      wd = *reinterpret_cast<const uint32_t *>(latb + offd);
     }
     const uint32_t t = __funnelshift_r(lo, hi, sb + 29u);  // bits 2,3,4: left, centre, right
     const uint32_t u = __funnelshift_r(wu, wu, sb + 27u);  // bit 5: up
@@ -644,7 +663,10 @@ __device__ __forceinline__ void rows_run(const SweepLaunch &p, int rep, const ui
   if constexpr (L == 64 && kRng == kRngXorwow && !kFloatCmp && kStoreAlways) {
     // the default L=64 kernel on the reference stream: blocks of 16 attempts
     // (total = 4096 * nsweeps is a multiple of 16)
+    // two blocks per loop iteration (4 blocks: 2.7e11, the body outgrows the
+    // instruction cache)
     uint32_t offc[16], sbits[16], x2[16];
+#pragma unroll 2
     for (int a = 0; a < total; a += 16) {
       row_draw64<L, 16>(rg, offc, sbits, x2, lane4, shrink);
       row_apply64<L, 16>(offc, sbits, x2, latb, thrb, lane4);
@@ -656,9 +678,17 @@ __device__ __forceinline__ void rows_run(const SweepLaunch &p, int rep, const ui
     // blocks of 16 attempts (total = L * L * nsweeps, a multiple of 16 for
     // L = 32, 96, 128)
     uint32_t offc[16], sbits[16], x2[16];
-    for (int a = 0; a < total; a += 16) {
-      row_draw<L, 16>(rg, offc, sbits, x2, lane4, shrink);
-      row_apply<L, 16>(offc, sbits, x2, latb, thrb, lane4);
+    if constexpr (L == 96) {  // one block per iteration (two: -4 to -10 %)
+      for (int a = 0; a < total; a += 16) {
+        row_draw<L, 16>(rg, offc, sbits, x2, lane4, shrink);
+        row_apply<L, 16>(offc, sbits, x2, latb, thrb, lane4);
+      }
+    } else {  // two blocks per iteration: L=32 +3.9 %, L=128 +3.3 % (with the row first)
+#pragma unroll 2
+      for (int a = 0; a < total; a += 16) {
+        row_draw<L, 16>(rg, offc, sbits, x2, lane4, shrink);
+        row_apply<L, 16>(offc, sbits, x2, latb, thrb, lane4);
+      }
     }
     rg.store(p.rng, p.rng_stride, rep);
     return;
