@@ -383,7 +383,7 @@ int gasp_grids_set_option(gasp_grids_t *g, int option, int value) {
   GridsExtra &x = impl(g)->x;
   // Variants 3, 4 and 8 (pairwise speculation, acceptance mask, two tiles
   // per warp) were measured slower than variant 0 and have been retired.
-  if (option == GASP_OPT_SWEEP_VARIANT && value >= 0 && value <= 9 && value != 3 &&
+  if (option == GASP_OPT_SWEEP_VARIANT && value >= 0 && value <= 10 && value != 3 &&
       value != 4 && value != 8) {
     x.variant = value;
     return GASP_OK;

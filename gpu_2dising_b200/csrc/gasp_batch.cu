@@ -303,6 +303,13 @@ int batch_reset(gasp_batch *b, cudaStream_t s) {
 SweepLaunch group_launch(gasp_batch *b, int g, int nsweeps) {
   SweepLaunch p = launch_for(b->grids[g], b->rngs[g]);
   p.nsweeps = nsweeps;
+  // The groups' kernels run side by side on the SMs: the row kernels' compact
+  // form (one block of attempts per loop iteration) keeps their code within
+  // the instruction cache.  Five-group uneven batch, 1000 sweeps: graph
+  // 1.10 s compact against 1.26 s with the two-block form, one persistent
+  // launch 1.04 s against 1.20 s (plain per-group launches, which run one
+  // kernel at a time, keep the two-block form: 2.08 s).
+  if (p.variant == 0) p.variant = 10;
   p.active = b->d_active[g];
   p.n_active = b->groups[g].ngrids;  // grid size; the live count is read on the device
   p.n_active_dev = b->d_small + 2 * g;

@@ -648,7 +648,10 @@ __device__ __forceinline__ void row_apply(const uint32_t (&offc)[K], const uint3
 // One lane's attempts of a row-kernel batch (N * nsweeps of them) on its
 // staged lattice, software-pipelined: draw order x1(a), x2(a), x1(a+1), ...
 // as in the reference.  The host keeps N*nsweeps < 2^31.
-template <int L, bool kFloatCmp, bool kStoreAlways, int kRng>
+// kCompact: one block of attempts per loop iteration at every side (half the
+// loop's code; for launches whose kernels share an SM's instruction cache
+// with other kernels, the batched groups).
+template <int L, bool kFloatCmp, bool kStoreAlways, int kRng, bool kCompact = false>
 __device__ __forceinline__ void rows_run(const SweepLaunch &p, int rep, const uint32_t *lat,
                                          const uint32_t *thrP, const float *paccP, int lane) {
   constexpr int N = L * L;
@@ -663,13 +666,20 @@ __device__ __forceinline__ void rows_run(const SweepLaunch &p, int rep, const ui
   if constexpr (L == 64 && kRng == kRngXorwow && !kFloatCmp && kStoreAlways) {
     // the default L=64 kernel on the reference stream: blocks of 16 attempts
     // (total = 4096 * nsweeps is a multiple of 16)
-    // two blocks per loop iteration (4 blocks: 2.7e11, the body outgrows the
-    // instruction cache)
     uint32_t offc[16], sbits[16], x2[16];
+    if constexpr (kCompact) {
+      for (int a = 0; a < total; a += 16) {
+        row_draw64<L, 16>(rg, offc, sbits, x2, lane4, shrink);
+        row_apply64<L, 16>(offc, sbits, x2, latb, thrb, lane4);
+      }
+    } else {
+      // two blocks per loop iteration (4 blocks: 2.7e11, the body outgrows
+      // the instruction cache)
 #pragma unroll 2
-    for (int a = 0; a < total; a += 16) {
-      row_draw64<L, 16>(rg, offc, sbits, x2, lane4, shrink);
-      row_apply64<L, 16>(offc, sbits, x2, latb, thrb, lane4);
+      for (int a = 0; a < total; a += 16) {
+        row_draw64<L, 16>(rg, offc, sbits, x2, lane4, shrink);
+        row_apply64<L, 16>(offc, sbits, x2, latb, thrb, lane4);
+      }
     }
     rg.store(p.rng, p.rng_stride, rep);
     return;
@@ -678,7 +688,7 @@ __device__ __forceinline__ void rows_run(const SweepLaunch &p, int rep, const ui
     // blocks of 16 attempts (total = L * L * nsweeps, a multiple of 16 for
     // L = 32, 96, 128)
     uint32_t offc[16], sbits[16], x2[16];
-    if constexpr (L == 96) {  // one block per iteration (two: -4 to -10 %)
+    if constexpr (L == 96 || kCompact) {  // one block per iteration (L=96, two: -4 to -10 %)
       for (int a = 0; a < total; a += 16) {
         row_draw<L, 16>(rg, offc, sbits, x2, lane4, shrink);
         row_apply<L, 16>(offc, sbits, x2, latb, thrb, lane4);
@@ -720,7 +730,7 @@ __device__ __forceinline__ void rows_run(const SweepLaunch &p, int rep, const ui
 }
 
 template <int L, bool kStatic, bool kFloatCmp, int kRng, bool kStoreAlways = false,
-          bool kBulk = false>
+          bool kBulk = false, bool kCompact = false>
 __global__ void __launch_bounds__(32) k_sweep_rows(SweepLaunch p) {
   static_assert(L % 32 == 0, "rows of whole words");
   constexpr int N = L * L;
@@ -752,7 +762,7 @@ __global__ void __launch_bounds__(32) k_sweep_rows(SweepLaunch p) {
   __syncwarp();
 
   if (live && staged && p.nsweeps > 0)
-    rows_run<L, kFloatCmp, kStoreAlways, kRng>(p, rep, lat, thrP, paccP, lane);
+    rows_run<L, kFloatCmp, kStoreAlways, kRng, kCompact>(p, rep, lat, thrP, paccP, lane);
   __syncwarp();
   if (!staged) return;  // the bulk load timed out: flagged, nothing written back
   epilogue_mag(lat + lane, p, N, W, live, rep);
@@ -799,10 +809,10 @@ __global__ void __launch_bounds__(32) k_sweep_multi(const SweepLaunch *groups,
   __syncwarp();
   if (live && p.nsweeps > 0) {
     switch (L) {
-      case 32: rows_run<32, false, true, kRng>(p, rep, dyn, thrP, paccP, lane); break;
-      case 64: rows_run<64, false, true, kRng>(p, rep, dyn, thrP, paccP, lane); break;
-      case 96: rows_run<96, false, true, kRng>(p, rep, dyn, thrP, paccP, lane); break;
-      case 128: rows_run<128, false, true, kRng>(p, rep, dyn, thrP, paccP, lane); break;
+      case 32: rows_run<32, false, true, kRng, true>(p, rep, dyn, thrP, paccP, lane); break;
+      case 64: rows_run<64, false, true, kRng, true>(p, rep, dyn, thrP, paccP, lane); break;
+      case 96: rows_run<96, false, true, kRng, true>(p, rep, dyn, thrP, paccP, lane); break;
+      case 128: rows_run<128, false, true, kRng, true>(p, rep, dyn, thrP, paccP, lane); break;
       case 48: exact_run<48, false, kRng, false>(p, rep, dyn + lane, L, thrP, paccP); break;
       default: exact_run<0, false, kRng, false>(p, rep, dyn + lane, L, thrP, paccP); break;
     }
@@ -1031,7 +1041,17 @@ int dispatch_kind(const SweepLaunch &p, cudaStream_t s) {
       default: break;  // other L: the default kernels
     }
   }
-  if (p.variant == 0) {  // the row kernel writing the centre word back on every attempt
+  if (p.variant == 10 && K == kRngXorwow) {  // variant 0 with one block per loop iteration
+    switch (p.L) {
+      case 32: return launch_rows(k_sweep_rows<32, true, F, K, true, false, true>, p, 0, s);
+      case 64: return launch_rows(k_sweep_rows<64, true, F, K, true, false, true>, p, 0, s);
+      case 96: return launch_rows(k_sweep_rows<96, false, F, K, true, false, true>, p, dyn96, s);
+      case 128:
+        return launch_rows(k_sweep_rows<128, false, F, K, true, false, true>, p, dyn128, s);
+      default: break;
+    }
+  }
+  if (p.variant == 0 || p.variant == 10) {  // the row kernel writing the centre word back on every attempt
     switch (p.L) {
       case 32: return launch_rows(k_sweep_rows<32, true, F, K, true>, p, 0, s);
       case 64: return launch_rows(k_sweep_rows<64, true, F, K, true>, p, 0, s);

@@ -138,8 +138,11 @@ int gasp_grids_shape(const gasp_grids_t *grids, int *L_out, int *ngrids_out);
  * loads and stores (L = 32, 64, 96, 128 in replica order, i.e. without an
  * active list; bit-identical to 0, measured slower; each launch reads back
  * a device flag, so a copy that did not complete within its bounded wait
- * returns GASP_ERR_TIMEOUT).  Values 3, 4 and 8 (retired kernels that were
- * measured slower) and values outside 0..9 return GASP_ERR_INVALID.
+ * returns GASP_ERR_TIMEOUT); 10 variant 0 with one block of attempts per
+ * loop iteration (half the loop's code, for kernels that share an SM's
+ * instruction cache with other kernels -- the batched groups use it; on the
+ * MWC64X stream the same as 0).  Values 3, 4 and 8 (retired kernels that
+ * were measured slower) and values outside 0..10 return GASP_ERR_INVALID.
  * GASP_OPT_WARPS_PER_CTA: tiles per CTA of the generic kernel (1..8).
  * GASP_OPT_TAIL_REPLICAS: device-side committor shooting (itask 1 with
  * compaction) sweeps with variant 6 once at most this many replicas are

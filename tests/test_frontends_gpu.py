@@ -179,18 +179,19 @@ def test_cli_committor_reads_gridinput(ref_gpu, tmp_path):
 @pytest.mark.parametrize("beta,h", [(0.45, 0.1), (0.5, 0.0), (1e-9, 0.1)])
 def test_kernel_variants_agree(L, kind, beta, h):
     """The generic (with and without the every-attempt store), row (with
-    and without it) and bulk-staged kernels give identical results for both
-    RNG kinds (96 replicas: three tiles).  h = 0 leaves six classes that can
-    reject; at beta = 1e-9 every P rounds to 1.0 and ten classes can reject.
-    The retired variants 3, 4 and 8 are refused."""
+    and without it, in blocks of two or one per loop iteration) and
+    bulk-staged kernels give identical results for both RNG kinds (96
+    replicas: three tiles).  h = 0 leaves six classes that can reject; at
+    beta = 1e-9 every P rounds to 1.0 and ten classes can reject.  The
+    retired variants 3, 4 and 8 are refused."""
     ng, seed = 96, 31 + L
     g0 = np.where(np.random.default_rng(seed).random((ng, L, L)) < 0.3, 1, -1).astype(np.int32)
     outs = []
     probe = engine.DeviceGrids(L, ng, g0)
-    for variant in (3, 4, 8, 10, -1):
+    for variant in (3, 4, 8, 11, -1):
         assert lib().gasp_grids_set_option(probe.handle, 1, variant) != 0
     probe.close()
-    for variant in (0, 1, 2, 5, 9):
+    for variant in (0, 1, 2, 5, 9, 10):
         dg = engine.DeviceGrids(L, ng, g0)
         dg.set_option(1, variant)
         r = engine.RngStates(ng, seed, kind=kind)
