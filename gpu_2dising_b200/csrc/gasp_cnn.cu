@@ -1503,7 +1503,8 @@ int cnn_upload(gasp_cnn *c, const int8_t *spins, const float *labels, int batch)
 // are bounded by shared memory (1 KiB reserved per CTA), registers, and TMEM
 // (512 columns, 32 per CTA).
 template <typename Kern>
-int launch_persistent(Kern kern, size_t smem_max, size_t smem, const ConvArgs &b, cudaStream_t s) {
+int launch_persistent(Kern kern, size_t smem_max, size_t smem, const ConvArgs &b, cudaStream_t s,
+                      int tmem_cols = 32) {
   GASP_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max));
   int dev = 0, nsm = 0, smem_sm = 0;
   GASP_CUDA(cudaGetDevice(&dev));
@@ -1514,7 +1515,9 @@ int launch_persistent(Kern kern, size_t smem_max, size_t smem, const ConvArgs &b
   GASP_CUDA(cudaFuncGetAttributes(&fa, kern));
   const int by_regs = fa.numRegs > 0 ? 65536 / (fa.numRegs * 128) : 16;
   if (per_sm > by_regs) per_sm = by_regs;
-  if (per_sm > 16) per_sm = 16;  // 2048 threads per SM; also all TMEM (16 x 32 columns)
+  if (per_sm > 16) per_sm = 16;  // 2048 threads per SM
+  // every resident CTA holds its TMEM columns until it exits (512 per SM)
+  if (per_sm > 512 / tmem_cols) per_sm = 512 / tmem_cols;
   if (per_sm < 1) per_sm = 1;
   const int grid = b.ntiles < nsm * per_sm ? b.ntiles : nsm * per_sm;
   kern<<<grid, 128, smem, s>>>(b);
@@ -1565,7 +1568,7 @@ int launch_conv(const ConvArgs &a, int batch, cudaStream_t s) {
     if (a.L == 64 && conv_gh64_enabled()) {  // one staged window copy (ghost columns)
       b.ntiles = batch * kGhTiles;
       return launch_persistent(k_conv_gh64, conv_gh64_smem(true), conv_gh64_smem(a.pool != nullptr),
-                               b, s);
+                               b, s, 64);
     }
   }
   if constexpr (MODE != kFwd1) {
