@@ -449,8 +449,8 @@ __device__ __forceinline__ void pattern_tables(const SweepLaunch &p, uint32_t *t
   paccP[lane] = p.pacc_f[2 * cls];
 }
 
-// The L=64 row kernel on the reference stream (integer thresholds, centre
-// word written back on every attempt) runs its attempts in blocks of K, each
+// The L=64 row kernel (integer thresholds, centre word written back on every
+// attempt; both streams) runs its attempts in blocks of K, each
 // in two phases: row_draw64 takes the block's 2K draws in the reference's
 // order (site, acceptance, site, ...) and each site's word offset, then
 // row_apply64 applies the K attempts in order.  The applies form a chain of
@@ -473,8 +473,10 @@ __device__ __forceinline__ void pattern_tables(const SweepLaunch &p, uint32_t *t
 // row_attempt loop: 4.41e11).  Blocks of 8 or 32, the up/down offsets
 // computed in the draw phase, the next block's draws interleaved with this
 // block's applies, and starting odd tiles half a block ahead were all
-// slower; the MWC64X instantiation keeps the unrolled loop (blocks: 4.87e11
-// against 4.92e11); with the marks below, blocks of 8 (4.50e11) or 32
+// slower.  On the MWC64X stream (site = the draw's top 12 bits, an exact
+// integer already): 5.11e11 against 4.91e11 for its unrolled loop (one block
+// per iteration without the marks had been slower, 4.87e11).  With the
+// marks below, blocks of 8 (4.50e11) or 32
 // (4.46e11), a second set of marks before the applies (4.50e11), a store
 // only on acceptance (4.35e11), a two-compare row window (4.51e11), four
 // blocks per iteration (2.7e11) and a register cap of 80 (4.42e11) were
@@ -504,8 +506,11 @@ __device__ __forceinline__ void row_draw64(Rng &rg, uint32_t (&offc)[K], uint32_
   block_marks();
 #pragma unroll
   for (int j = 0; j < K; ++j) {
-    const uint32_t sb =
-        __float_as_uint(__fadd_rd(shrink * _curand_uniform(rg.next()), 8388608.0f));
+    uint32_t sb;
+    if constexpr (Rng::kKind == kRngXorwow)
+      sb = __float_as_uint(__fadd_rd(shrink * _curand_uniform(rg.next()), 8388608.0f));
+    else  // MWC64X: the draw's top 12 bits (N = 4096)
+      sb = rg.template site<N>(shrink, N);
     x2[j] = rg.next();
     offc[j] = ((sb << 2) & kMask) | lane4;
     sbits[j] = sb;
@@ -663,7 +668,7 @@ __device__ __forceinline__ void rows_run(const SweepLaunch &p, int rep, const ui
   const float shrink = (1.0f - FLT_EPSILON) * (float)N;
   const uint32_t lane4 = (uint32_t)lane << 2;
   const int total = N * p.nsweeps;
-  if constexpr (L == 64 && kRng == kRngXorwow && !kFloatCmp && kStoreAlways) {
+  if constexpr (L == 64 && !kFloatCmp && kStoreAlways) {
     // the default L=64 kernel on the reference stream: blocks of 16 attempts
     // (total = 4096 * nsweeps is a multiple of 16)
     uint32_t offc[16], sbits[16], x2[16];
@@ -1041,7 +1046,7 @@ int dispatch_kind(const SweepLaunch &p, cudaStream_t s) {
       default: break;  // other L: the default kernels
     }
   }
-  if (p.variant == 10 && K == kRngXorwow) {  // variant 0 with one block per loop iteration
+  if (p.variant == 10) {  // variant 0 with one block per loop iteration
     switch (p.L) {
       case 32: return launch_rows(k_sweep_rows<32, true, F, K, true, false, true>, p, 0, s);
       case 64: return launch_rows(k_sweep_rows<64, true, F, K, true, false, true>, p, 0, s);

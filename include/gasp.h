@@ -141,7 +141,7 @@ int gasp_grids_shape(const gasp_grids_t *grids, int *L_out, int *ngrids_out);
  * returns GASP_ERR_TIMEOUT); 10 variant 0 with one block of attempts per
  * loop iteration (half the loop's code, for kernels that share an SM's
  * instruction cache with other kernels -- the batched groups use it; on the
- * MWC64X stream the same as 0).  Values 3, 4 and 8 (retired kernels that
+ * MWC64X stream it differs from 0 only at L = 64).  Values 3, 4 and 8 (retired kernels that
  * were measured slower) and values outside 0..10 return GASP_ERR_INVALID.
  * GASP_OPT_WARPS_PER_CTA: tiles per CTA of the generic kernel (1..8).
  * GASP_OPT_TAIL_REPLICAS: device-side committor shooting (itask 1 with
