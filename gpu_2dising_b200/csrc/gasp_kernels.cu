@@ -555,8 +555,9 @@ __device__ __forceinline__ void row_apply64(const uint32_t (&offc)[K], const uin
 // +3.6 % (32768; 16384: -0.3 %); the uneven batch 3 % faster on both its
 // paths.  Two blocks per iteration then gave L=32 a further 3.9 % and, with
 // the site's row loaded first, L=128 3.3 %; L=96 lost 4-10 % with either.
-// The MWC64X instantiations keep the unrolled loop (blocks: -0.5 to -2 % at
-// most sizes).
+// On the MWC64X stream the final form gives L=32 +5 % (16384 replicas) to
+// +9 % (32768) and L=128 +2 % over the unrolled loop; L=96 keeps that loop
+// (blocks: -1.9 %).
 
 // Word part of a byte offset into a tile image of 4N bytes, rounded up to a
 // power of two (the offset of the site's word is (site << 2) under it).
@@ -570,14 +571,17 @@ __host__ __device__ constexpr uint32_t row_word_mask() {
 template <int L, int K, typename Rng>
 __device__ __forceinline__ void row_draw(Rng &rg, uint32_t (&offc)[K], uint32_t (&sbits)[K],
                                          uint32_t (&x2)[K], uint32_t lane4, float shrink) {
-  static_assert(Rng::kKind == kRngXorwow, "reference stream");
   static_assert(L * L <= (1 << 15), "site bits and word offsets below 2^17");
+  constexpr int N = L * L;
   constexpr uint32_t kMaskD = row_word_mask<L>();
   block_marks();
 #pragma unroll
   for (int j = 0; j < K; ++j) {
-    const uint32_t sb =
-        __float_as_uint(__fadd_rd(shrink * _curand_uniform(rg.next()), 8388608.0f));
+    uint32_t sb;
+    if constexpr (Rng::kKind == kRngXorwow)
+      sb = __float_as_uint(__fadd_rd(shrink * _curand_uniform(rg.next()), 8388608.0f));
+    else  // MWC64X: the exact integer site (power-of-two N: top bits; L=96: high product)
+      sb = rg.template site<N>(shrink, N);
     x2[j] = rg.next();
     offc[j] = ((sb << 2) & kMaskD) | lane4;
     sbits[j] = sb;
@@ -689,7 +693,8 @@ __device__ __forceinline__ void rows_run(const SweepLaunch &p, int rep, const ui
     rg.store(p.rng, p.rng_stride, rep);
     return;
   }
-  if constexpr (L != 64 && kRng == kRngXorwow && !kFloatCmp && kStoreAlways) {
+  // (MWC64X at L=96 keeps the unrolled loop: blocks -1.9 %)
+  if constexpr (L != 64 && (kRng == kRngXorwow || L != 96) && !kFloatCmp && kStoreAlways) {
     // blocks of 16 attempts (total = L * L * nsweeps, a multiple of 16 for
     // L = 32, 96, 128)
     uint32_t offc[16], sbits[16], x2[16];
