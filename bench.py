@@ -241,10 +241,14 @@ def run_reference(args, rank, world):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * run["wall_s"] / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "i32",
         "data": "synthetic (all-down L=64 lattices, seeded MT19937 per process)",
-        "config": {"workload": f"plain reversal on the CPU: L=64, beta=0.54, h=0.07, all-down, "
-                               f"{run['replicas']} replicas, {run['sweeps']} sweeps, "
-                               f"magnetisation checked every {CPU_CONFIG['mag_output_int']}",
-                   **CPU_CONFIG},
+        # the same workload as this script's own line (the same system: L=64,
+        # beta=0.54, h=0.07, all-down), timed on a bounded sample of it -- the
+        # CPU configuration, described by "cpu_config" and the sample text
+        "config": CONFIG,
+        "cpu_config": {"workload": f"plain reversal on the CPU: L=64, beta=0.54, h=0.07, "
+                                   f"all-down, {run['replicas']} replicas, {run['sweeps']} "
+                                   f"sweeps, magnetisation checked every "
+                                   f"{CPU_CONFIG['mag_output_int']}", **CPU_CONFIG},
         "impl": "reference",
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": run["cores"], "kind": "reference",
                          "sample": sample},

@@ -28,7 +28,11 @@ def test_reference_arm_prints_contract_line():
     assert line["value"] > 0 and line["higher_is_better"] is True
     assert line["warmup"] >= 3 and line["steps"] == 2 and len(line["step_ms"]) == 2
     assert line["n_gpus"] == 1
-    assert line["config"]["replicas"] == 48 and line["config"]["sweeps"] == 300
+    # the same workload config as the GPU arm's line, timed on the CPU sample
+    sys.path.insert(0, REPO)
+    import bench
+    assert line["config"] == bench.CONFIG
+    assert line["cpu_config"]["replicas"] == 48 and line["cpu_config"]["sweeps"] == 300
     cpu = line["cpu_baseline"]
     assert cpu["kind"] == "reference" and cpu["cores"] >= 1 and cpu["value"] == line["value"]
     assert "mc_driver_cpu" in cpu["sample"]
