@@ -199,6 +199,21 @@ __device__ __forceinline__ uint32_t bit_at(const uint32_t *my, int s) {
   return (my[(s >> 5) * kTile] >> (s & 31)) & 1u;
 }
 
+// Five opaque register constants materialised at the top of each block.
+// They take no part in the arithmetic; they change how the compiler orders
+// a block's draws against the previous block's applies.  Measured: 4.57-4.59e11
+// attempts/s with them, 4.48e11 without, 4.47-4.55e11 with 1, 2, 3 or 8 of
+// them or with an empty asm statement or a memory clobber instead.  Results
+// are bit-identical either way.
+__device__ __forceinline__ void block_marks() {
+  [[maybe_unused]] uint32_t m0, m1, m2, m3, m4;
+  asm volatile("mov.u32 %0, 16;" : "=r"(m0));
+  asm volatile("mov.u32 %0, 2;" : "=r"(m1));
+  asm volatile("mov.u32 %0, 1073741824;" : "=r"(m2));
+  asm volatile("mov.u32 %0, 1;" : "=r"(m3));
+  asm volatile("mov.u32 %0, 362437;" : "=r"(m4));
+}
+
 __device__ __forceinline__ void epilogue_mag(const uint32_t *my, const SweepLaunch &p, int N,
                                              int W, bool live, int rep) {
   if (p.mag_out != nullptr && live) {
@@ -218,11 +233,44 @@ __device__ __forceinline__ void exact_run(const SweepLaunch &p, int rep, uint32_
   RngPolicy<kRng> rg;
   rg.load(p.rng, p.rng_stride, rep);
   const float shrink = (1.0f - FLT_EPSILON) * (float)N;
-  for (int sw = 0; sw < p.nsweeps; ++sw) {
-    // unroll 4: 1.2-1.5x over the compiler's choice on the reference stream
-    // (L=48: 2.45e11 vs 2.04e11 attempts/s at 32768 replicas; L=100: 3.3e10 vs 2.2e10)
-#pragma unroll 4
-    for (int a = 0; a < N; ++a) {
+  // MWC64X stream: attempts in blocks of 16, the block's 32 draws first (see
+  // row_draw64), flat over all attempts of the batch.  Measured against the
+  // per-sweep loop below: L=20 +9 %, L=48 +2 to +5 %, L=100 +18 % (4096 and
+  // 32768 replicas); on the XORWOW stream the blocks were slower (L=48 -29 %,
+  // L=100 -2 %), so that stream keeps the loop below.
+  if constexpr (!kFloatCmp && kRng == kRngMwc) {
+    const int total = N * p.nsweeps;
+    int a = 0;
+    for (; a + 16 <= total; a += 16) {
+      uint32_t ss[16], xx[16];
+      block_marks();
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        ss[j] = rg.template site<(L_ > 0 ? L_ * L_ : 0)>(shrink, N);
+        xx[j] = rg.next();
+      }
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        const int s = (int)ss[j];
+        const int row = s / L;
+        const int col = s - row * L;
+        const int su = row == 0 ? s + N - L : s - L;
+        const int sd = row == L - 1 ? s - N + L : s + L;
+        const int sl = col == 0 ? s + L - 1 : s - 1;
+        const int sr = col == L - 1 ? s - L + 1 : s + 1;
+        const uint32_t wc = my[(s >> 5) * kTile];
+        const uint32_t bs = (wc >> (s & 31)) & 1u;
+        const uint32_t k = bit_at(my, su) + bit_at(my, sd) + bit_at(my, sl) + bit_at(my, sr);
+        const uint32_t cls = 5u * bs + k;
+        const bool acc = xx[j] <= thr_s[cls];
+        if constexpr (kStoreAlways) {
+          my[(s >> 5) * kTile] = acc ? wc ^ (1u << (s & 31)) : wc;
+        } else {
+          if (acc) my[(s >> 5) * kTile] = wc ^ (1u << (s & 31));
+        }
+      }
+    }
+    for (; a < total; ++a) {
       const int s = (int)rg.template site<(L_ > 0 ? L_ * L_ : 0)>(shrink, N);
       const int row = s / L;
       const int col = s - row * L;
@@ -235,16 +283,42 @@ __device__ __forceinline__ void exact_run(const SweepLaunch &p, int rep, uint32_
       const uint32_t k = bit_at(my, su) + bit_at(my, sd) + bit_at(my, sl) + bit_at(my, sr);
       const uint32_t cls = 5u * bs + k;
       const uint32_t x2 = rg.next();
-      bool acc;
-      if (kFloatCmp) {
-        acc = _curand_uniform(x2) < pacc_s[2 * cls];  // index 10*bs + 2k
-      } else {
-        acc = x2 <= thr_s[cls];
-      }
-      if constexpr (kStoreAlways) {  // written back unchanged when rejected: no branch
+      const bool acc = x2 <= thr_s[cls];
+      if constexpr (kStoreAlways) {
         my[(s >> 5) * kTile] = acc ? wc ^ (1u << (s & 31)) : wc;
       } else {
         if (acc) my[(s >> 5) * kTile] = wc ^ (1u << (s & 31));
+      }
+    }
+  } else {
+    for (int sw = 0; sw < p.nsweeps; ++sw) {
+      // unroll 4: 1.2-1.5x over the compiler's choice on the reference stream
+      // (L=48: 2.45e11 vs 2.04e11 attempts/s at 32768 replicas; L=100: 3.3e10 vs 2.2e10)
+#pragma unroll 4
+      for (int a = 0; a < N; ++a) {
+        const int s = (int)rg.template site<(L_ > 0 ? L_ * L_ : 0)>(shrink, N);
+        const int row = s / L;
+        const int col = s - row * L;
+        const int su = row == 0 ? s + N - L : s - L;
+        const int sd = row == L - 1 ? s - N + L : s + L;
+        const int sl = col == 0 ? s + L - 1 : s - 1;
+        const int sr = col == L - 1 ? s - L + 1 : s + 1;
+        const uint32_t wc = my[(s >> 5) * kTile];
+        const uint32_t bs = (wc >> (s & 31)) & 1u;
+        const uint32_t k = bit_at(my, su) + bit_at(my, sd) + bit_at(my, sl) + bit_at(my, sr);
+        const uint32_t cls = 5u * bs + k;
+        const uint32_t x2 = rg.next();
+        bool acc;
+        if (kFloatCmp) {
+          acc = _curand_uniform(x2) < pacc_s[2 * cls];  // index 10*bs + 2k
+        } else {
+          acc = x2 <= thr_s[cls];
+        }
+        if constexpr (kStoreAlways) {  // written back unchanged when rejected: no branch
+          my[(s >> 5) * kTile] = acc ? wc ^ (1u << (s & 31)) : wc;
+        } else {
+          if (acc) my[(s >> 5) * kTile] = wc ^ (1u << (s & 31));
+        }
       }
     }
   }
@@ -482,20 +556,6 @@ __device__ __forceinline__ void pattern_tables(const SweepLaunch &p, uint32_t *t
 // blocks per iteration (2.7e11) and a register cap of 80 (4.42e11) were
 // slower.
 
-// Five opaque register constants materialised at the top of each block.
-// They take no part in the arithmetic; they change how the compiler orders
-// a block's draws against the previous block's applies.  Measured: 4.57-4.59e11
-// attempts/s with them, 4.48e11 without, 4.47-4.55e11 with 1, 2, 3 or 8 of
-// them or with an empty asm statement or a memory clobber instead.  Results
-// are bit-identical either way.
-__device__ __forceinline__ void block_marks() {
-  [[maybe_unused]] uint32_t m0, m1, m2, m3, m4;
-  asm volatile("mov.u32 %0, 16;" : "=r"(m0));
-  asm volatile("mov.u32 %0, 2;" : "=r"(m1));
-  asm volatile("mov.u32 %0, 1073741824;" : "=r"(m2));
-  asm volatile("mov.u32 %0, 1;" : "=r"(m3));
-  asm volatile("mov.u32 %0, 362437;" : "=r"(m4));
-}
 
 template <int L, int K, typename Rng>
 __device__ __forceinline__ void row_draw64(Rng &rg, uint32_t (&offc)[K], uint32_t (&sbits)[K],
