@@ -75,7 +75,13 @@ struct GridsExtra {
   int variant = 0;          // GASP_OPT_SWEEP_VARIANT
   int warps_per_cta = 1;    // GASP_OPT_WARPS_PER_CTA
   int tail_replicas = -1;   // GASP_OPT_TAIL_REPLICAS (-1: the stream's default)
+  int *d_upchunk = nullptr; // int32 staging of whole-set uploads, kUploadChunk replicas
 };
+
+// Replicas per chunk of a whole-set upload without the set's int32 buffer
+// (16 MiB at L=64): allocating a set-sized int32 buffer (512 MiB at L=64 x
+// 32768) cost 5-30 ms on a B200, two to three times the copy itself.
+constexpr int kUploadChunk = 1024;
 
 // Extra state kept beside the public struct (allocated with it).
 struct GridsImpl {
@@ -313,6 +319,7 @@ int gasp_free_grid(gasp_grids_t *g) {
   cudaFree(im->x.d_active);
   cudaFree(im->x.d_lclus);
   cudaFree(im->x.d_cwork);
+  cudaFree(im->x.d_upchunk);
   delete im;
   return GASP_OK;
 }
@@ -327,8 +334,29 @@ int gasp_grids_upload(gasp_grids_t *g, const int *host_grids) {
   if (!g || !host_grids) return GASP_ERR_INVALID;
   int rc = check_device_of(g->device);
   if (rc) return rc;
-  if ((rc = ensure_scratch32(g))) return rc;
   cudaStream_t s = current_stream();
+  if (!g->d_scratch32) {
+    // No set-sized int32 buffer yet: upload in chunks of kUploadChunk
+    // replicas through one reusable staging buffer, each chunk copied then
+    // packed into its tiles (stream order keeps a chunk's copy behind the
+    // previous chunk's pack); the copies run at the full host-to-device rate.
+    GridsExtra &x = impl(g)->x;
+    const int chunk = g->ngrids < kUploadChunk ? g->ngrids : kUploadChunk;
+    if (!x.d_upchunk) GASP_CUDA(cudaMalloc(&x.d_upchunk, (size_t)chunk * g->N * sizeof(int)));
+    for (int r0 = 0; r0 < g->ngrids; r0 += chunk) {
+      const int n = g->ngrids - r0 < chunk ? g->ngrids - r0 : chunk;
+      GASP_CUDA(cudaMemcpyAsync(x.d_upchunk, host_grids + (size_t)r0 * g->N,
+                                (size_t)n * g->N * sizeof(int), cudaMemcpyHostToDevice, s));
+      // kUploadChunk is a multiple of the 32-replica tile: chunks start on tiles
+      rc = launch_pack_grids(x.d_upchunk, g->d_lat + (size_t)(r0 / kTile) * g->W * kTile, g->L,
+                             n, s);
+      if (rc) break;
+    }
+    const cudaError_t se = cudaStreamSynchronize(s);
+    if (rc) return rc;
+    if (se != cudaSuccess) return cuda_fail(se, "cudaStreamSynchronize", __FILE__, __LINE__);
+    return GASP_OK;
+  }
   GASP_CUDA(cudaMemcpyAsync(g->d_scratch32, host_grids, (size_t)g->ngrids * g->N * sizeof(int),
                             cudaMemcpyHostToDevice, s));
   rc = launch_pack_grids(g->d_scratch32, g->d_lat, g->L, g->ngrids, s);
