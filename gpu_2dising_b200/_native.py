@@ -53,7 +53,8 @@ EXPORTED = (
     "gasp_init_grids_uniform", "gasp_init_grids_from_file", "gasp_init_grids_from_array",
     "gasp_init_fates", "gasp_read_input_grid", "gasp_write_ising_grids",
     "gasp_write_packed_frame", "gasp_bootstrap_errbar", "gasp_committor_from_fates",
-    "gasp_read_frame", "gasp_write_input_grid", "gasp_checkpoint_save", "gasp_checkpoint_info",
+    "gasp_read_frame", "gasp_write_input_grid", "gasp_create_ising_grids_hdf5",
+    "gasp_write_ising_grids_hdf5", "gasp_checkpoint_save", "gasp_checkpoint_info",
     "gasp_checkpoint_load",
     "gasp_batch_create", "gasp_batch_free", "gasp_batch_swarm", "gasp_batch_autotune",
     "gasp_batch_layout",
@@ -175,6 +176,9 @@ def _bind(lib):
         "gasp_read_frame": (I, [C.c_char_p, I, C.POINTER(C.c_int), C.POINTER(C.c_int),
                                 C.POINTER(C.c_int), C.c_void_p, C.c_longlong]),
         "gasp_write_input_grid": (I, [C.c_char_p, I, _i32p]),
+        "gasp_create_ising_grids_hdf5": (I, [I, I, I, C.c_double, C.c_double, I, C.c_char_p]),
+        "gasp_write_ising_grids_hdf5": (I, [I, I, _i32p, I, P, P, C.c_char_p, C.c_double,
+                                            C.c_double, C.c_char_p]),
         "gasp_checkpoint_save": (I, [C.c_char_p, P, P, C.c_void_p, I]),
         "gasp_checkpoint_info": (I, [C.c_char_p] + [C.POINTER(C.c_int)] * 5),
         "gasp_checkpoint_load": (I, [C.c_char_p, P, P, C.c_void_p, C.POINTER(C.c_int)]),

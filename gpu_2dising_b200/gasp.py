@@ -8,12 +8,13 @@
 
 Same entry points, keyword names, defaults, validation errors and return
 values; the module-level ``grids`` / ``magnetisation`` / ``largest_cluster``
-lists and ``gpu_nsms`` behave as in the reference.  Differences, all
-deliberate:
+lists and ``gpu_nsms`` behave as in the reference, and every grid dump is
+written to the HDF5 side file (gridstates.hdf5 for swarms, pBgrids.hdf5 for
+committor runs, created at the start of each run) by the library's own
+writer, which follows the HDF5 file format specification without libhdf5
+(src/io.c:132-301).  Differences, all deliberate:
 
 * there is no CPU fallback: without a CUDA device the calls raise;
-* the HDF5 side files (gridstates.hdf5 / pBgrids.hdf5) are not written
-  (HDF5 is not a dependency of this library);
 * with ``cv='largest_cluster'`` and thresholds below 2 in magnitude a
   UserWarning is issued through ``warnings`` (the reference sets the warning
   as a pending exception, src/ising_ext.cu:572-577);
@@ -99,16 +100,30 @@ def _reset_lists():
 
 
 class _History:
-    """The snapshot store of append_grids_list (src/ising_ext.cu:280-463)."""
+    """The grid-output callback of PyGASP, append_grids_list
+    (src/ising_ext.cu:280-463): module lists, the HDF5 side file, the
+    snapshot store."""
 
-    def __init__(self, keep, maxhist, L):
+    def __init__(self, keep, maxhist, L, cv="magnetisation", h5file=None):
         self.keep, self.maxhist, self.L = keep, maxhist, L
+        self.cv, self.h5file = cv, h5file
         self.ihist = 0
+        self.error = None
 
     def __call__(self, L, ngrids, g, isweep, mag, dn, up, lclus=None):
         magnetisation.append([float(x) for x in mag])
         if lclus is not None:  # recorded only when it is the cv (src/ising_ext.cu:331-357)
             largest_cluster.append([float(x) for x in lclus])
+        if self.h5file is not None:  # always written (src/ising_ext.cu:360-366)
+            mag32 = np.ascontiguousarray(mag, np.float32)
+            lc32 = None if lclus is None else np.ascontiguousarray(lclus, np.float32)
+            rc = lib().gasp_write_ising_grids_hdf5(
+                L, ngrids, np.ascontiguousarray(g, np.int32).reshape(-1), isweep,
+                mag32.ctypes.data, None if lc32 is None else lc32.ctypes.data,
+                self.cv.encode(), dn, up, self.h5file.encode())
+            if rc != 0:
+                self.error = RuntimeError("Error writing HDF5 file")
+                return 1
         if not self.keep or self.ihist >= self.maxhist:
             return 0
         snaps = []
@@ -130,6 +145,24 @@ class _History:
         if snaps:
             grids.append(snaps)
         return 0
+
+
+def _create_h5(L, ngrid, tot_nsweeps, h, beta, itask, path):
+    """create_ising_grids_hdf5 at the start of a run (src/ising_ext.cu:659-660,
+    :1025-1026); a failure is reported on stderr and the run goes on, as in
+    the reference."""
+    lib().gasp_create_ising_grids_hdf5(L, ngrid, tot_nsweeps, h, beta, itask, path.encode())
+
+
+def _run(hist, **kw):
+    """engine.run_driver, raising the output callback's own error if it stopped
+    the run."""
+    try:
+        return engine.run_driver(**kw)
+    except GaspError:
+        if hist.error is not None:
+            raise hist.error from None
+        raise
 
 
 def _require_device():
@@ -173,15 +206,17 @@ def run_nucleation_swarm(L, ngrid, tot_nsweeps, beta, h, initial_spin=-1, cv="ma
     _reset_lists()
     nsnaps = tot_nsweeps // grid_output_int + 1
     maxhist = max_keep_grids if max_keep_grids else nsnaps * ngrid
-    hist = _History(bool(keep_grids), maxhist, L)
+    hist = _History(bool(keep_grids), maxhist, L, cv, "gridstates.hdf5")
     host = np.full((ngrid, L, L), int(initial_spin), np.int32)
     engine.select_gpu_method(L, ngrid, threadsPerBlock)  # evaluated, then ignored (as :678)
     seed = int(time.time()) if seed is None else int(seed)
+    _create_h5(L, ngrid, tot_nsweeps, h, beta, 0, hist.h5file)
     dg = engine.DeviceGrids(L, ngrid, host)
     rng = engine.RngStates(ngrid, seed, kind=_rng_kind(rng))
     try:
-        res, _, _, _ = engine.run_driver(
-            dg, rng, beta, h, tot_nsweeps, mag_output_int, grid_output_int, itask=0,
+        res, _, _, _ = _run(
+            hist, dgrids=dg, rng=rng, beta=beta, h=h, tot_nsweeps=tot_nsweeps,
+            mag_output_int=mag_output_int, grid_output_int=grid_output_int, itask=0,
             dn_thr=dn_threshold, up_thr=up_threshold, host_grids=host,
             outfunc=lambda L_, ng_, g, isweep, m, *lc: hist(L_, ng_, g, isweep, m, dn_threshold,
                                                              up_threshold, *lc),
@@ -243,7 +278,7 @@ def run_committor_calc(L, ngrid, tot_nsweeps, beta, h, initial_spin=-1, cv="magn
     _reset_lists()
     nsnaps = tot_nsweeps // grid_output_int + 1
     maxhist = max_keep_grids if max_keep_grids else nsnaps * ngrid
-    hist = _History(bool(keep_grids), maxhist, L)
+    hist = _History(bool(keep_grids), maxhist, L, cv, "pBgrids.hdf5")
     host = np.empty((ngrid, L, L), np.int32)
     if grid_input == "gridstates.bin":
         rc = lib().gasp_init_grids_from_file(b"gridinput.bin", L, ngrid, host.reshape(-1))
@@ -258,11 +293,13 @@ def run_committor_calc(L, ngrid, tot_nsweeps, beta, h, initial_spin=-1, cv="magn
     fates = np.full(ngrid, -1, np.int32)
     engine.select_gpu_method(L, ngrid, threadsPerBlock)
     seed = int(time.time()) if seed is None else int(seed)
+    _create_h5(L, ngrid, tot_nsweeps, h, beta, 1, hist.h5file)
     dg = engine.DeviceGrids(L, ngrid, host)
     rng = engine.RngStates(ngrid, seed, kind=_rng_kind(rng))
     try:
-        res, fates, _, _ = engine.run_driver(
-            dg, rng, beta, h, tot_nsweeps, mag_output_int, grid_output_int, itask=1,
+        res, fates, _, _ = _run(
+            hist, dgrids=dg, rng=rng, beta=beta, h=h, tot_nsweeps=tot_nsweeps,
+            mag_output_int=mag_output_int, grid_output_int=grid_output_int, itask=1,
             dn_thr=dn_threshold, up_thr=up_threshold, ninputs=count, host_grids=host,
             fates=fates, compact=compact,
             outfunc=lambda L_, ng_, g, isweep, m, *lc: hist(L_, ng_, g, isweep, m, dn_threshold,

@@ -440,6 +440,30 @@ int gasp_read_frame(const char *path, int iframe, int *L_out, int *ngrids_out, i
  * reads.  path NULL: "gridinput.bin". */
 int gasp_write_input_grid(const char *path, int L, const int *grid);
 
+/* Replaces create_ising_grids_hdf5 (include/io.h, src/io.c:132-199), the
+ * PyGASP side file gridstates.hdf5 / pBgrids.hdf5, written without libhdf5
+ * (csrc/gasp_hdf5.c follows the HDF5 file format specification: version 0
+ * superblock, version 1 object headers, symbol-table groups): creates or
+ * truncates filename with the scalars L, ngrids, tot_nsweeps (int32), h,
+ * beta (double) and total_saved_grids = 0.  itask is accepted and unused.
+ * GASP_ERR_IO (and the reference's stderr message) if the file cannot be
+ * created. */
+int gasp_create_ising_grids_hdf5(int L, int ngrids, int tot_nsweeps, double h, double beta,
+                                 int itask, const char *filename);
+/* Replaces write_ising_grids_hdf5 (src/io.c:201-301) with its GridOutputFunc
+ * arguments: appends the group /sweep_<isweep> holding grid_<g> (int32
+ * [L][L]) for every replica, each with the string attributes magnetisation
+ * and lclus_size ("%g" of the value, "null" when the array is NULL),
+ * committor and committor_error ("null"), and adds ngrids to
+ * total_saved_grids.  ngrids == 0 writes no group (the reference creates it
+ * and deletes it again).  GASP_ERR_IO if the file cannot be opened or
+ * already holds /sweep_<isweep>; GASP_ERR_FORMAT if it was not made by
+ * gasp_create_ising_grids_hdf5. */
+int gasp_write_ising_grids_hdf5(int L, int ngrids, const int *ising_grids, int isweep,
+                                const float *magnetisation, const float *lclus_size,
+                                const char *cv, double dn_thr, double up_thr,
+                                const char *filename);
+
 /* ----------------------------------------------------------- checkpoints */
 /* Checkpoint / resume of a run's state (no reference counterpart; the
  * reference can only restart from gridinput.bin, src/io.c:4-65): the grids,

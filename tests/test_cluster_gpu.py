@@ -146,5 +146,12 @@ def test_pygasp_swarm_with_largest_cluster(ref_gpu, tmp_path, monkeypatch):
                               fl[k * ng:(k + 1) * ng])
     snaps = [s for frame in gasp.grids for s in frame]
     assert snaps and all(dn < s.lclus_size < up for s in snaps)
+    import h5read
+    f = h5read.read("gridstates.hdf5")
+    assert f["total_saved_grids"].value == n * ng
+    for k in range(n):
+        grp = f[f"sweep_{k * grid}"]
+        assert [grp[f"grid_{i}"].attrs["lclus_size"] for i in range(ng)] == \
+            ["%g" % x for x in gasp.largest_cluster[k]]
     with pytest.warns(UserWarning):
         gasp.run_nucleation_swarm(16, 32, 10, beta, h, cv="largest_cluster", seed=1)

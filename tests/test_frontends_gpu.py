@@ -7,6 +7,7 @@ import subprocess
 import numpy as np
 import pytest
 
+import h5read
 import oracle
 from conftest import REPO
 from gpu_2dising_b200 import engine
@@ -61,6 +62,20 @@ def test_pygasp_swarm_matches_reference(ref_gpu, gasp_mod, tmp_path, monkeypatch
         m = oracle.magnetisation_gpu(L, r_fg[i]).astype(np.float64)
         nexp += int(np.count_nonzero((m > dn) & (m < up)))
     assert len(snaps) == nexp
+    # the HDF5 side file: every dump's grids and magnetisations
+    # (src/ising_ext.cu:360-366, src/io.c:201-301)
+    f = h5read.read("gridstates.hdf5")
+    assert (f["L"].value, f["ngrids"].value, f["tot_nsweeps"].value) == (L, ng, tot)
+    assert (f["beta"].value, f["h"].value) == (beta, h)
+    assert f["total_saved_grids"].value == len(r_fi) * ng
+    assert sorted(k for k in f if k.startswith("sweep_")) == sorted(f"sweep_{i}" for i in r_fi)
+    for k, isw in enumerate(r_fi):
+        grp = f[f"sweep_{isw}"]
+        for i in range(ng):
+            assert np.array_equal(grp[f"grid_{i}"].value, r_fg[k][i])
+            assert grp[f"grid_{i}"].attrs == {
+                "magnetisation": "%g" % gasp_mod.magnetisation[k][i], "lclus_size": "null",
+                "committor": "null", "committor_error": "null"}
 
 
 def test_pygasp_committor_matches_reference(ref_gpu, gasp_mod, tmp_path, monkeypatch):
@@ -82,6 +97,12 @@ def test_pygasp_committor_matches_reference(ref_gpu, gasp_mod, tmp_path, monkeyp
             for i in range(2)]
     assert [o[0] for o in out] == [float(x) for x in r_res]
     assert [o[1] for o in out] == errs
+    f = h5read.read("pBgrids.hdf5")
+    ndump = len(gasp_mod.magnetisation)
+    assert f["ngrids"].value == ng and f["total_saved_grids"].value == ndump * ng
+    assert len([k for k in f if k.startswith("sweep_")]) == ndump
+    first = f["sweep_0"]
+    assert all(np.array_equal(first[f"grid_{i}"].value, g0[i]) for i in range(ng))
     # compaction gives the same committors
     oracle.lib().orc_srand(1)
     out2 = gasp_mod.run_committor_calc(L, ng, tot, beta, h, up_threshold=up, dn_threshold=dn,
