@@ -7,7 +7,10 @@
 // D[128 x 32] (FP32, in TMEM) = A[128 x K] (BF16) * B[32 x K]^T (weights,
 // BF16), K = 9 taps * 32 channels = 288 (16 for the first layer).  A is an
 // im2col buffer (k_conv_tc) or, for the 32-channel layers, shifted windows
-// over the tile's staged input rows (k_conv_win).  Operands are K-major in
+// over the tile's staged input rows (k_conv_win, k_conv_gh64).  The first
+// layer (one input channel of +-1 spins) has only 512 distinct input
+// neighbourhoods: k_conv_tc computes their activations once per call and
+// k_conv1_lookup writes each pixel's row of that table.  Operands are K-major in
 // shared memory in the no-swizzle interleaved layout (8-row x 16-byte core
 // matrices); one thread issues K/16 tcgen05.mma (kind::f16, M=128, N=32), a
 // tcgen05.commit arrives on an mbarrier, and every warp reads its 32 rows of D
@@ -132,14 +135,18 @@ __device__ __forceinline__ int nbr(int p, int tap, int L) {
   return yy * L + xx;
 }
 
-enum { kFwd1 = 0, kFwd = 1, kBwd = 2 };
+// kTab1: layer 1 on the 512 patterns of a 3x3 spin neighbourhood (row q of
+// A holds +1 for tap k where bit k of q is set, -1 elsewhere); its outputs are
+// the first layer's activation table (k_conv1_lookup).
+enum { kFwd = 1, kBwd = 2, kTab1 = 3 };
+constexpr int kNPatterns = 512;
 
 struct ConvArgs {
   int L;
-  const int8_t *spins;           // kFwd1: [B][N]
+  const int8_t *spins;           // layer 1 (k_conv1_lookup): [B][N]
   const __nv_bfloat16 *x;        // kFwd: activations in; kBwd: dZ of this layer
   const __nv_bfloat16 *w;        // [32][K] (kBwd: transposed weights)
-  const float *bias;             // kFwd1/kFwd
+  const float *bias;             // kTab1/kFwd
   __nv_bfloat16 *y;              // kFwd: activations out; kBwd: dZ of the previous layer
   const __nv_bfloat16 *mask_src; // kBwd: activations of the previous layer (ReLU mask)
   float *pool;                   // layer 4 forward: per-image channel sums [B][32]
@@ -151,7 +158,7 @@ struct ConvArgs {
 // then loops over 128-pixel tiles (tile = image * tiles_per_image + index).
 template <int MODE>
 __global__ void __launch_bounds__(128) k_conv_tc(ConvArgs a) {
-  constexpr int K = (MODE == kFwd1) ? 16 : 9 * kC;
+  constexpr int K = MODE == kTab1 ? 16 : 9 * kC;
   constexpr int SBO = K * 16;  // bytes between 8-row groups
   extern __shared__ __align__(1024) unsigned char smem[];
   unsigned char *sA = smem;                               // 128 x K bf16
@@ -160,7 +167,7 @@ __global__ void __launch_bounds__(128) k_conv_tc(ConvArgs a) {
   uint32_t *tslot = reinterpret_cast<uint32_t *>(mbar + 1);
   float *red = reinterpret_cast<float *>(tslot + 4);     // [128][33] (pool)
 
-  const int L = a.L, N = L * L;
+  const int L = a.L, N = MODE == kTab1 ? kNPatterns : L * L;
   const int tid = threadIdx.x, warp = tid >> 5;
   const int tiles_per_img = N / kTileM;
 
@@ -193,12 +200,11 @@ __global__ void __launch_bounds__(128) k_conv_tc(ConvArgs a) {
     const int p = p0 + tid;  // this thread's pixel in the epilogue
 
     // ---- stage A (im2col rows of the tile) ----
-    if constexpr (MODE == kFwd1) {
-      const int8_t *sp = a.spins + (size_t)img * N;
+    if constexpr (MODE == kTab1) {
       __align__(16) __nv_bfloat16 v[16];
 #pragma unroll
       for (int k = 0; k < 16; ++k)
-        v[k] = __float2bfloat16_rn(k < 9 ? (float)sp[nbr(p, k, L)] : 0.0f);
+        v[k] = __float2bfloat16_rn(k < 9 ? ((p >> k) & 1 ? 1.0f : -1.0f) : 0.0f);
       *reinterpret_cast<uint4 *>(sA + il_off(tid, 0, SBO)) = *reinterpret_cast<uint4 *>(&v[0]);
       *reinterpret_cast<uint4 *>(sA + il_off(tid, 8, SBO)) = *reinterpret_cast<uint4 *>(&v[8]);
     } else {
@@ -296,6 +302,47 @@ __global__ void __launch_bounds__(128) k_conv_tc(ConvArgs a) {
   if (warp == 0) {
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(32)
                  : "memory");
+  }
+}
+
+// The first layer from its activation table: pixel p's 32 BF16 activations
+// are row q of the table, q the pattern of its 3x3 neighbourhood (bit
+// (dy+1)*3 + (dx+1) set where that spin is +1).  k_conv_tc<kTab1> fills the
+// table with the same A rows (+-1 per tap, zero padding to K = 16), weights,
+// MMA and epilogue as a per-pixel first layer, so the activations equal
+// those of the im2col form (checked byte for byte on the GPU), which has to
+// stage and multiply every pixel of the batch.  This kernel only writes 64
+// bytes per pixel (HBM bound): lane l finds the pattern of pixel base + l,
+// then the warp writes its 32 rows as four 512-byte stretches, lane l taking
+// 16-byte chunk l % 4 of pixel base + 8 i + l / 4 in step i.  Spins other
+// than +1 count as -1.  Grid: x over 256-pixel blocks of an image, y over
+// images (strided when the batch exceeds gridDim.y).
+__global__ void __launch_bounds__(256) k_conv1_lookup(const int8_t *spins,
+                                                      const __nv_bfloat16 *tab,
+                                                      __nv_bfloat16 *y, int L, int batch) {
+  const int N = L * L;
+  const int lane = threadIdx.x & 31;
+  const int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31);  // the warp's first pixel
+  if (base >= N) return;
+  const int p = base + lane;
+  const bool own = p < N;
+  const int pc = own ? p : N - 1;
+  const int r = pc / L, col = pc - r * L;
+  const int rows[3] = {(r == 0 ? L - 1 : r - 1) * L, r * L, (r == L - 1 ? 0 : r + 1) * L};
+  const int cols[3] = {col == 0 ? L - 1 : col - 1, col, col == L - 1 ? 0 : col + 1};
+  const uint4 *tab16 = reinterpret_cast<const uint4 *>(tab);
+  for (int img = blockIdx.y; img < batch; img += gridDim.y) {
+    const int8_t *sp = spins + (size_t)img * N;
+    int q = 0;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) q |= (sp[rows[k / 3] + cols[k % 3]] > 0 ? 1 : 0) << k;
+    uint4 *dst = reinterpret_cast<uint4 *>(y + ((size_t)img * N + base) * kC);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int j = 8 * i + (lane >> 2);  // pixel base + j, chunk lane % 4
+      const int qj = __shfl_sync(0xffffffffu, q, j);
+      if (base + j < N) dst[4 * j + (lane & 3)] = tab16[4 * qj + (lane & 3)];
+    }
   }
 }
 
@@ -997,7 +1044,7 @@ size_t conv_win_smem(int L, bool pool) {
 }
 
 size_t conv_smem(int mode) {
-  const int K = mode == kFwd1 ? 16 : 9 * kC;
+  const int K = mode == kTab1 ? 16 : 9 * kC;
   return (size_t)kTileM * K * 2 + (size_t)kC * K * 2 + 64 + (size_t)kTileM * 33 * 4;
 }
 
@@ -1481,6 +1528,7 @@ struct gasp_cnn {
   cudaStream_t copy_stream;
   cudaEvent_t ev_copied[2], ev_used[2];
   __nv_bfloat16 *d_act[4];  // a1..a4
+  __nv_bfloat16 *d_tab;     // first-layer activations by neighbourhood pattern [512][32]
   __nv_bfloat16 *d_dz[2];   // ping-pong data gradients
   int *d_err;
   int adam_t;
@@ -1571,22 +1619,38 @@ int launch_conv(const ConvArgs &a, int batch, cudaStream_t s) {
                                b, s, 64);
     }
   }
-  if constexpr (MODE != kFwd1) {
-    const size_t win_max = conv_win_smem(a.L, MODE == kFwd);
-    if (win_max <= kWinSmemLimit) {
-      const size_t sm = conv_win_smem(a.L, a.pool != nullptr);
-      switch (a.L) {
-        case 32: return launch_persistent(k_conv_win<MODE, 32>, win_max, sm, b, s);
-        case 64: return launch_persistent(k_conv_win<MODE, 64>, win_max, sm, b, s);
-        case 128: return launch_persistent(k_conv_win<MODE, 128>, win_max, sm, b, s);
-        default: return launch_persistent(k_conv_win<MODE, 0>, win_max, sm, b, s);
-      }
+  const size_t win_max = conv_win_smem(a.L, MODE == kFwd);
+  if (win_max <= kWinSmemLimit) {
+    const size_t sm = conv_win_smem(a.L, a.pool != nullptr);
+    switch (a.L) {
+      case 32: return launch_persistent(k_conv_win<MODE, 32>, win_max, sm, b, s);
+      case 64: return launch_persistent(k_conv_win<MODE, 64>, win_max, sm, b, s);
+      case 128: return launch_persistent(k_conv_win<MODE, 128>, win_max, sm, b, s);
+      default: return launch_persistent(k_conv_win<MODE, 0>, win_max, sm, b, s);
     }
   }
   const size_t smem_max = conv_smem(MODE);
   // the pooling scratch at the end is only touched by the layer that pools
   const size_t smem = a.pool ? smem_max : smem_max - (size_t)kTileM * 33 * 4;
   return launch_persistent(k_conv_tc<MODE>, smem_max, smem, b, s);
+}
+
+// The first layer: its 512-row activation table (four tiles of k_conv_tc on
+// the neighbourhood patterns), then one table row per pixel.
+int launch_conv1(const ConvArgs &a, __nv_bfloat16 *tab, int batch, cudaStream_t s) {
+  ConvArgs t = a;
+  t.y = tab;
+  t.pool = nullptr;
+  t.ntiles = kNPatterns / kTileM;
+  const size_t smem_max = conv_smem(kTab1);
+  int rc = launch_persistent(k_conv_tc<kTab1>, smem_max, smem_max - (size_t)kTileM * 33 * 4, t,
+                             s);
+  if (rc) return rc;
+  const int N = a.L * a.L;
+  const dim3 grid((unsigned)((N + 255) / 256), (unsigned)(batch < 65535 ? batch : 65535));
+  k_conv1_lookup<<<grid, 256, 0, s>>>(a.spins, tab, a.y, a.L, batch);
+  GASP_CUDA(cudaGetLastError());
+  return GASP_OK;
 }
 
 // keep_last: store the last layer's activations (training's ReLU mask); the
@@ -1606,7 +1670,7 @@ int cnn_forward(gasp_cnn *c, int batch, cudaStream_t s, const int8_t *spins = nu
   a.w = c->d_w1;
   a.bias = c->d_params + kOffB1;
   a.y = c->d_act[0];
-  if ((rc = launch_conv<kFwd1>(a, B, s))) return rc;
+  if ((rc = launch_conv1(a, c->d_tab, B, s))) return rc;
   for (int l = 0; l < 3; ++l) {
     a.x = c->d_act[l];
     a.w = c->d_w + l * 9216;
@@ -1821,6 +1885,7 @@ int gasp_cnn_create(int L, int max_batch, gasp_cnn_t **out) {
   A((void **)&c->d_dmean, (size_t)max_batch * kC * sizeof(float));
   A((void **)&c->d_loss, sizeof(float));
   A((void **)&c->d_err, sizeof(int));
+  A((void **)&c->d_tab, (size_t)kNPatterns * kC * sizeof(__nv_bfloat16));
   for (int i = 0; i < 4; ++i) A((void **)&c->d_act[i], act);
   for (int i = 0; i < 2; ++i) A((void **)&c->d_dz[i], act);
   if (e == cudaSuccess) e = cudaMemset(c->d_params, 0, kNParam * sizeof(float));
@@ -1838,7 +1903,7 @@ int gasp_cnn_create(int L, int max_batch, gasp_cnn_t **out) {
 int gasp_cnn_free(gasp_cnn_t *c) {
   if (!c) return GASP_OK;
   void *ptrs[] = {c->d_params, c->d_grad, c->d_m, c->d_v, c->d_w1, c->d_w, c->d_wt, c->d_spins,
-                  c->d_labels, c->d_q, c->d_mag, c->d_pool, c->d_dmean, c->d_loss, c->d_err,
+                  c->d_labels, c->d_q, c->d_mag, c->d_pool, c->d_dmean, c->d_loss, c->d_err, c->d_tab,
                   c->d_act[0], c->d_act[1], c->d_act[2], c->d_act[3], c->d_dz[0], c->d_dz[1]};
   for (void *p : ptrs) cudaFree(p);
   if (c->copy_stream) {
