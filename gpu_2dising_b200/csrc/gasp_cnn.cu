@@ -1473,21 +1473,31 @@ __global__ void k_head(int B, int N, const float *pool, const float *params, con
 }
 
 // dZ4 = dmean / N on every pixel where the layer-4 activation is positive.
-// One thread per 8 channels of a pixel (16-byte loads and stores).
-__global__ void k_dz4(int B, int N, const float *dmean, const __nv_bfloat16 *a4,
-                      __nv_bfloat16 *dz4) {
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;  // 8-channel chunk
-  if (i >= (long long)B * N * (kC / 8)) return;
-  const int c0 = (int)(i % (kC / 8)) * 8;
-  const long long b = i / ((long long)N * (kC / 8));
-  const uint4 av = reinterpret_cast<const uint4 *>(a4)[i];
-  const __nv_bfloat16 *ah = reinterpret_cast<const __nv_bfloat16 *>(&av);
-  const float *dm = dmean + b * kC + c0;
-  __align__(16) __nv_bfloat16 o[8];
+// One thread per 8 channels of a pixel (16-byte loads and stores); grid x
+// over 256-chunk blocks of one image, y over images (strided when the batch
+// exceeds gridDim.y).  A block divides its image's 32 dmean values once, in
+// shared memory (the same division per value as per pixel, so the same
+// bytes, for 32 divisions a block instead of 8 a thread).
+__global__ void __launch_bounds__(256) k_dz4(int B, int N, const float *dmean,
+                                             const __nv_bfloat16 *a4, __nv_bfloat16 *dz4) {
+  __shared__ float q[kC];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;  // chunk within the image
+  const int c0 = (threadIdx.x & (kC / 8 - 1)) * 8;
+  for (int b = blockIdx.y; b < B; b += gridDim.y) {
+    __syncthreads();  // the previous image's quotients are no longer read
+    if (threadIdx.x < kC) q[threadIdx.x] = dmean[(size_t)b * kC + threadIdx.x] / (float)N;
+    __syncthreads();
+    if (i < N * (kC / 8)) {
+      const size_t at = (size_t)b * N * (kC / 8) + i;
+      const uint4 av = reinterpret_cast<const uint4 *>(a4)[at];
+      const __nv_bfloat16 *ah = reinterpret_cast<const __nv_bfloat16 *>(&av);
+      __align__(16) __nv_bfloat16 o[8];
 #pragma unroll
-  for (int e = 0; e < 8; ++e)
-    o[e] = __float2bfloat16_rn(__bfloat162float(ah[e]) > 0.0f ? dm[e] / (float)N : 0.0f);
-  reinterpret_cast<uint4 *>(dz4)[i] = *reinterpret_cast<const uint4 *>(o);
+      for (int e = 0; e < 8; ++e)
+        o[e] = __float2bfloat16_rn(__bfloat162float(ah[e]) > 0.0f ? q[c0 + e] : 0.0f);
+      reinterpret_cast<uint4 *>(dz4)[at] = *reinterpret_cast<const uint4 *>(o);
+    }
+  }
 }
 
 // BF16 copies of the weights: W1 [32][16] (taps padded), W2..4 [32][288]
@@ -1808,8 +1818,8 @@ int cnn_backward(gasp_cnn *c, int batch, cudaStream_t s) {
   k_head<<<(B + 7) / 8, 256, 0, s>>>(B, N, c->d_pool, c->d_params, c->d_labels, c->d_q, c->d_loss,
                                      c->d_grad, c->d_dmean);
   GASP_CUDA(cudaGetLastError());
-  const long long tot = (long long)B * N * (kC / 8);
-  k_dz4<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(B, N, c->d_dmean, c->d_act[3], c->d_dz[0]);
+  const dim3 gz((unsigned)((N * (kC / 8) + 255) / 256), (unsigned)(B < 65535 ? B : 65535));
+  k_dz4<<<gz, 256, 0, s>>>(B, N, c->d_dmean, c->d_act[3], c->d_dz[0]);
   GASP_CUDA(cudaGetLastError());
   int cur = 0;
   int dev = 0, nsm = 148;
