@@ -1,8 +1,9 @@
 """A small HDF5 reader for the tests, written from the HDF5 file format
-specification (version 0/1 superblocks, version 1 object headers,
-symbol-table groups, contiguous and compact layouts, fixed-point, floating
-point, fixed-length and variable-length string types, version 1/2
-dataspaces, version 1 attributes, global heap collections).
+specification (version 0/1 superblocks, after a user block or not, version 1
+object headers, symbol-table groups, contiguous layouts (layout messages
+versions 1 to 3) and compact ones, fixed-point, floating point, fixed-length
+and variable-length string types, version 1/2 dataspaces, version 1
+attributes, global heap collections).
 
 It is the checker of the library's HDF5 writer: besides reading the content
 back it asserts the structural rules a conforming reader relies on (the
@@ -31,19 +32,25 @@ class Dataset:
 class H5Read:
     def __init__(self, path):
         with open(path, "rb") as f:
-            self.b = f.read()
+            raw = f.read()
         self.gcol_cache = {}
-        b = self.b
-        assert b[:8] == SIG, "superblock signature"
+        # the superblock sits at 0, 512, 1024, 2048, ... (after a user block)
+        at = 0
+        while raw[at:at + 8] != SIG:
+            at = 512 if at == 0 else 2 * at
+            assert at < len(raw), "superblock signature"
+        b = raw[at:]
         ver = b[8]
         assert ver in (0, 1), f"superblock version {ver}"
         self.so, self.sl = b[13], b[14]
         assert (self.so, self.sl) == (8, 8), "8-byte offsets and lengths"
         self.leaf_k, self.node_k = struct.unpack_from("<HH", b, 16)
         p = 24 + (4 if ver == 1 else 0)
-        base, _free, self.eof, _drv = struct.unpack_from("<4Q", b, p)
-        assert base == 0
-        assert self.eof == len(b), f"end-of-file address {self.eof} vs size {len(b)}"
+        base, _free, eof, _drv = struct.unpack_from("<4Q", b, p)
+        assert base == at, "addresses are relative to the superblock"
+        # the stored end-of-file address counts the bytes before the base
+        assert eof == len(raw), f"end-of-file address {eof} vs size {len(raw)}"
+        self.b, self.eof = b, eof - base
         p += 32
         _name_off, root_oh, cache, _ = struct.unpack_from("<QQII", b, p)
         scratch = struct.unpack_from("<QQ", b, p + 24)
@@ -213,18 +220,28 @@ class H5Read:
                 name, val = self.attribute(d)
                 attrs[name] = val
         assert dt is not None and shape is not None and layout is not None
-        ver, cls = layout[0], layout[1]
-        assert ver == 3
+        ver = layout[0]
         n = int(np.prod(shape)) if shape else 1
+        if ver == 3:
+            cls = layout[1]
+            if cls == 1:
+                a, sz = struct.unpack_from("<QQ", layout, 2)
+                assert sz == n * dt["size"], "contiguous size = elements x element size"
+            else:
+                assert cls == 0
+                sz = struct.unpack_from("<H", layout, 2)[0]
+                raw = layout[4:4 + sz]
+        else:  # versions 1 and 2: rank (+1 for the element size), class, 5 reserved
+            assert ver in (1, 2)
+            nd, cls = layout[1], layout[2]
+            assert cls == 1, "contiguous"
+            a = struct.unpack_from("<Q", layout, 8)[0]
+            dims = struct.unpack_from(f"<{nd}I", layout, 16)
+            sz = int(np.prod(dims))
+            assert sz == n * dt["size"]
         if cls == 1:
-            a, sz = struct.unpack_from("<QQ", layout, 2)
-            assert sz == n * dt["size"], "contiguous size = elements x element size"
             self.check_addr(a, sz)
             raw = self.b[a:a + sz]
-        else:
-            assert cls == 0
-            sz = struct.unpack_from("<H", layout, 2)[0]
-            raw = layout[4:4 + sz]
         return Dataset(self.decode(dt, shape, raw), attrs, dt)
 
     def attribute(self, d):

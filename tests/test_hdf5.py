@@ -3,7 +3,10 @@ src/io.c:132-301) written by gasp_create_ising_grids_hdf5 /
 gasp_write_ising_grids_hdf5 through the C ABI, read back by tests/h5read.py,
 an independent reader written from the HDF5 file format specification that
 also checks the structures a conforming reader relies on.  libhdf5 is not
-installed here, so the files are not opened by it."""
+installed here, so the files are not opened by it; the reader itself, and
+two of the writer's encodings, are pinned on a file that libhdf5 wrote
+(scipy's MATLAB 7.3-format test data, HDF5 after a 512-byte user block)."""
+import os
 import struct
 
 import numpy as np
@@ -120,3 +123,63 @@ def test_create_truncates(tmp_path):
     assert _create(p, 16, 2, itask=1) == GASP_OK
     r = h5read.read(p)
     assert "sweep_0" not in r and r["L"].value == 16 and r["ngrids"].value == 2
+
+
+def _libhdf5_file():
+    """scipy's test file testhdf5_7.4_GLNX86.mat: written by MATLAB 7.4 through
+    libhdf5 (a 9x1 double dataset 'testdouble' = (0:8) * pi/4 with the
+    fixed-length string attribute MATLAB_class = 'double')."""
+    try:
+        import scipy.io.matlab as sm
+    except ImportError:
+        return None
+    p = os.path.join(os.path.dirname(sm.__file__), "tests", "data", "testhdf5_7.4_GLNX86.mat")
+    return p if os.path.exists(p) else None
+
+
+def _root_symtab(r):
+    d = next(d for t, _, d in r.messages(r.root_oh) if t == 0x0011)
+    return struct.unpack_from("<QQ", d)
+
+
+def _root_heap_free_list(r):
+    """(free-list head, the first free block's next link or None) of the root
+    group's local heap."""
+    _, heap = _root_symtab(r)
+    size, head, seg = r.u("QQQ", heap + 8)
+    nxt = r.u("Q", seg + head)[0] if head < size else None
+    return head, nxt
+
+
+def _entry_header(r, name):
+    bt, hp = _root_symtab(r)
+    out = []
+    r.walk(bt, r.local_heap(hp), out, None, None, None)
+    return next(oh for n, oh, _, _ in out if n == name)
+
+
+def _datatype_message(r, oh):
+    return next(d for t, _, d in r.messages(oh) if t == 0x0003)
+
+
+def test_reader_and_encodings_pinned_on_a_libhdf5_file(tmp_path):
+    src = _libhdf5_file()
+    if src is None:
+        pytest.skip("scipy's HDF5 test file is not installed")
+    ref = h5read.H5Read(src)
+    content = ref.root()
+    assert list(content) == ["testdouble"]
+    d = content["testdouble"]
+    assert d.value.shape == (9, 1) and d.value.dtype == np.float64
+    assert np.allclose(d.value.ravel(), np.arange(9) * np.pi / 4, rtol=0, atol=1e-15)
+    assert d.attrs == {"MATLAB_class": "double"}
+    # libhdf5 ends a local heap's free list with the value 1; the writer marks
+    # "no free block" with the same value
+    assert _root_heap_free_list(ref)[1] == 1
+    p = tmp_path / "f.hdf5"
+    assert _create(p, 8, 4, h=0.25) == GASP_OK
+    ours = h5read.H5Read(p)
+    assert _root_heap_free_list(ours)[0] == 1
+    # the IEEE little-endian double datatype message, byte for byte
+    assert (_datatype_message(ours, _entry_header(ours, "h")) ==
+            _datatype_message(ref, _entry_header(ref, "testdouble")))
