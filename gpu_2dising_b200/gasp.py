@@ -15,6 +15,9 @@ writer, which follows the HDF5 file format specification without libhdf5
 (src/io.c:132-301).  Differences, all deliberate:
 
 * there is no CPU fallback: without a CUDA device the calls raise;
+* a failed HDF5 write stops the run and raises RuntimeError("Error writing
+  HDF5 file"); the reference sets the same error and lets its driver run on,
+  since it ignores the output callback's return (src/ising_ext.cu:360-366);
 * with ``cv='largest_cluster'`` and thresholds below 2 in magnitude a
   UserWarning is issued through ``warnings`` (the reference sets the warning
   as a pending exception, src/ising_ext.cu:572-577);
