@@ -112,6 +112,19 @@ def test_pygasp_committor_matches_reference(ref_gpu, gasp_mod, tmp_path, monkeyp
     assert out2 == out
 
 
+def test_pygasp_hdf5_write_failure_raises(gasp_mod, tmp_path, monkeypatch, capfd):
+    """A side file that cannot be written stops the run with the reference's
+    RuntimeError text (src/ising_ext.cu:360-366)."""
+    monkeypatch.chdir(tmp_path)
+    os.mkdir("gridstates.hdf5")  # neither creatable nor openable as a file
+    with pytest.raises(RuntimeError, match="Error writing HDF5 file"):
+        gasp_mod.run_nucleation_swarm(16, 32, 40, 0.5, 0.1, mag_output_int=10,
+                                      grid_output_int=20, seed=3)
+    err = capfd.readouterr().err
+    assert "failed to create HDF5 file 'gridstates.hdf5'" in err
+    assert "failed to open HDF5 file 'gridstates.hdf5' for writing" in err
+
+
 def test_pygasp_validation(gasp_mod):
     with pytest.raises(ValueError):
         gasp_mod.run_nucleation_swarm(16, 32, 10, 0.5, 0.1, cv="energy")
